@@ -1,0 +1,213 @@
+/*
+ * ptk.h -- C ABI of the B200 (sm_100a) per-grain tracking path.
+ *
+ * Replaces the call surface of p-tracker's `ptracker` class for particle
+ * tracking (reference src/p-tracker.hpp:66-238): the data members it reads
+ * (images, grains, search zones, options) become a context, and the per-grain
+ * member functions called from OpenMP loops become batched calls over all
+ * grains.  Every function returns an int status (PTK_OK = 0); the reference
+ * instead calls std::exit on I/O errors (src/p-tracker.cpp:98,216,1217,1317).
+ *
+ * Ownership: the caller owns every host array passed in or out; the context
+ * owns its device memory and one CUDA stream (or borrows a caller stream, see
+ * ptk_set_stream).  A context is not thread-safe; distinct contexts are
+ * independent.  All device work of a call is enqueued on the context stream;
+ * calls that return host data synchronise that stream.
+ */
+#ifndef PTK_H
+#define PTK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  PTK_OK = 0,
+  PTK_ERR_ARG = 1,     /* invalid argument                                  */
+  PTK_ERR_STATE = 2,   /* call out of order (e.g. no frame loaded)          */
+  PTK_ERR_CUDA = 3,    /* CUDA runtime error (message in ptk_last_error)    */
+  PTK_ERR_IO = 4,      /* file could not be read or written                 */
+  PTK_ERR_LIMIT = 5,   /* size beyond a documented limit                    */
+  PTK_ERR_TIMEOUT = 6  /* a bounded device wait gave up                     */
+};
+
+/* ---- per-grain status bits (ptk_grain.status) -------------------------- */
+enum {
+  PTK_ST_RESCUED = 1,        /* pixel NCC < NCC_min: rescue search ran        */
+  PTK_ST_SUPER_RESCUED = 2,  /* rescue NCC < NCC_min_super: super-rescue ran  */
+  PTK_ST_FAILED = 4,         /* super-rescue did not exceed NCC_min_super     */
+  PTK_ST_OUT_OF_BOUNDS = 8,  /* pattern + zone + interpolation support leaves
+                                the frame: grain not searched (the reference
+                                reads out of bounds here, src/interpol.cpp:28) */
+  PTK_ST_MASKED = 16,        /* grain_type_2D::masked (src/grain_type_2D.hpp:53) */
+  PTK_ST_SUBPIX_CLAMPED = 32 /* a subpixel sample was clamped to the frame     */
+};
+
+enum { PTK_INTERP_LINEAR = 0, PTK_INTERP_CUBIC = 1, PTK_INTERP_QUINTIC = 2 };
+enum { PTK_SUBPIX_POWELL = 0, PTK_SUBPIX_ADJOINT_LM = 1 };
+enum { PTK_SEARCH_EXACT = 0, PTK_SEARCH_BF16 = 1 };
+enum { PTK_LEVEL_PIXEL = 0, PTK_LEVEL_RESCUE = 1, PTK_LEVEL_SUPER_RESCUE = 2 };
+enum { PTK_PATTERN_CIRC = 0, PTK_PATTERN_RING = 1, PTK_PATTERN_RECT = 2, PTK_PATTERN_GRAIN_DIAMETER = 3 };
+
+/* search_zone_type, reference src/search_zone_type.hpp:20-27 */
+typedef struct ptk_zone {
+  int32_t left, right, up, down; /* pixels, >= 0                             */
+  int32_t num_rot;               /* rotations tested: the list produced by
+                                    for (d = -|inc*num|; d <= |inc*num|; d += inc) */
+  double inc_rot;                /* radians                                   */
+} ptk_zone;
+
+/* One grain: the 13 columns of a dic_out file (reference
+ * src/p-tracker.cpp:1330-1343, grain_type_2D src/grain_type_2D.hpp:23-71). */
+typedef struct ptk_grain {
+  int32_t refcoord_xpix, refcoord_ypix;
+  double refrot, radius_pix;
+  double dx, dy, drot;
+  double upix, vpix, rot_inc;
+  double NCC, NCC_rescue, NCC_subpix;
+  uint8_t masked; /* input: grain is skipped (mask_rect)                      */
+  uint8_t status; /* output: PTK_ST_* bits of the last tracked frame         */
+  uint8_t pad_[6];
+} ptk_grain;
+
+/* Options of the command file that drive tracking (reference
+ * src/p-tracker.cpp:1487-1784; defaults src/p-tracker.hpp:67-178). */
+typedef struct ptk_config {
+  int32_t dimx, dimy;            /* frame size in pixels                      */
+  int32_t rescue_level;          /* -1..2, default 2                          */
+  double NCC_min;                /* default 0.7                               */
+  double NCC_min_super;          /* default 0.5                               */
+  int32_t subpixel;              /* 0/1, default 1                            */
+  double subpix_tol;             /* Powell ftol, default 1e-8                 */
+  double initial_direction[3];   /* dx, dy, dr, default 0.01 each             */
+  int32_t image_interpolator;    /* PTK_INTERP_*, default cubic               */
+  double overflow_stiffness;     /* default 0                                 */
+  double subpix_displacement_max;/* default 3                                 */
+  int32_t rotations;             /* 0 disables rotation search (init rule
+                                    src/p-tracker.cpp:1191-1201)              */
+  ptk_zone zone[3];              /* pixel, rescue, super-rescue               */
+  int32_t iraz;                  /* reference change period, default 0        */
+  int32_t subpix_method;         /* PTK_SUBPIX_*, default POWELL              */
+  int32_t search_method;         /* PTK_SEARCH_*, default EXACT               */
+  int32_t topk;                  /* BF16 search: candidates rescored exactly  */
+  int32_t lm_max_iter;           /* adjoint LM: iteration cap                 */
+  double lm_tol;                 /* adjoint LM: step tolerance (pixels)       */
+} ptk_config;
+
+typedef struct ptk_ctx ptk_ctx;
+
+/* Fills *cfg with the reference defaults (src/p-tracker.hpp:67-178); search
+ * zones (which have no default in the reference) become 0 px, 0 rotations. */
+int ptk_config_default(ptk_config* cfg);
+
+/* Context lifetime.  Replaces ptracker::ptracker / ptracker::init
+ * (src/p-tracker.cpp:19-73, 1150-1210). */
+int ptk_create(ptk_ctx** out, const ptk_config* cfg);
+int ptk_destroy(ptk_ctx* ctx);
+int ptk_set_config(ptk_ctx* ctx, const ptk_config* cfg);
+
+/* Replaces ptracker::search_zone / search_zone_rescue / search_zone_super_rescue
+ * assignment in read_data (src/p-tracker.cpp:1616-1669). */
+int ptk_set_search_zone(ptk_ctx* ctx, int level, const ptk_zone* zone);
+
+/* Grains.  Replaces read_grains' fill of ptracker::grain
+ * (src/p-tracker.cpp:1213-1278) and the dic_out write (src/p-tracker.cpp:1313-1360). */
+int ptk_set_grains(ptk_ctx* ctx, const ptk_grain* grains, int n);
+int ptk_get_grains(ptk_ctx* ctx, ptk_grain* out, int n);
+
+/* Patterns as CSR: grain g owns offsets_xy[2*starts[g] .. 2*starts[g+1]).
+ * Replaces make_custom_pattern (src/p-tracker.cpp:1444-1476). */
+int ptk_set_patterns(ptk_ctx* ctx, const int32_t* offsets_xy, const int64_t* starts, int n);
+/* Generators of the `pattern` token (src/p-tracker.cpp:1650-1688):
+ * CIRC a, RING a b, RECT a b, GRAIN_DIAMETER (radius_reduction=a, min_radius=b);
+ * applied to every grain whose radius equals target_radius, or to all grains
+ * when target_radius < 0 (targetRadiusPattern). */
+int ptk_make_patterns(ptk_ctx* ctx, int kind, double a, double b, double target_radius);
+int ptk_pattern_size(ptk_ctx* ctx, int grain, int* npts);
+
+/* Frames.  slot 0 = reference image, 1 = current image (ptracker::image[
+ * im_index_ref / im_index_current], src/p-tracker.hpp:80-83).  `pix` is a
+ * row-major host buffer of 1- or 2-byte grey levels with `pitch_bytes` per
+ * row; 1-byte values are widened to uint16 unchanged.  Replaces read_image
+ * (src/p-tracker.cpp:75-83) after decode. */
+int ptk_load_frame(ptk_ctx* ctx, int slot, const void* pix, int dimx, int dimy, int bytes_per_px,
+                   size_t pitch_bytes);
+/* Same with a device pointer (uint16, row-major, pitch in bytes). */
+int ptk_load_frame_device(ptk_ctx* ctx, int slot, const void* dev_pix, size_t pitch_bytes);
+/* Copies a slot back to the host as uint16 rows of dimx values. */
+int ptk_read_frame(ptk_ctx* ctx, int slot, uint16_t* out);
+
+/* Stages.  ptk_precompute replaces do_precomputations (src/p-tracker.cpp:624-656).
+ * ptk_search(level) replaces the omp loops of follow_pattern_pixel /
+ * follow_pattern_rescue_pixel / follow_pattern_super_rescue_pixel
+ * (src/p-tracker.cpp:471-536, 659-1016); level 0 also performs the
+ * reset()/backup() of every grain (src/p-tracker.cpp:478-479) and rebuilds
+ * the rescue list, levels 1/2 consume the lists left by the previous level.
+ * ptk_subpixel replaces follow_pattern_subpixel_xyR (src/p-tracker.cpp:1090-1128). */
+int ptk_precompute(ptk_ctx* ctx);
+int ptk_search(ptk_ctx* ctx, int level);
+int ptk_subpixel(ptk_ctx* ctx, int method);
+/* Increments upix = dx - dx_prev ... and, when num_image - iref >= iraz, the
+ * reference change (src/p-tracker.cpp:577-611). */
+int ptk_end_frame(ptk_ctx* ctx, int num_image);
+/* The whole per-frame body of particle_tracking after the image read
+ * (src/p-tracker.cpp:458-611, file output excluded), captured once as a CUDA
+ * graph and replayed. */
+int ptk_track_frame(ptk_ctx* ctx, int num_image);
+/* Forces the reference change of ptk_end_frame regardless of iraz. */
+int ptk_swap_reference(ptk_ctx* ctx, int num_image);
+int ptk_set_iref(ptk_ctx* ctx, int iref);
+
+/* Rescue bookkeeping of the last frame: counts of ptracker::to_be_rescued /
+ * to_be_super_rescued (src/p-tracker.hpp:108-118). */
+int ptk_get_rescue_counts(ptk_ctx* ctx, int* n_rescued, int* n_super_rescued);
+
+/* Subpixel objective NCC_to_minimize_xyR (src/p-tracker.cpp:1018-1088) for
+ * every grain at X[3*g .. 3*g+2]; f[g] receives (1 - NCC) * W. */
+int ptk_objective(ptk_ctx* ctx, const double* X3n, double* f);
+/* Same objective and its gradient with respect to (dx, dy, drot) through the
+ * cubic interpolation (adjoint kernel; no reference counterpart). */
+int ptk_grad(ptk_ctx* ctx, const double* X3n, double* f, double* g3n);
+
+/* Distortion correction.  params14 in the order of
+ * ptracker::disto_parameters (src/p-tracker.hpp:151-165) as used by undistor
+ * (src/distortion_correction.cpp:20-61).  ptk_remap_frame resamples a slot so
+ * that pixel (x, y) holds the distorted frame at the point whose undistor()
+ * image is (x, y) (cubic interpolation, rounded); pixels whose support leaves
+ * the frame become 0.  The inverse map is computed once per parameter set and
+ * cached on the device. */
+int ptk_set_distortion(ptk_ctx* ctx, const double* params14);
+int ptk_remap_frame(ptk_ctx* ctx, int slot);
+
+/* Stream control.  A non-null stream is borrowed (not destroyed). */
+int ptk_set_stream(ptk_ctx* ctx, void* cuda_stream);
+void* ptk_get_stream(ptk_ctx* ctx);
+int ptk_synchronize(ptk_ctx* ctx);
+/* Number of device kernels this context launched since creation. */
+int64_t ptk_kernel_launches(ptk_ctx* ctx);
+
+/* sizeof of the ABI structs as compiled into the library, for FFI binders. */
+int ptk_abi_sizes(size_t* config_bytes, size_t* grain_bytes, size_t* zone_bytes);
+
+/* Last error message of the context (static storage if ctx is NULL). */
+const char* ptk_last_error(ptk_ctx* ctx);
+
+/* Grain files.  ptk_read_grains_file parses the 13-column dic_out form
+ * (format13 != 0, restart_file, src/p-tracker.cpp:1235-1252) or the
+ * 4-column start form (format13 == 0, grains_to_follow,
+ * src/p-tracker.cpp:1253-1272).  Call once with out == NULL to get the count.
+ * ptk_save_grains_file writes the dic_out form byte for byte as
+ * save_grains (src/p-tracker.cpp:1313-1360). */
+int ptk_read_grains_file(const char* path, int format13, ptk_grain* out, int capacity, int* n);
+int ptk_save_grains_file(const char* path, const ptk_grain* grains, int n, const char* from_image,
+                         const char* from_datetime, const char* to_image, const char* to_datetime);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PTK_H */

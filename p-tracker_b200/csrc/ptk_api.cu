@@ -1,0 +1,939 @@
+// Host runtime of the C ABI declared in include/ptk.h.
+//
+// A context owns: both frames (uint16, row-major, pitch rounded to 64 pixels),
+// the grain state as one device block of structure-of-arrays, the patterns in
+// CSR form, the rotation-step lists of the three zones, the device-built
+// rescue lists, the search scratch, the cached undistortion map, and the CUDA
+// graphs of the per-frame pipeline.  Every launch goes to the context stream.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ptk_internal.cuh"
+
+using namespace ptk;
+
+namespace {
+
+constexpr int kMaxRotSteps = 4096;
+thread_local std::string g_static_error;
+
+// Layout of the grain block: 16 double fields, 2 int64 fields, 3 int32 fields,
+// 2 uint8 fields, each n entries, in this order.
+enum { D_REFROT, D_RADIUS, D_DX, D_DY, D_DROT, D_DXP, D_DYP, D_DROTP, D_UPIX, D_VPIX, D_ROTINC, D_NCC, D_NCCR, D_NCCS,
+       D_MEAN0, D_C0C0, D_COUNT };
+enum { L_S0, L_S00, L_COUNT };
+enum { I_REFX, I_REFY, I_FLAGS, I_COUNT };
+enum { B_MASKED, B_STATUS, B_COUNT };
+
+struct BlockLayout {
+  size_t d_off, l_off, i_off, b_off, total;
+  explicit BlockLayout(int n) {
+    const size_t nn = (size_t)(n > 0 ? n : 1);
+    d_off = 0;
+    l_off = d_off + D_COUNT * nn * 8;
+    i_off = l_off + L_COUNT * nn * 8;
+    b_off = i_off + ((I_COUNT * nn * 4 + 15) & ~(size_t)15);
+    total = b_off + ((B_COUNT * nn + 15) & ~(size_t)15);
+  }
+};
+
+}  // namespace
+
+struct ptk_ctx {
+  ptk_config cfg{};
+  int device{0};
+  int num_sms{148};
+  cudaStream_t stream{nullptr};
+  cudaStream_t own_stream{nullptr};
+  cudaStream_t cap_stream{nullptr};
+  std::string err;
+  int64_t launches{0};
+
+  // frames
+  int pitch{0};
+  uint16_t* d_img[2]{nullptr, nullptr};
+  uint16_t* d_tmp{nullptr};
+  uint8_t* d_u8{nullptr};
+  int ref_slot{0}, cur_slot{1};
+  bool loaded[2]{false, false};
+
+  // grains
+  int n{0};
+  void* d_block{nullptr};
+  GrainsDev g{};
+  std::vector<double> h_radius;
+
+  // patterns
+  std::vector<std::vector<short2>> h_pat;
+  int* d_pstart{nullptr};
+  short2* d_pat{nullptr};
+  short2* d_pat0{nullptr};
+  uint16_t* d_w0{nullptr};
+  int* d_order{nullptr};
+  int max_P{0};
+  int max_R{0};
+  bool patterns_ok{false};
+
+  // zones
+  std::vector<double> steps[3];
+  double* d_steps[3]{nullptr, nullptr, nullptr};
+
+  // lists: counts[0] = n (level-0 list), counts[1] rescue, counts[2] super-rescue
+  int* d_counts{nullptr};
+  int* d_lists{nullptr};  // [rescue n][super n]
+  int* d_work{nullptr};
+  SearchBest* d_best{nullptr};
+  size_t best_cap{0};
+
+  // distortion
+  double disto[14]{};
+  bool have_disto{false};
+  double2* d_map{nullptr};
+  bool map_valid{false};
+
+  // objective buffers
+  double* d_X{nullptr};
+  double* d_f{nullptr};
+  double* d_gr{nullptr};
+
+  // per-frame graphs, keyed by (ref_slot, precompute, swap)
+  cudaGraphExec_t graph[8]{};
+  bool graph_dirty{true};
+
+  int iref{0};
+  bool need_precompute{true};
+};
+
+namespace {
+
+int fail(ptk_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  else g_static_error = msg;
+  return code;
+}
+
+int cuda_fail(ptk_ctx* c, cudaError_t e, const char* what) {
+  return fail(c, PTK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                      \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+  } while (0)
+
+void drop_graphs(ptk_ctx* c) {
+  for (auto& ge : c->graph)
+    if (ge) {
+      cudaGraphExecDestroy(ge);
+      ge = nullptr;
+    }
+  c->graph_dirty = false;
+}
+
+void invalidate(ptk_ctx* c) { c->graph_dirty = true; }
+
+FrameDev frame(const ptk_ctx* c, int phys) {
+  return FrameDev{c->d_img[phys], c->pitch, c->cfg.dimx, c->cfg.dimy};
+}
+
+SubpixParams subpix_params(const ptk_ctx* c) {
+  SubpixParams sp;
+  sp.tol = c->cfg.subpix_tol;
+  for (int i = 0; i < 3; ++i) sp.init_dir[i] = c->cfg.initial_direction[i];
+  sp.disp_max = c->cfg.subpix_displacement_max;
+  sp.stiffness = c->cfg.overflow_stiffness;
+  sp.interp = c->cfg.image_interpolator;
+  return sp;
+}
+
+// Rotation steps exactly as the reference's loops produce them
+// (src/p-tracker.cpp:684-686); with `rotations 0` every zone becomes
+// inc_rot = 1, num_rot = 0 (src/p-tracker.cpp:1191-1201).
+int build_steps(ptk_ctx* c, int level) {
+  const ptk_zone& z = c->cfg.zone[level];
+  double inc = z.inc_rot;
+  int num = z.num_rot;
+  if (c->cfg.rotations == 0) {
+    inc = 1.0;
+    num = 0;
+  }
+  std::vector<double> s;
+  const double rotmax = std::fabs(inc * num);
+  if (!(inc > 0.0)) return fail(c, PTK_ERR_ARG, "search zone inc_rot must be > 0 (the reference loops forever)");
+  for (double drot = -rotmax; drot <= rotmax; drot += inc) {
+    s.push_back(drot);
+    if ((int)s.size() > kMaxRotSteps) return fail(c, PTK_ERR_LIMIT, "more than 4096 rotation steps in a zone");
+  }
+  if (z.left < 0 || z.right < 0 || z.up < 0 || z.down < 0) return fail(c, PTK_ERR_ARG, "negative search zone");
+  if ((long long)(z.left + z.right + 1) * (z.up + z.down + 1) * (long long)s.size() > (1ll << 30))
+    return fail(c, PTK_ERR_LIMIT, "search zone has more than 2^30 candidates");
+  c->steps[level] = s;
+  if (c->d_steps[level]) cudaFree(c->d_steps[level]);
+  c->d_steps[level] = nullptr;
+  cudaError_t e = cudaMalloc(&c->d_steps[level], sizeof(double) * (s.size() ? s.size() : 1));
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc(steps)");
+  e = cudaMemcpy(c->d_steps[level], s.data(), sizeof(double) * s.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaMemcpy(steps)");
+  invalidate(c);
+  return PTK_OK;
+}
+
+void bind_grains(ptk_ctx* c) {
+  BlockLayout L(c->n);
+  char* base = static_cast<char*>(c->d_block);
+  const size_t nn = (size_t)(c->n > 0 ? c->n : 1);
+  auto D = [&](int k) { return reinterpret_cast<double*>(base + L.d_off + k * nn * 8); };
+  auto Lf = [&](int k) { return reinterpret_cast<long long*>(base + L.l_off + k * nn * 8); };
+  auto I = [&](int k) { return reinterpret_cast<int*>(base + L.i_off + k * nn * 4); };
+  auto B = [&](int k) { return reinterpret_cast<uint8_t*>(base + L.b_off + k * nn); };
+  GrainsDev& g = c->g;
+  g.n = c->n;
+  g.refrot = D(D_REFROT);
+  g.radius = D(D_RADIUS);
+  g.dx = D(D_DX);
+  g.dy = D(D_DY);
+  g.drot = D(D_DROT);
+  g.dx_prev = D(D_DXP);
+  g.dy_prev = D(D_DYP);
+  g.drot_prev = D(D_DROTP);
+  g.upix = D(D_UPIX);
+  g.vpix = D(D_VPIX);
+  g.rot_inc = D(D_ROTINC);
+  g.ncc = D(D_NCC);
+  g.ncc_rescue = D(D_NCCR);
+  g.ncc_subpix = D(D_NCCS);
+  g.mean0 = D(D_MEAN0);
+  g.c0c0 = D(D_C0C0);
+  g.s0 = Lf(L_S0);
+  g.s00 = Lf(L_S00);
+  g.refx = I(I_REFX);
+  g.refy = I(I_REFY);
+  g.flags = I(I_FLAGS);
+  g.masked = B(B_MASKED);
+  g.status = B(B_STATUS);
+  g.pstart = c->d_pstart;
+  g.pat = c->d_pat;
+  g.pat0 = c->d_pat0;
+  g.w0 = c->d_w0;
+}
+
+int upload_patterns(ptk_ctx* c) {
+  const int n = c->n;
+  std::vector<int> start(n + 1, 0);
+  int maxP = 0;
+  double maxnorm = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const size_t P = c->h_pat[i].size();
+    if (P > (size_t)kMaxPatternPoints)
+      return fail(c, PTK_ERR_LIMIT, "pattern of grain " + std::to_string(i) + " has more than 16384 points");
+    if ((long long)start[i] + (long long)P > (1ll << 30)) return fail(c, PTK_ERR_LIMIT, "too many pattern points");
+    start[i + 1] = start[i] + (int)P;
+    maxP = std::max(maxP, (int)P);
+    for (const short2& q : c->h_pat[i]) maxnorm = std::max(maxnorm, std::sqrt((double)q.x * q.x + (double)q.y * q.y));
+  }
+  const size_t total = (size_t)start[n];
+  std::vector<short2> flat;
+  flat.reserve(total);
+  for (int i = 0; i < n; ++i) flat.insert(flat.end(), c->h_pat[i].begin(), c->h_pat[i].end());
+  cudaFree(c->d_pstart);
+  cudaFree(c->d_pat);
+  cudaFree(c->d_pat0);
+  cudaFree(c->d_w0);
+  cudaFree(c->d_order);
+  c->d_pstart = nullptr;
+  c->d_pat = c->d_pat0 = nullptr;
+  c->d_w0 = nullptr;
+  c->d_order = nullptr;
+  CK(cudaMalloc(&c->d_pstart, sizeof(int) * (n + 1)));
+  CK(cudaMalloc(&c->d_pat, sizeof(short2) * (total ? total : 1)));
+  CK(cudaMalloc(&c->d_pat0, sizeof(short2) * (total ? total : 1)));
+  CK(cudaMalloc(&c->d_w0, sizeof(uint16_t) * (total ? total : 1)));
+  CK(cudaMalloc(&c->d_order, sizeof(int) * (n ? n : 1)));
+  CK(cudaMemcpy(c->d_pstart, start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  if (total) CK(cudaMemcpy(c->d_pat, flat.data(), sizeof(short2) * total, cudaMemcpyHostToDevice));
+  // level-0 work order: decreasing pattern size (heavy grains first)
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return c->h_pat[a].size() > c->h_pat[b].size(); });
+  if (n) CK(cudaMemcpy(c->d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  int cnt0 = n;
+  CK(cudaMemcpy(c->d_counts, &cnt0, sizeof(int), cudaMemcpyHostToDevice));
+  c->max_P = maxP;
+  c->max_R = (int)std::ceil(maxnorm) + 1;
+  c->patterns_ok = true;
+  for (int i = 0; i < n; ++i)
+    if (c->h_pat[i].empty()) c->patterns_ok = false;
+  bind_grains(c);
+  c->need_precompute = true;
+  invalidate(c);
+  return PTK_OK;
+}
+
+int check_ready(ptk_ctx* c, bool need_frames) {
+  if (c->n <= 0) return fail(c, PTK_ERR_STATE, "no grains set");
+  if (!c->patterns_ok) return fail(c, PTK_ERR_STATE, "some grains have no pattern");
+  if (need_frames && !(c->loaded[0] && c->loaded[1])) return fail(c, PTK_ERR_STATE, "both frames must be loaded");
+  return PTK_OK;
+}
+
+// Enqueue helpers (no synchronisation; usable inside stream capture).
+int enqueue_precompute(ptk_ctx* c, cudaStream_t s) {
+  launch_precompute(c->g, frame(c, c->ref_slot), s);
+  c->launches += 1;
+  return PTK_OK;
+}
+
+struct SearchGeom {
+  int nrot, nu, nv, tiles_u, tiles_v;
+  size_t smem;
+  int grid;
+  size_t items;
+};
+
+int search_geometry(ptk_ctx* c, int level, SearchGeom* sg) {
+  const ptk_zone& z = c->cfg.zone[level];
+  sg->nrot = (int)c->steps[level].size();
+  sg->nu = z.left + z.right + 1;
+  sg->nv = z.up + z.down + 1;
+  sg->tiles_u = (sg->nu + kTileU - 1) / kTileU;
+  sg->tiles_v = (sg->nv + kTileV - 1) / kTileV;
+  const int span = 2 * c->max_R + kTileU;
+  sg->smem = search_smem_bytes(c->max_P, span * span);
+  if (sg->smem > 227 * 1024) return fail(c, PTK_ERR_LIMIT, "pattern too large for the shared-memory search tile");
+  sg->items = (size_t)c->n * sg->nrot * sg->tiles_u * sg->tiles_v;
+  if (sg->items > (size_t)INT32_MAX) return fail(c, PTK_ERR_LIMIT, "too many search work items");
+  const int occ = search_occupancy(sg->smem);
+  sg->grid = c->num_sms * (occ > 0 ? occ : 1);
+  return PTK_OK;
+}
+
+int ensure_best(ptk_ctx* c, size_t items) {
+  if (items <= c->best_cap) return PTK_OK;
+  cudaFree(c->d_best);
+  c->d_best = nullptr;
+  CK(cudaMalloc(&c->d_best, sizeof(SearchBest) * items));
+  c->best_cap = items;
+  invalidate(c);
+  return PTK_OK;
+}
+
+int enqueue_search(ptk_ctx* c, int level, cudaStream_t s) {
+  SearchGeom sg;
+  int rc = search_geometry(c, level, &sg);
+  if (rc) return rc;
+  if (c->best_cap < sg.items) return fail(c, PTK_ERR_STATE, "search scratch not prepared");
+  if (level == 0) {
+    launch_stage_begin(c->g, c->d_counts, s);
+    c->launches += 1;
+  }
+  const int* list = level == 0 ? c->d_order : (level == 1 ? c->d_lists : c->d_lists + c->n);
+  const int* count = c->d_counts + level;
+  CK(cudaMemsetAsync(c->d_work, 0, sizeof(int), s));
+  const ptk_zone& z = c->cfg.zone[level];
+  SearchLaunch p;
+  p.g = c->g;
+  p.cur = frame(c, c->cur_slot);
+  p.list = list;
+  p.list_count = count;
+  p.work_next = c->d_work;
+  p.steps = c->d_steps[level];
+  p.nrot = sg.nrot;
+  p.left = z.left;
+  p.right = z.right;
+  p.up = z.up;
+  p.down = z.down;
+  p.tiles_u = sg.tiles_u;
+  p.tiles_v = sg.tiles_v;
+  p.best = c->d_best;
+  p.max_items = (int)c->best_cap;
+  launch_search(p, sg.grid, sg.smem, s);
+  FinalizeLaunch f;
+  f.g = c->g;
+  f.list = list;
+  f.list_count = count;
+  f.steps = c->d_steps[level];
+  f.nrot = sg.nrot;
+  f.left = z.left;
+  f.up = z.up;
+  f.nu = sg.nu;
+  f.nv = sg.nv;
+  f.tiles = sg.tiles_u * sg.tiles_v;
+  f.best = c->d_best;
+  f.level = level;
+  f.NCC_min = c->cfg.NCC_min;
+  f.NCC_min_super = c->cfg.NCC_min_super;
+  f.out_list = level == 0 ? c->d_lists : c->d_lists + c->n;
+  f.out_count = c->d_counts + (level == 0 ? 1 : 2);
+  launch_finalize(f, c->n, s);
+  c->launches += 2;
+  return PTK_OK;
+}
+
+int enqueue_subpixel(ptk_ctx* c, int method, cudaStream_t s) {
+  if (method != PTK_SUBPIX_POWELL) return fail(c, PTK_ERR_ARG, "subpixel method not available");
+  launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, s);
+  c->launches += 1;
+  return PTK_OK;
+}
+
+int prepare_searches(ptk_ctx* c) {
+  size_t need = 0;
+  for (int level = 0; level < 3; ++level) {
+    if (level > c->cfg.rescue_level) break;
+    SearchGeom sg;
+    int rc = search_geometry(c, level, &sg);
+    if (rc) return rc;
+    need = std::max(need, sg.items);
+  }
+  return ensure_best(c, need ? need : 1);
+}
+
+// Enqueues one frame body; `swap` decided by the caller.
+int enqueue_frame(ptk_ctx* c, bool precompute, bool swap, cudaStream_t s) {
+  int rc;
+  if (precompute && (rc = enqueue_precompute(c, s))) return rc;
+  if (c->cfg.rescue_level >= 0 && (rc = enqueue_search(c, 0, s))) return rc;
+  if (c->cfg.rescue_level >= 1 && (rc = enqueue_search(c, 1, s))) return rc;
+  if (c->cfg.rescue_level >= 2 && (rc = enqueue_search(c, 2, s))) return rc;
+  if (c->cfg.subpixel && (rc = enqueue_subpixel(c, c->cfg.subpix_method, s))) return rc;
+  launch_end_frame(c->g, swap ? 1 : 0, s);
+  c->launches += 1;
+  return PTK_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int ptk_config_default(ptk_config* cfg) {
+  if (!cfg) return fail(nullptr, PTK_ERR_ARG, "null config");
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->rescue_level = 2;
+  cfg->NCC_min = 0.7;
+  cfg->NCC_min_super = 0.5;
+  cfg->subpixel = 1;
+  cfg->subpix_tol = 1e-8;
+  cfg->initial_direction[0] = cfg->initial_direction[1] = cfg->initial_direction[2] = 0.01;
+  cfg->image_interpolator = PTK_INTERP_CUBIC;
+  cfg->overflow_stiffness = 0.0;
+  cfg->subpix_displacement_max = 3.0;
+  cfg->rotations = 1;
+  for (int l = 0; l < 3; ++l) {
+    cfg->zone[l].inc_rot = 1.0;
+    cfg->zone[l].num_rot = 0;
+  }
+  cfg->iraz = 0;
+  cfg->subpix_method = PTK_SUBPIX_POWELL;
+  cfg->search_method = PTK_SEARCH_EXACT;
+  cfg->topk = 8;
+  cfg->lm_max_iter = 30;
+  cfg->lm_tol = 1e-6;
+  return PTK_OK;
+}
+
+int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
+  if (!out || !cfg) return fail(nullptr, PTK_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (cfg->dimx < 4 || cfg->dimy < 4 || cfg->dimx > 65535 || cfg->dimy > 65535)
+    return fail(nullptr, PTK_ERR_ARG, "frame size must be within 4..65535 pixels");
+  ptk_ctx* c = new ptk_ctx();
+  c->cfg = *cfg;
+  auto bail = [&](int rc) {
+    g_static_error = c->err;
+    ptk_destroy(c);
+    return rc;
+  };
+  cudaError_t e = cudaGetDevice(&c->device);
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaGetDevice"));
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+  e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
+  e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
+  c->stream = c->own_stream;
+  c->pitch = (cfg->dimx + 63) & ~63;
+  const size_t bytes = (size_t)c->pitch * cfg->dimy * sizeof(uint16_t);
+  for (int k = 0; k < 2; ++k) {
+    e = cudaMalloc(&c->d_img[k], bytes);
+    if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(frame)"));
+    cudaMemset(c->d_img[k], 0, bytes);
+  }
+  e = cudaMalloc(&c->d_counts, 4 * sizeof(int));
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(counts)"));
+  cudaMemset(c->d_counts, 0, 4 * sizeof(int));
+  e = cudaMalloc(&c->d_work, sizeof(int));
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(work)"));
+  for (int l = 0; l < 3; ++l) {
+    int rc = build_steps(c, l);
+    if (rc) return bail(rc);
+  }
+  *out = c;
+  return PTK_OK;
+}
+
+int ptk_destroy(ptk_ctx* c) {
+  if (!c) return PTK_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  cudaFree(c->d_img[0]);
+  cudaFree(c->d_img[1]);
+  cudaFree(c->d_tmp);
+  cudaFree(c->d_u8);
+  cudaFree(c->d_block);
+  cudaFree(c->d_pstart);
+  cudaFree(c->d_pat);
+  cudaFree(c->d_pat0);
+  cudaFree(c->d_w0);
+  cudaFree(c->d_order);
+  for (int l = 0; l < 3; ++l) cudaFree(c->d_steps[l]);
+  cudaFree(c->d_counts);
+  cudaFree(c->d_lists);
+  cudaFree(c->d_work);
+  cudaFree(c->d_best);
+  cudaFree(c->d_map);
+  cudaFree(c->d_X);
+  cudaFree(c->d_f);
+  cudaFree(c->d_gr);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  delete c;
+  return PTK_OK;
+}
+
+int ptk_set_config(ptk_ctx* c, const ptk_config* cfg) {
+  if (!c || !cfg) return fail(c, PTK_ERR_ARG, "null argument");
+  if (cfg->dimx != c->cfg.dimx || cfg->dimy != c->cfg.dimy)
+    return fail(c, PTK_ERR_ARG, "frame size cannot change on a context");
+  if (cfg->rescue_level < -1 || cfg->rescue_level > 2) return fail(c, PTK_ERR_ARG, "rescue_level must be -1..2");
+  c->cfg = *cfg;
+  for (int l = 0; l < 3; ++l) {
+    int rc = build_steps(c, l);
+    if (rc) return rc;
+  }
+  invalidate(c);
+  return PTK_OK;
+}
+
+int ptk_set_search_zone(ptk_ctx* c, int level, const ptk_zone* z) {
+  if (!c || !z || level < 0 || level > 2) return fail(c, PTK_ERR_ARG, "bad search zone arguments");
+  const ptk_zone old = c->cfg.zone[level];
+  c->cfg.zone[level] = *z;
+  int rc = build_steps(c, level);
+  if (rc) c->cfg.zone[level] = old;
+  return rc;
+}
+
+int ptk_set_grains(ptk_ctx* c, const ptk_grain* grains, int n) {
+  if (!c || (n > 0 && !grains) || n < 0) return fail(c, PTK_ERR_ARG, "bad grain arguments");
+  CK(cudaStreamSynchronize(c->stream));
+  if (n != c->n) {
+    cudaFree(c->d_block);
+    cudaFree(c->d_lists);
+    c->d_block = nullptr;
+    c->d_lists = nullptr;
+    c->n = n;
+    BlockLayout L(n);
+    CK(cudaMalloc(&c->d_block, L.total));
+    CK(cudaMalloc(&c->d_lists, sizeof(int) * 2 * (n > 0 ? n : 1)));
+    c->h_pat.assign(n, std::vector<short2>());
+    c->patterns_ok = false;
+    cudaFree(c->d_best);
+    c->d_best = nullptr;
+    c->best_cap = 0;
+  }
+  BlockLayout L(n);
+  std::vector<char> h(L.total, 0);
+  const size_t nn = (size_t)(n > 0 ? n : 1);
+  auto D = [&](int k) { return reinterpret_cast<double*>(h.data() + L.d_off + k * nn * 8); };
+  auto I = [&](int k) { return reinterpret_cast<int*>(h.data() + L.i_off + k * nn * 4); };
+  auto B = [&](int k) { return reinterpret_cast<uint8_t*>(h.data() + L.b_off + k * nn); };
+  c->h_radius.resize(n);
+  for (int i = 0; i < n; ++i) {
+    const ptk_grain& s = grains[i];
+    I(I_REFX)[i] = s.refcoord_xpix;
+    I(I_REFY)[i] = s.refcoord_ypix;
+    D(D_REFROT)[i] = s.refrot;
+    D(D_RADIUS)[i] = s.radius_pix;
+    D(D_DX)[i] = s.dx;
+    D(D_DY)[i] = s.dy;
+    D(D_DROT)[i] = s.drot;
+    D(D_DXP)[i] = s.dx;
+    D(D_DYP)[i] = s.dy;
+    D(D_DROTP)[i] = s.drot;
+    D(D_UPIX)[i] = s.upix;
+    D(D_VPIX)[i] = s.vpix;
+    D(D_ROTINC)[i] = s.rot_inc;
+    D(D_NCC)[i] = s.NCC;
+    D(D_NCCR)[i] = s.NCC_rescue;
+    D(D_NCCS)[i] = s.NCC_subpix;
+    B(B_MASKED)[i] = s.masked ? 1 : 0;
+    c->h_radius[i] = s.radius_pix;
+  }
+  if (n) CK(cudaMemcpy(c->d_block, h.data(), L.total, cudaMemcpyHostToDevice));
+  bind_grains(c);
+  c->need_precompute = true;
+  invalidate(c);
+  return PTK_OK;
+}
+
+int ptk_get_grains(ptk_ctx* c, ptk_grain* out, int n) {
+  if (!c || (n > 0 && !out)) return fail(c, PTK_ERR_ARG, "bad arguments");
+  if (n != c->n) return fail(c, PTK_ERR_ARG, "grain count mismatch");
+  if (n == 0) return PTK_OK;
+  BlockLayout L(n);
+  std::vector<char> h(L.total);
+  CK(cudaMemcpyAsync(h.data(), c->d_block, L.total, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const size_t nn = (size_t)n;
+  auto D = [&](int k) { return reinterpret_cast<const double*>(h.data() + L.d_off + k * nn * 8); };
+  auto I = [&](int k) { return reinterpret_cast<const int*>(h.data() + L.i_off + k * nn * 4); };
+  auto B = [&](int k) { return reinterpret_cast<const uint8_t*>(h.data() + L.b_off + k * nn); };
+  for (int i = 0; i < n; ++i) {
+    ptk_grain& s = out[i];
+    std::memset(&s, 0, sizeof(s));
+    s.refcoord_xpix = I(I_REFX)[i];
+    s.refcoord_ypix = I(I_REFY)[i];
+    s.refrot = D(D_REFROT)[i];
+    s.radius_pix = D(D_RADIUS)[i];
+    s.dx = D(D_DX)[i];
+    s.dy = D(D_DY)[i];
+    s.drot = D(D_DROT)[i];
+    s.upix = D(D_UPIX)[i];
+    s.vpix = D(D_VPIX)[i];
+    s.rot_inc = D(D_ROTINC)[i];
+    s.NCC = D(D_NCC)[i];
+    s.NCC_rescue = D(D_NCCR)[i];
+    s.NCC_subpix = D(D_NCCS)[i];
+    s.masked = B(B_MASKED)[i];
+    s.status = B(B_STATUS)[i];
+  }
+  return PTK_OK;
+}
+
+int ptk_set_patterns(ptk_ctx* c, const int32_t* xy, const int64_t* starts, int n) {
+  if (!c || n != c->n || (n > 0 && (!xy || !starts))) return fail(c, PTK_ERR_ARG, "bad pattern arguments");
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < n; ++i) {
+    if (starts[i + 1] < starts[i]) return fail(c, PTK_ERR_ARG, "pattern starts must be non-decreasing");
+    std::vector<short2>& v = c->h_pat[i];
+    v.clear();
+    for (int64_t k = starts[i]; k < starts[i + 1]; ++k) {
+      const int32_t x = xy[2 * k], y = xy[2 * k + 1];
+      if (x < -4096 || x > 4096 || y < -4096 || y > 4096) return fail(c, PTK_ERR_LIMIT, "pattern offset beyond 4096 px");
+      v.push_back(make_short2((short)x, (short)y));
+    }
+  }
+  return upload_patterns(c);
+}
+
+int ptk_make_patterns(ptk_ctx* c, int kind, double a, double b, double target_radius) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  if (c->n <= 0) return fail(c, PTK_ERR_STATE, "set grains before patterns");
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < c->n; ++i) {
+    if (!(target_radius < 0.0 || c->h_radius[i] == target_radius)) continue;
+    std::vector<short2>& v = c->h_pat[i];
+    v.clear();
+    int r_in = 0, r_out = 0, hw = 0, hh = 0;
+    int k = kind;
+    if (kind == PTK_PATTERN_GRAIN_DIAMETER) {
+      // src/p-tracker.cpp:1656-1666
+      int radius = (int)(c->h_radius[i] * a);
+      if (radius < b) radius = (int)b;
+      r_out = radius;
+      k = PTK_PATTERN_CIRC;
+    } else if (kind == PTK_PATTERN_CIRC) {
+      r_out = (int)a;
+    } else if (kind == PTK_PATTERN_RING) {
+      r_in = (int)a;
+      r_out = (int)b;
+    } else if (kind == PTK_PATTERN_RECT) {
+      hw = (int)a;
+      hh = (int)b;
+    } else {
+      return fail(c, PTK_ERR_ARG, "unknown pattern kind");
+    }
+    if (r_out > 64 || hw > 64 || hh > 64) return fail(c, PTK_ERR_LIMIT, "pattern radius above 64 px");
+    if (k == PTK_PATTERN_RECT) {  // src/p-tracker.cpp:1369-1384
+      for (int dy = -hh; dy <= hh; ++dy)
+        for (int dx = -hw; dx <= hw; ++dx) v.push_back(make_short2((short)dx, (short)dy));
+    } else {  // circ / ring, src/p-tracker.cpp:1386-1442
+      for (int dy = -r_out; dy <= r_out; ++dy)
+        for (int dx = -r_out; dx <= r_out; ++dx) {
+          const double dst = std::sqrt((double)dx * (double)dx + (double)dy * (double)dy);
+          const bool in = k == PTK_PATTERN_CIRC ? dst <= (double)r_out
+                                                 : (dst <= (double)r_out && dst >= (double)r_in);
+          if (in) v.push_back(make_short2((short)dx, (short)dy));
+        }
+    }
+  }
+  return upload_patterns(c);
+}
+
+int ptk_pattern_size(ptk_ctx* c, int grain, int* npts) {
+  if (!c || !npts || grain < 0 || grain >= c->n) return fail(c, PTK_ERR_ARG, "bad arguments");
+  *npts = (int)c->h_pat[grain].size();
+  return PTK_OK;
+}
+
+int ptk_load_frame(ptk_ctx* c, int slot, const void* pix, int dimx, int dimy, int bpp, size_t pitch_bytes) {
+  if (!c || !pix || slot < 0 || slot > 1) return fail(c, PTK_ERR_ARG, "bad frame arguments");
+  if (dimx != c->cfg.dimx || dimy != c->cfg.dimy) return fail(c, PTK_ERR_ARG, "frame size differs from the context");
+  if (bpp != 1 && bpp != 2) return fail(c, PTK_ERR_ARG, "bytes_per_px must be 1 or 2");
+  if (pitch_bytes < (size_t)dimx * bpp) return fail(c, PTK_ERR_ARG, "pitch smaller than a row");
+  const int phys = slot == 0 ? c->ref_slot : c->cur_slot;
+  if (bpp == 2) {
+    CK(cudaMemcpy2DAsync(c->d_img[phys], (size_t)c->pitch * 2, pix, pitch_bytes, (size_t)dimx * 2, dimy,
+                         cudaMemcpyHostToDevice, c->stream));
+  } else {
+    if (!c->d_u8) CK(cudaMalloc(&c->d_u8, (size_t)c->pitch * dimy));
+    CK(cudaMemcpy2DAsync(c->d_u8, (size_t)c->pitch, pix, pitch_bytes, (size_t)dimx, dimy, cudaMemcpyHostToDevice,
+                         c->stream));
+    launch_widen_u8(c->d_u8, (size_t)c->pitch, c->d_img[phys], c->pitch, dimx, dimy, c->stream);
+    c->launches += 1;
+  }
+  c->loaded[slot] = true;
+  if (slot == 0) c->need_precompute = true;
+  return PTK_OK;
+}
+
+int ptk_load_frame_device(ptk_ctx* c, int slot, const void* dev_pix, size_t pitch_bytes) {
+  if (!c || !dev_pix || slot < 0 || slot > 1) return fail(c, PTK_ERR_ARG, "bad frame arguments");
+  if (pitch_bytes < (size_t)c->cfg.dimx * 2) return fail(c, PTK_ERR_ARG, "pitch smaller than a row");
+  const int phys = slot == 0 ? c->ref_slot : c->cur_slot;
+  CK(cudaMemcpy2DAsync(c->d_img[phys], (size_t)c->pitch * 2, dev_pix, pitch_bytes, (size_t)c->cfg.dimx * 2,
+                       c->cfg.dimy, cudaMemcpyDeviceToDevice, c->stream));
+  c->loaded[slot] = true;
+  if (slot == 0) c->need_precompute = true;
+  return PTK_OK;
+}
+
+int ptk_read_frame(ptk_ctx* c, int slot, uint16_t* out) {
+  if (!c || !out || slot < 0 || slot > 1) return fail(c, PTK_ERR_ARG, "bad arguments");
+  const int phys = slot == 0 ? c->ref_slot : c->cur_slot;
+  CK(cudaMemcpy2DAsync(out, (size_t)c->cfg.dimx * 2, c->d_img[phys], (size_t)c->pitch * 2, (size_t)c->cfg.dimx * 2,
+                       c->cfg.dimy, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PTK_OK;
+}
+
+int ptk_precompute(ptk_ctx* c) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  int rc = check_ready(c, false);
+  if (rc) return rc;
+  if (!c->loaded[0]) return fail(c, PTK_ERR_STATE, "reference frame not loaded");
+  rc = enqueue_precompute(c, c->stream);
+  if (rc) return rc;
+  c->need_precompute = false;
+  CK(cudaGetLastError());
+  return PTK_OK;
+}
+
+int ptk_search(ptk_ctx* c, int level) {
+  if (!c || level < 0 || level > 2) return fail(c, PTK_ERR_ARG, "bad search level");
+  int rc = check_ready(c, true);
+  if (rc) return rc;
+  if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
+  SearchGeom sg;
+  if ((rc = search_geometry(c, level, &sg))) return rc;
+  if ((rc = ensure_best(c, sg.items))) return rc;
+  if ((rc = enqueue_search(c, level, c->stream))) return rc;
+  CK(cudaGetLastError());
+  return PTK_OK;
+}
+
+int ptk_subpixel(ptk_ctx* c, int method) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  int rc = check_ready(c, true);
+  if (rc) return rc;
+  if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
+  if ((rc = enqueue_subpixel(c, method, c->stream))) return rc;
+  CK(cudaGetLastError());
+  return PTK_OK;
+}
+
+int ptk_end_frame(ptk_ctx* c, int num_image) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  if (c->n <= 0) return fail(c, PTK_ERR_STATE, "no grains set");
+  const bool swap = num_image - c->iref >= c->cfg.iraz;
+  launch_end_frame(c->g, swap ? 1 : 0, c->stream);
+  c->launches += 1;
+  CK(cudaGetLastError());
+  if (swap) {
+    std::swap(c->ref_slot, c->cur_slot);
+    c->iref = num_image;
+    c->need_precompute = true;
+  }
+  return PTK_OK;
+}
+
+int ptk_swap_reference(ptk_ctx* c, int num_image) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  const int saved = c->cfg.iraz;
+  c->cfg.iraz = INT32_MIN / 2;
+  int rc = ptk_end_frame(c, num_image);
+  c->cfg.iraz = saved;
+  return rc;
+}
+
+int ptk_set_iref(ptk_ctx* c, int iref) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  c->iref = iref;
+  return PTK_OK;
+}
+
+int ptk_track_frame(ptk_ctx* c, int num_image) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  int rc = check_ready(c, true);
+  if (rc) return rc;
+  if ((rc = prepare_searches(c))) return rc;
+  if (c->graph_dirty) drop_graphs(c);
+  const bool pre = c->need_precompute;
+  const bool swap = num_image - c->iref >= c->cfg.iraz;
+  const int key = (c->ref_slot ? 4 : 0) | (pre ? 2 : 0) | (swap ? 1 : 0);
+  if (!c->graph[key]) {
+    // all attribute and occupancy queries happen before capture
+    for (int l = 0; l <= c->cfg.rescue_level && l < 3; ++l) {
+      SearchGeom sg;
+      if ((rc = search_geometry(c, l, &sg))) return rc;
+    }
+    const int64_t before = c->launches;
+    CK(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeRelaxed));
+    rc = enqueue_frame(c, pre, swap, c->cap_stream);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->cap_stream, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&c->graph[key], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+    c->launches = before;  // counted again at each replay below
+  }
+  CK(cudaGraphLaunch(c->graph[key], c->stream));
+  // launches of one frame: precompute, stage_begin, (search, finalize) per level,
+  // subpixel, end_frame
+  int64_t nk = (pre ? 1 : 0) + 1;
+  for (int l = 0; l <= c->cfg.rescue_level && l < 3; ++l) nk += (l == 0 ? 3 : 2);
+  if (c->cfg.subpixel) nk += 1;
+  c->launches += nk;
+  if (swap) {
+    std::swap(c->ref_slot, c->cur_slot);
+    c->iref = num_image;
+    c->need_precompute = true;
+  } else {
+    c->need_precompute = false;
+  }
+  return PTK_OK;
+}
+
+int ptk_get_rescue_counts(ptk_ctx* c, int* n_rescued, int* n_super) {
+  if (!c || !n_rescued || !n_super) return fail(c, PTK_ERR_ARG, "null argument");
+  int h[3];
+  CK(cudaMemcpyAsync(h, c->d_counts, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *n_rescued = h[1];
+  *n_super = h[2];
+  return PTK_OK;
+}
+
+static int objective_common(ptk_ctx* c, const double* X3n, double* f, double* g3n) {
+  if (!c || !X3n || !f) return fail(c, PTK_ERR_ARG, "null argument");
+  int rc = check_ready(c, true);
+  if (rc) return rc;
+  if (g3n && c->cfg.image_interpolator != PTK_INTERP_CUBIC)
+    return fail(c, PTK_ERR_ARG, "the gradient is implemented for the cubic interpolator");
+  if (g3n && (size_t)c->max_P * 24 > 227 * 1024) return fail(c, PTK_ERR_LIMIT, "pattern too large for ptk_grad");
+  if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
+  const size_t n = (size_t)c->n;
+  if (!c->d_X) {
+    CK(cudaMalloc(&c->d_X, sizeof(double) * 3 * n));
+    CK(cudaMalloc(&c->d_f, sizeof(double) * n));
+    CK(cudaMalloc(&c->d_gr, sizeof(double) * 3 * n));
+  }
+  CK(cudaMemcpyAsync(c->d_X, X3n, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+  launch_objective(c->g, frame(c, c->cur_slot), subpix_params(c), c->d_X, c->d_f, g3n ? c->d_gr : nullptr, c->max_P,
+                   c->stream);
+  c->launches += 1;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(f, c->d_f, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  if (g3n) CK(cudaMemcpyAsync(g3n, c->d_gr, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PTK_OK;
+}
+
+int ptk_objective(ptk_ctx* c, const double* X3n, double* f) { return objective_common(c, X3n, f, nullptr); }
+
+int ptk_grad(ptk_ctx* c, const double* X3n, double* f, double* g3n) {
+  if (!g3n) return fail(c, PTK_ERR_ARG, "null gradient");
+  return objective_common(c, X3n, f, g3n);
+}
+
+int ptk_set_distortion(ptk_ctx* c, const double* p14) {
+  if (!c || !p14) return fail(c, PTK_ERR_ARG, "null argument");
+  std::memcpy(c->disto, p14, sizeof(c->disto));
+  c->have_disto = true;
+  c->map_valid = false;
+  return PTK_OK;
+}
+
+int ptk_remap_frame(ptk_ctx* c, int slot) {
+  if (!c || slot < 0 || slot > 1) return fail(c, PTK_ERR_ARG, "bad arguments");
+  if (!c->have_disto) return fail(c, PTK_ERR_STATE, "no distortion parameters set");
+  if (!c->loaded[slot]) return fail(c, PTK_ERR_STATE, "frame not loaded");
+  const int dimx = c->cfg.dimx, dimy = c->cfg.dimy;
+  if (!c->d_map) CK(cudaMalloc(&c->d_map, sizeof(double2) * (size_t)dimx * dimy));
+  if (!c->d_tmp) CK(cudaMalloc(&c->d_tmp, (size_t)c->pitch * dimy * 2));
+  if (!c->map_valid) {
+    const double trig[4] = {std::cos(c->disto[10]), -std::sin(c->disto[10]), -std::sin(c->disto[12]),
+                            std::cos(c->disto[12])};
+    launch_remap_build(c->disto, trig, c->d_map, dimx, dimy, c->stream);
+    c->launches += 1;
+    c->map_valid = true;
+  }
+  const int phys = slot == 0 ? c->ref_slot : c->cur_slot;
+  launch_remap_apply(c->d_map, c->d_img[phys], c->d_tmp, c->pitch, dimx, dimy, c->stream);
+  c->launches += 1;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->d_img[phys], c->d_tmp, (size_t)c->pitch * dimy * 2, cudaMemcpyDeviceToDevice, c->stream));
+  if (slot == 0) c->need_precompute = true;
+  return PTK_OK;
+}
+
+int ptk_set_stream(ptk_ctx* c, void* s) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  CK(cudaStreamSynchronize(c->stream));
+  c->stream = s ? static_cast<cudaStream_t>(s) : c->own_stream;
+  return PTK_OK;
+}
+
+void* ptk_get_stream(ptk_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int ptk_synchronize(ptk_ctx* c) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  CK(cudaStreamSynchronize(c->stream));
+  return PTK_OK;
+}
+
+int64_t ptk_kernel_launches(ptk_ctx* c) { return c ? c->launches : 0; }
+
+int ptk_abi_sizes(size_t* config_bytes, size_t* grain_bytes, size_t* zone_bytes) {
+  if (!config_bytes || !grain_bytes || !zone_bytes) return fail(nullptr, PTK_ERR_ARG, "null argument");
+  *config_bytes = sizeof(ptk_config);
+  *grain_bytes = sizeof(ptk_grain);
+  *zone_bytes = sizeof(ptk_zone);
+  return PTK_OK;
+}
+
+const char* ptk_last_error(ptk_ctx* c) { return c ? c->err.c_str() : g_static_error.c_str(); }
+
+}  // extern "C"

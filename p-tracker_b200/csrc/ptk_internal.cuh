@@ -1,0 +1,124 @@
+// Internal declarations shared by the kernels and the host runtime of the
+// sm_100a tracking path.  Not part of the public ABI (include/ptk.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/ptk.h"
+
+namespace ptk {
+
+// Largest pattern (points per grain) the search and subpixel kernels stage in
+// shared memory.  A disc of radius 50 has 7845 points.
+constexpr int kMaxPatternPoints = 16384;
+// Candidate tile of one search work item: 32 x-offsets (one per lane) by up
+// to 32 y-offsets (8 warps x 4 rows).
+constexpr int kTileU = 32;
+constexpr int kTileV = 32;
+constexpr int kSearchThreads = 256;
+constexpr int kSubpixThreads = 128;
+
+// Device view of the grain state, structure of arrays (one entry per grain).
+struct GrainsDev {
+  int n;
+  int* refx;
+  int* refy;
+  double* refrot;
+  double* radius;
+  double* dx;
+  double* dy;
+  double* drot;
+  double* dx_prev;
+  double* dy_prev;
+  double* drot_prev;
+  double* upix;
+  double* vpix;
+  double* rot_inc;
+  double* ncc;
+  double* ncc_rescue;
+  double* ncc_subpix;
+  double* mean0;     // mean of the reference pattern pixels
+  double* c0c0;      // sum of squared deviations of the reference pattern pixels
+  long long* s0;     // exact sum of reference pattern pixels
+  long long* s00;    // exact sum of their squares
+  uint8_t* masked;
+  uint8_t* status;   // PTK_ST_* bits
+  int* flags;        // per-stage scratch flag (bit 0: footprint out of frame)
+  const int* pstart; // CSR offsets into the pattern arrays, n + 1 entries
+  const short2* pat; // pattern offsets (grain_type_2D::pattern)
+  short2* pat0;      // pattern rotated by refrot and rounded (pattern0_rotated)
+  uint16_t* w0;      // reference pixel at each pattern0_rotated point
+};
+
+struct FrameDev {
+  const uint16_t* pix;  // row-major, `pitch` elements per row
+  int pitch;
+  int dimx, dimy;
+};
+
+// Best candidate of one search work item: NCC value and its position in the
+// reference's iteration order (rotation-major, then x, then y).
+struct SearchBest {
+  double ncc;
+  int idx;
+  int pad;
+};
+
+struct SearchLaunch {
+  GrainsDev g;
+  FrameDev cur;
+  const int* list;        // grains to search (ordered by decreasing cost for level 0)
+  const int* list_count;  // number of entries in `list` (device)
+  int* work_next;         // work-queue head (zeroed before launch)
+  const double* steps;    // rotation steps of the zone
+  int nrot;
+  int left, right, up, down;
+  int tiles_u, tiles_v;
+  SearchBest* best;       // [list entry][rotation][tile]
+  int max_items;          // capacity of `best` in work items
+};
+
+struct FinalizeLaunch {
+  GrainsDev g;
+  const int* list;
+  const int* list_count;
+  const double* steps;
+  int nrot, left, up;
+  int nu, nv;  // zone width (left + right + 1) and height (up + down + 1)
+  int tiles;   // tiles_u * tiles_v
+  const SearchBest* best;
+  int level;
+  double NCC_min, NCC_min_super;
+  int* out_list;   // next-level list (rescue / super-rescue)
+  int* out_count;
+};
+
+struct SubpixParams {
+  double tol;
+  double init_dir[3];
+  double disp_max;
+  double stiffness;
+  int interp;
+};
+
+// ---- host-side launchers (defined in the kernel files) ------------------
+void launch_precompute(const GrainsDev& g, const FrameDev& ref, cudaStream_t s);
+void launch_stage_begin(const GrainsDev& g, int* counts, cudaStream_t s);
+void launch_search(const SearchLaunch& p, int grid, size_t smem, cudaStream_t s);
+size_t search_smem_bytes(int max_points, int max_patch_elems);
+int search_occupancy(size_t smem);
+void launch_finalize(const FinalizeLaunch& p, int n_grains, cudaStream_t s);
+void launch_end_frame(const GrainsDev& g, int swap_reference, cudaStream_t s);
+void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& ref,
+                          const SubpixParams& sp, int max_points, cudaStream_t s);
+void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const double* X,
+                      double* f, double* grad, int max_points, cudaStream_t s);
+void launch_widen_u8(const uint8_t* src, size_t src_pitch, uint16_t* dst, int dst_pitch, int dimx, int dimy,
+                     cudaStream_t s);
+void launch_remap_build(const double* params14, const double* trig4, double2* map, int dimx, int dimy,
+                        cudaStream_t s);
+void launch_remap_apply(const double2* map, const uint16_t* src, uint16_t* dst, int pitch, int dimx, int dimy,
+                        cudaStream_t s);
+
+}  // namespace ptk
