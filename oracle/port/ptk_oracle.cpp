@@ -156,11 +156,14 @@ SearchResult search(const Tracker& t, const Grain& g, const Zone& z) {
           r.best_v = v;
           r.best_drot = drot;
         }
-        // diagnostic top-two (not part of the reference)
+        // diagnostic (not part of the reference): the best NCC and the best
+        // value distinct from it.  Bit-identical values (identical rotated
+        // patterns at neighbouring rotation steps) are resolved by iteration
+        // order in every implementation and are not near-ties.
         if (ncc > r.top1) {
           r.top2 = r.top1;
           r.top1 = ncc;
-        } else if (ncc > r.top2) {
+        } else if (ncc < r.top1 && ncc > r.top2) {
           r.top2 = ncc;
         }
       }

@@ -126,6 +126,7 @@ class Powell {
     std::vector<double> pstart = p, ptt(n), xit(n), trial(n);
     fret = func(p);
     nfev = 1;
+    if (!std::isfinite(fret)) return p;  // flat window: NCC undefined, nothing to minimise
     for (iter = 0; iter < kPowellMaxIter; ++iter) {
       const double fp = fret;
       size_t ibig = 0;

@@ -804,6 +804,7 @@ int ptk_track_frame(ptk_ctx* c, int num_image) {
       SearchGeom sg;
       if ((rc = search_geometry(c, l, &sg))) return rc;
     }
+    prepare_subpix(c->max_P);
     const int64_t before = c->launches;
     CK(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeRelaxed));
     rc = enqueue_frame(c, pre, swap, c->cap_stream);

@@ -110,6 +110,7 @@ size_t search_smem_bytes(int max_points, int max_patch_elems);
 int search_occupancy(size_t smem);
 void launch_finalize(const FinalizeLaunch& p, int n_grains, cudaStream_t s);
 void launch_end_frame(const GrainsDev& g, int swap_reference, cudaStream_t s);
+void prepare_subpix(int max_points);
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& ref,
                           const SubpixParams& sp, int max_points, cudaStream_t s);
 void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const double* X,

@@ -422,19 +422,21 @@ void launch_stage_begin(const GrainsDev& g, int* counts, cudaStream_t s) {
   k_stage_begin<<<(n + 255) / 256, 256, 0, s>>>(g, counts);
 }
 
-void launch_search(const SearchLaunch& p, int grid, size_t smem, cudaStream_t s) {
-  static bool attr_set = false;
+static void search_attr(size_t smem) {
   static size_t attr_bytes = 0;
-  if (!attr_set || smem > attr_bytes) {
+  if (smem > attr_bytes) {
     cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_set = true;
     attr_bytes = smem;
   }
+}
+
+void launch_search(const SearchLaunch& p, int grid, size_t smem, cudaStream_t s) {
+  search_attr(smem);
   k_search<<<grid, kSearchThreads, smem, s>>>(p);
 }
 
 int search_occupancy(size_t smem) {
-  cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  search_attr(smem);
   int blocks = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_search, kSearchThreads, smem);
   return blocks;

@@ -395,6 +395,10 @@ __device__ void powell_minimize(F& f, double p[3], const double step[3], double 
   double dirs[3][3] = {{step[0], 0.0, 0.0}, {0.0, step[1], 0.0}, {0.0, 0.0, step[2]}};
   double pstart[3] = {p[0], p[1], p[2]};
   double fret = f(p);
+  if (!isfinite(fret)) {  // flat window: NCC undefined, nothing to minimise
+    *fret_out = fret;
+    return;
+  }
   for (int iter = 0; iter < kPowellMaxIter; ++iter) {
     const double fp = fret;
     int ibig = 0;
@@ -510,19 +514,33 @@ __global__ void __launch_bounds__(kSubpixThreads) k_objective(GrainsDev g, Frame
   if (threadIdx.x == 0) f[gi] = val;
 }
 
+void prepare_subpix(int max_points) {
+  static size_t powell_bytes = 0, objective_bytes = 0;
+  const size_t a = (size_t)max_points * sizeof(double);
+  if (a > powell_bytes) {
+    cudaFuncSetAttribute(k_subpix_powell, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a);
+    powell_bytes = a;
+  }
+  const size_t b = (size_t)max_points * sizeof(double) * 3;
+  if (b > objective_bytes && b <= 227 * 1024) {
+    cudaFuncSetAttribute(k_objective, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+    objective_bytes = b;
+  }
+}
+
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& /*ref*/, const SubpixParams& sp,
                           int max_points, cudaStream_t s) {
   if (g.n <= 0) return;
+  prepare_subpix(max_points);
   const size_t smem = (size_t)max_points * sizeof(double);
-  cudaFuncSetAttribute(k_subpix_powell, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_subpix_powell<<<g.n, kSubpixThreads, smem, s>>>(g, cur, sp);
 }
 
 void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const double* X, double* f,
                       double* grad, int max_points, cudaStream_t s) {
   if (g.n <= 0) return;
+  prepare_subpix(max_points);
   const size_t smem = (size_t)max_points * sizeof(double) * (grad ? 3 : 1);
-  cudaFuncSetAttribute(k_objective, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_objective<<<g.n, kSubpixThreads, smem, s>>>(g, cur, sp, X, f, grad);
 }
 
