@@ -118,6 +118,12 @@ int ptk_set_search_zone(ptk_ctx* ctx, int level, const ptk_zone* zone);
  * (src/p-tracker.cpp:1213-1278) and the dic_out write (src/p-tracker.cpp:1313-1360). */
 int ptk_set_grains(ptk_ctx* ctx, const ptk_grain* grains, int n);
 int ptk_get_grains(ptk_ctx* ctx, ptk_grain* out, int n);
+/* Device-side copy of the whole grain state and its restoration (stream
+ * ordered, no host transfer).  The per-frame dic_out files are the
+ * reference's checkpoint (src/p-tracker.cpp:584, restart_file :1515-1518);
+ * these keep one in device memory, e.g. to re-track a frame pair. */
+int ptk_snapshot_grains(ptk_ctx* ctx);
+int ptk_restore_grains(ptk_ctx* ctx);
 
 /* Patterns as CSR: grain g owns offsets_xy[2*starts[g] .. 2*starts[g+1]).
  * Replaces make_custom_pattern (src/p-tracker.cpp:1444-1476). */

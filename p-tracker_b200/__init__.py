@@ -67,6 +67,8 @@ _SIGS = {
     "ptk_set_search_zone": (C.c_int, [_P, C.c_int, C.POINTER(Zone)]),
     "ptk_set_grains": (C.c_int, [_P, _P, C.c_int]),
     "ptk_get_grains": (C.c_int, [_P, _P, C.c_int]),
+    "ptk_snapshot_grains": (C.c_int, [_P]),
+    "ptk_restore_grains": (C.c_int, [_P]),
     "ptk_set_patterns": (C.c_int, [_P, _P, _P, C.c_int]),
     "ptk_make_patterns": (C.c_int, [_P, C.c_int, C.c_double, C.c_double, C.c_double]),
     "ptk_pattern_size": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
@@ -247,6 +249,12 @@ class Tracker:
 
     def get_grains(self) -> np.ndarray:
         return structs_to_records(self.get_grains_structs())
+
+    def snapshot_grains(self):
+        self._check(self._L.ptk_snapshot_grains(self.h), self.h)
+
+    def restore_grains(self):
+        self._check(self._L.ptk_restore_grains(self.h), self.h)
 
     def status(self) -> np.ndarray:
         return self.get_grains_structs()["status"].copy()

@@ -64,6 +64,9 @@ struct ptk_ctx {
   // grains
   int n{0};
   void* d_block{nullptr};
+  void* d_snap{nullptr};     // device copy of the grain block (ptk_snapshot_grains)
+  void* h_stage{nullptr};    // pinned staging for grain upload / download
+  size_t h_stage_bytes{0};
   GrainsDev g{};
   std::vector<double> h_radius;
 
@@ -272,6 +275,16 @@ int upload_patterns(ptk_ctx* c) {
   bind_grains(c);
   c->need_precompute = true;
   invalidate(c);
+  return PTK_OK;
+}
+
+int ensure_stage(ptk_ctx* c, size_t bytes) {
+  if (bytes <= c->h_stage_bytes) return PTK_OK;
+  if (c->h_stage) cudaFreeHost(c->h_stage);
+  c->h_stage = nullptr;
+  c->h_stage_bytes = 0;
+  CK(cudaHostAlloc(&c->h_stage, bytes, cudaHostAllocDefault));
+  c->h_stage_bytes = bytes;
   return PTK_OK;
 }
 
@@ -487,6 +500,8 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_tmp);
   cudaFree(c->d_u8);
   cudaFree(c->d_block);
+  cudaFree(c->d_snap);
+  if (c->h_stage) cudaFreeHost(c->h_stage);
   cudaFree(c->d_pstart);
   cudaFree(c->d_pat);
   cudaFree(c->d_pat0);
@@ -535,8 +550,10 @@ int ptk_set_grains(ptk_ctx* c, const ptk_grain* grains, int n) {
   CK(cudaStreamSynchronize(c->stream));
   if (n != c->n) {
     cudaFree(c->d_block);
+    cudaFree(c->d_snap);
     cudaFree(c->d_lists);
     c->d_block = nullptr;
+    c->d_snap = nullptr;
     c->d_lists = nullptr;
     c->n = n;
     BlockLayout L(n);
@@ -549,11 +566,14 @@ int ptk_set_grains(ptk_ctx* c, const ptk_grain* grains, int n) {
     c->best_cap = 0;
   }
   BlockLayout L(n);
-  std::vector<char> h(L.total, 0);
+  int rc = ensure_stage(c, L.total);
+  if (rc) return rc;
+  char* h = static_cast<char*>(c->h_stage);
+  std::memset(h, 0, L.total);
   const size_t nn = (size_t)(n > 0 ? n : 1);
-  auto D = [&](int k) { return reinterpret_cast<double*>(h.data() + L.d_off + k * nn * 8); };
-  auto I = [&](int k) { return reinterpret_cast<int*>(h.data() + L.i_off + k * nn * 4); };
-  auto B = [&](int k) { return reinterpret_cast<uint8_t*>(h.data() + L.b_off + k * nn); };
+  auto D = [&](int k) { return reinterpret_cast<double*>(h + L.d_off + k * nn * 8); };
+  auto I = [&](int k) { return reinterpret_cast<int*>(h + L.i_off + k * nn * 4); };
+  auto B = [&](int k) { return reinterpret_cast<uint8_t*>(h + L.b_off + k * nn); };
   c->h_radius.resize(n);
   for (int i = 0; i < n; ++i) {
     const ptk_grain& s = grains[i];
@@ -576,7 +596,8 @@ int ptk_set_grains(ptk_ctx* c, const ptk_grain* grains, int n) {
     B(B_MASKED)[i] = s.masked ? 1 : 0;
     c->h_radius[i] = s.radius_pix;
   }
-  if (n) CK(cudaMemcpy(c->d_block, h.data(), L.total, cudaMemcpyHostToDevice));
+  // the next call that touches the staging buffer synchronises the stream first
+  if (n) CK(cudaMemcpyAsync(c->d_block, h, L.total, cudaMemcpyHostToDevice, c->stream));
   bind_grains(c);
   c->need_precompute = true;
   invalidate(c);
@@ -588,13 +609,16 @@ int ptk_get_grains(ptk_ctx* c, ptk_grain* out, int n) {
   if (n != c->n) return fail(c, PTK_ERR_ARG, "grain count mismatch");
   if (n == 0) return PTK_OK;
   BlockLayout L(n);
-  std::vector<char> h(L.total);
-  CK(cudaMemcpyAsync(h.data(), c->d_block, L.total, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int rc = ensure_stage(c, L.total);
+  if (rc) return rc;
+  const char* h = static_cast<const char*>(c->h_stage);
+  CK(cudaMemcpyAsync(c->h_stage, c->d_block, L.total, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   const size_t nn = (size_t)n;
-  auto D = [&](int k) { return reinterpret_cast<const double*>(h.data() + L.d_off + k * nn * 8); };
-  auto I = [&](int k) { return reinterpret_cast<const int*>(h.data() + L.i_off + k * nn * 4); };
-  auto B = [&](int k) { return reinterpret_cast<const uint8_t*>(h.data() + L.b_off + k * nn); };
+  auto D = [&](int k) { return reinterpret_cast<const double*>(h + L.d_off + k * nn * 8); };
+  auto I = [&](int k) { return reinterpret_cast<const int*>(h + L.i_off + k * nn * 4); };
+  auto B = [&](int k) { return reinterpret_cast<const uint8_t*>(h + L.b_off + k * nn); };
   for (int i = 0; i < n; ++i) {
     ptk_grain& s = out[i];
     std::memset(&s, 0, sizeof(s));
@@ -614,6 +638,24 @@ int ptk_get_grains(ptk_ctx* c, ptk_grain* out, int n) {
     s.masked = B(B_MASKED)[i];
     s.status = B(B_STATUS)[i];
   }
+  return PTK_OK;
+}
+
+int ptk_snapshot_grains(ptk_ctx* c) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  if (c->n <= 0) return fail(c, PTK_ERR_STATE, "no grains set");
+  BlockLayout L(c->n);
+  if (!c->d_snap) CK(cudaMalloc(&c->d_snap, L.total));
+  CK(cudaMemcpyAsync(c->d_snap, c->d_block, L.total, cudaMemcpyDeviceToDevice, c->stream));
+  return PTK_OK;
+}
+
+int ptk_restore_grains(ptk_ctx* c) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  if (!c->d_snap) return fail(c, PTK_ERR_STATE, "no grain snapshot");
+  BlockLayout L(c->n);
+  CK(cudaMemcpyAsync(c->d_block, c->d_snap, L.total, cudaMemcpyDeviceToDevice, c->stream));
+  c->need_precompute = true;
   return PTK_OK;
 }
 
