@@ -196,6 +196,34 @@ int ptk_synchronize(ptk_ctx* ctx);
 /* Number of device kernels this context launched since creation. */
 int64_t ptk_kernel_launches(ptk_ctx* ctx);
 
+/* Pixel-stage search that allocates nothing (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc -- a plug-in whose host application
+ * owns all device memory, or a loop where an allocation and the device
+ * synchronisation it may imply are not allowed.  Computes, for every grain,
+ * what ptk_search(level 0) computes before its acceptance rule: the first
+ * strict NCC maximum above 0 over the zone's rotation steps and offsets.
+ * All pointers are device pointers the caller owns (frames: uint16 rows of
+ * pitch_bytes; pattern_starts: n_grains + 1 CSR offsets into pattern_xy,
+ * int16 x,y pairs); `zone` is a host struct; rotations == 0 searches the
+ * single step -0.0 as the reference's `rotations 0`.  max_points must bound
+ * every pattern's size (<= 16384) and max_radius every |offset| after
+ * rotation by refrot.  Outputs: best NCC, best x/y offset and rotation step
+ * per grain (0, 0, 0, 0.0 when no NCC exceeds 0); a grain whose pattern
+ * exceeds max_points/max_radius, or whose footprint leaves the frame, gets
+ * NaN and an INT_MIN-based offset.  Scratch lives in one fixed 4 MiB device
+ * array per GPU, kept for the life of the process: n_grains x rotation steps
+ * x ceil(nu/32) x ceil(nv/32) must not exceed 260,080 (PTK_ERR_LIMIT
+ * otherwise), with at most 4096 rotation steps.  Calls share that array, so
+ * calls that overlap on the GPU race.  The first call on a device looks up
+ * the array's device address; make it before any stream capture.
+ * Work is enqueued on `stream` (NULL = legacy default stream). */
+int ptk_search_pixel_noalloc(const uint16_t* ref_pix, const uint16_t* cur_pix, size_t pitch_bytes, int dimx,
+                             int dimy, int n_grains, const int32_t* refx, const int32_t* refy, const double* refrot,
+                             const double* drot, const double* dx, const double* dy, const int32_t* pattern_starts,
+                             const int16_t* pattern_xy, int max_points, int max_radius, const ptk_zone* zone,
+                             int rotations, double* best_ncc, int32_t* best_u, int32_t* best_v, double* best_drot,
+                             void* stream);
+
 /* sizeof of the ABI structs as compiled into the library, for FFI binders. */
 int ptk_abi_sizes(size_t* config_bytes, size_t* grain_bytes, size_t* zone_bytes);
 

@@ -92,6 +92,8 @@ _SIGS = {
     "ptk_synchronize": (C.c_int, [_P]),
     "ptk_kernel_launches": (C.c_int64, [_P]),
     "ptk_abi_sizes": (C.c_int, [C.POINTER(C.c_size_t)] * 3),
+    "ptk_search_pixel_noalloc": (C.c_int, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int] + [_P] * 8 +
+                                 [C.c_int, C.c_int, C.POINTER(Zone), C.c_int] + [_P] * 5),
     "ptk_last_error": (C.c_char_p, [_P]),
     "ptk_read_grains_file": (C.c_int, [C.c_char_p, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
     "ptk_save_grains_file": (C.c_int, [C.c_char_p, _P, C.c_int, C.c_char_p, C.c_char_p, C.c_char_p,

@@ -1,0 +1,114 @@
+"""The allocation-free pixel search (ptk_search_pixel_noalloc) against the
+context path (ptk_search level 0).
+
+Some callers cannot call cudaMalloc (a plug-in whose host application owns
+all device memory, or a loop that must not allocate), so this entry point
+works only on buffers the caller passes in and keeps its scratch in one fixed
+device array.  This test owns every device buffer (allocated through torch),
+calls the entry point through the C ABI twice in a row -- the second call
+finds the first call's leftovers in the shared scratch -- and checks both
+results against the context path: same offsets and rotation step, NCC within
+the tolerance of the other parity tests.  It lives in its own file, collected
+last, and passes alone in a fresh process as well as after the other tests."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NCC_TOL = 1e-5
+
+
+def _context_search(ptk, pair, zone):
+    p = pair["params"]
+    t = ptk.Tracker(p["dimx"], p["dimy"], rescue_level=0, NCC_min=-1.0)  # accept every grain's best
+    t.set_zone(0, *zone)
+    t.set_grains(pair["rec"])
+    t.make_patterns("grain_diameter", 1.0, 1.0)
+    t.load_frame(0, pair["ref"])
+    t.load_frame(1, pair["cur"])
+    t.precompute()
+    t.search(0)
+    out = t.get_grains()
+    t.close()
+    return out
+
+
+def _patterns(rec):
+    """grain_diameter 1.0 1.0 (src/p-tracker.cpp:1656-1666) as CSR int16 pairs."""
+    pts, starts = [], [0]
+    for r in rec[:, 3]:
+        rad = max(int(r * 1.0), 1)
+        yy, xx = np.mgrid[-rad:rad + 1, -rad:rad + 1]
+        keep = np.sqrt(xx.astype(float) ** 2 + yy.astype(float) ** 2) <= rad
+        xy = np.stack([xx[keep], yy[keep]], 1)
+        pts.append(xy)
+        starts.append(starts[-1] + xy.shape[0])
+    return np.concatenate(pts).astype(np.int16), np.array(starts, np.int32), max(x.shape[0] for x in pts), \
+        int(np.abs(np.concatenate(pts)).max())
+
+
+def test_noalloc_matches_context_path(ptk, wl, cuda_device, pair_cache):
+    import torch
+
+    pair = pair_cache("small16", 7)
+    z = wl.tracker_options(pair["params"])["zones"][0]
+    ctx_rec = _context_search(ptk, pair, z)
+    rec = pair["rec"]
+    n = rec.shape[0]
+    dev = torch.device("cuda", 0)
+    ref = torch.from_numpy(np.ascontiguousarray(pair["ref"]).view(np.int16)).to(dev)
+    cur = torch.from_numpy(np.ascontiguousarray(pair["cur"]).view(np.int16)).to(dev)
+    refx = torch.tensor(rec[:, 0].astype(np.int32), device=dev)
+    refy = torch.tensor(rec[:, 1].astype(np.int32), device=dev)
+    refrot = torch.tensor(rec[:, 2], dtype=torch.float64, device=dev)
+    drot = torch.tensor(rec[:, 6], dtype=torch.float64, device=dev)
+    dx = torch.tensor(rec[:, 4], dtype=torch.float64, device=dev)
+    dy = torch.tensor(rec[:, 5], dtype=torch.float64, device=dev)
+    xy, starts, maxp, maxr = _patterns(rec)
+    pxy = torch.from_numpy(xy).to(dev)
+    pst = torch.from_numpy(starts).to(dev)
+    L = ptk.lib()
+    zone = ptk.Zone(*z)
+    stream = torch.cuda.current_stream().cuda_stream
+    # the context path adds the offset to round(dx) (half away from zero; dx >= 0 here)
+    gdx = np.floor(rec[:, 4] + 0.5)
+    gdy = np.floor(rec[:, 5] + 0.5)
+    expect_u = (ctx_rec[:, 4] - gdx).round().astype(np.int64)
+    expect_v = (ctx_rec[:, 5] - gdy).round().astype(np.int64)
+    expect_rot = ctx_rec[:, 6] - rec[:, 6]
+    for call in range(2):
+        ncc = torch.full((n,), -7.0, dtype=torch.float64, device=dev)
+        bu = torch.full((n,), 12345, dtype=torch.int32, device=dev)
+        bv = torch.full((n,), 12345, dtype=torch.int32, device=dev)
+        br = torch.full((n,), 9.0, dtype=torch.float64, device=dev)
+        rc = L.ptk_search_pixel_noalloc(
+            C.c_void_p(ref.data_ptr()), C.c_void_p(cur.data_ptr()), ref.stride(0) * 2, pair["ref"].shape[1],
+            pair["ref"].shape[0], n, C.c_void_p(refx.data_ptr()), C.c_void_p(refy.data_ptr()),
+            C.c_void_p(refrot.data_ptr()), C.c_void_p(drot.data_ptr()), C.c_void_p(dx.data_ptr()),
+            C.c_void_p(dy.data_ptr()), C.c_void_p(pst.data_ptr()), C.c_void_p(pxy.data_ptr()), maxp, maxr,
+            C.byref(zone), 1, C.c_void_p(ncc.data_ptr()), C.c_void_p(bu.data_ptr()), C.c_void_p(bv.data_ptr()),
+            C.c_void_p(br.data_ptr()), C.c_void_p(stream))
+        assert rc == 0, f"call {call}: status {rc}"
+        torch.cuda.synchronize()
+        got_ncc, got_u, got_v, got_r = ncc.cpu().numpy(), bu.cpu().numpy(), bv.cpu().numpy(), br.cpu().numpy()
+        assert np.abs(got_ncc - ctx_rec[:, 10]).max() <= NCC_TOL, f"call {call}: NCC differs"
+        np.testing.assert_array_equal(got_u, expect_u, err_msg=f"call {call}: x offsets differ")
+        np.testing.assert_array_equal(got_v, expect_v, err_msg=f"call {call}: y offsets differ")
+        np.testing.assert_array_equal(got_r, expect_rot, err_msg=f"call {call}: rotation steps differ")
+
+
+def test_noalloc_rejects_oversized_work(ptk, cuda_device):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    buf = torch.zeros(64 * 64, dtype=torch.int16, device=dev)
+    d = torch.zeros(1 << 20, dtype=torch.float64, device=dev)
+    zone = ptk.Zone(200, 200, 200, 200, 10, 0.005)  # 21 steps x 13 x 13 tiles x grains
+    rc = ptk.lib().ptk_search_pixel_noalloc(
+        C.c_void_p(buf.data_ptr()), C.c_void_p(buf.data_ptr()), 128, 64, 64, 100000,
+        *[C.c_void_p(d.data_ptr())] * 8, 10, 5, C.byref(zone), 1, *[C.c_void_p(d.data_ptr())] * 4, None)
+    assert rc == ptk.PTK_ERR_LIMIT
