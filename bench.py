@@ -58,6 +58,26 @@ def cpu_threads() -> int:
     return max(1, min(48, n))
 
 
+def rank_seed(rank: int) -> int:
+    """Each rank tracks its own pair: grains are independent (weak scaling)."""
+    return 1000 + rank
+
+
+def reduce_max(values, world: int, device="cpu") -> list:
+    """Max over ranks of per-rank timings (the only collective of the bench)."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def aggregate_rate(units_per_rank: int, world: int, ms_per_step: float) -> float:
+    """Whole-job rate: units of all ranks over the slowest rank's step time."""
+    return units_per_rank * world / (ms_per_step * 1e-3)
+
+
 def sample_indices(n: int, k: int) -> np.ndarray:
     """Evenly spaced sample of k grains (keeps the radius mix)."""
     k = min(n, k)
@@ -215,7 +235,7 @@ def main() -> int:
     ptk = importlib.import_module("p-tracker_b200")
     wl = importlib.import_module("p-tracker_b200.workloads")
 
-    pair = wl.make_pair(args.workload, seed=1000 + rank)
+    pair = wl.make_pair(args.workload, seed=rank_seed(rank))
     p = pair["params"]
     n = pair["rec"].shape[0]
     opts = wl.tracker_options(p)
@@ -306,10 +326,7 @@ def main() -> int:
     ms_step = total_ms / args.steps
     e2e_step = statistics.mean(e2e_ms)
     s_ms = statistics.median(search_ms)
-    stats = torch.tensor([ms_step, e2e_step, s_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(stats, op=dist.ReduceOp.MAX)
-    ms_step, e2e_step, s_ms = stats.tolist()
+    ms_step, e2e_step, s_ms = reduce_max([ms_step, e2e_step, s_ms], world, device="cuda")
 
     if rank == 0:
         sys.path.insert(0, str(ROOT / "oracle"))
@@ -325,7 +342,7 @@ def main() -> int:
         nn = n
         block = 16 * 8 * nn + 2 * 8 * nn + ((12 * nn + 15) // 16) * 16 + ((2 * nn + 15) // 16) * 16
         line = {
-            "metric": METRIC, "value": n * world / (ms_step * 1e-3), "unit": UNIT, "n_gpus": world,
+            "metric": METRIC, "value": aggregate_rate(n, world, ms_step), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64+f64", "data": "synthetic",
             "config": {"workload": f"{args.workload}: {p['dimx']}x{p['dimy']} "
@@ -333,7 +350,7 @@ def main() -> int:
                                    f" {nrot} rotation steps, Powell subpixel",
                        "form": "plain (exact integer search + FP64 Powell)", "grains_per_gpu": n,
                        "l2": "flushed (256 MiB write) before each timed step", "parallelism": f"grain shards x{world}"},
-            "e2e": {"value": n * world / (e2e_step * 1e-3), "unit": UNIT,
+            "e2e": {"value": aggregate_rate(n, world, e2e_step), "unit": UNIT,
                     "h2d_bytes_per_step": int(frame_bytes + block), "d2h_bytes_per_step": int(block)},
             "gpu_launches": int(launches),
             "roofline": {"kernel": "k_search (pixel + rotation stage)", "bound": "tensor", "achieved": achieved,
