@@ -49,7 +49,10 @@ enum {
 
 enum { PTK_INTERP_LINEAR = 0, PTK_INTERP_CUBIC = 1, PTK_INTERP_QUINTIC = 2 };
 enum { PTK_SUBPIX_POWELL = 0, PTK_SUBPIX_ADJOINT_LM = 1 };
-enum { PTK_SEARCH_EXACT = 0, PTK_SEARCH_BF16 = 1 };
+/* PTK_SEARCH_EXACT picks the register-tiled exact kernel when its shared-memory
+ * layout fits, else the direct one; PTK_SEARCH_EXACT_DIRECT forces the direct
+ * per-point kernel.  Both return identical results. */
+enum { PTK_SEARCH_EXACT = 0, PTK_SEARCH_BF16 = 1, PTK_SEARCH_EXACT_DIRECT = 2 };
 enum { PTK_LEVEL_PIXEL = 0, PTK_LEVEL_RESCUE = 1, PTK_LEVEL_SUPER_RESCUE = 2 };
 enum { PTK_PATTERN_CIRC = 0, PTK_PATTERN_RING = 1, PTK_PATTERN_RECT = 2, PTK_PATTERN_GRAIN_DIAMETER = 3 };
 

@@ -79,6 +79,7 @@ struct ptk_ctx {
   int* d_order{nullptr};
   int max_P{0};
   int max_R{0};
+  int max_dup{1};  // largest repeat count of one offset within a pattern
   bool patterns_ok{false};
 
   // zones
@@ -269,6 +270,20 @@ int upload_patterns(ptk_ctx* c) {
   CK(cudaMemcpy(c->d_counts, &cnt0, sizeof(int), cudaMemcpyHostToDevice));
   c->max_P = maxP;
   c->max_R = (int)std::ceil(maxnorm) + 1;
+  int max_dup = 1;
+  for (int i = 0; i < n; ++i) {
+    std::vector<int> keys;
+    keys.reserve(c->h_pat[i].size());
+    for (const short2& q : c->h_pat[i]) keys.push_back(((int)q.y << 16) ^ ((int)q.x & 0xffff));
+    std::sort(keys.begin(), keys.end());
+    for (size_t k = 0; k < keys.size();) {
+      size_t e = k;
+      while (e < keys.size() && keys[e] == keys[k]) ++e;
+      max_dup = std::max(max_dup, (int)(e - k));
+      k = e;
+    }
+  }
+  c->max_dup = max_dup;
   c->patterns_ok = true;
   for (int i = 0; i < n; ++i)
     if (c->h_pat[i].empty()) c->patterns_ok = false;
@@ -307,6 +322,7 @@ struct SearchGeom {
   size_t smem;
   int grid;
   size_t items;
+  bool tiled;  // register-tiled exact kernel (else the direct one)
 };
 
 int search_geometry(ptk_ctx* c, int level, SearchGeom* sg) {
@@ -316,11 +332,23 @@ int search_geometry(ptk_ctx* c, int level, SearchGeom* sg) {
   sg->nv = z.up + z.down + 1;
   sg->tiles_u = (sg->nu + kTileU - 1) / kTileU;
   sg->tiles_v = (sg->nv + kTileV - 1) / kTileV;
+  sg->items = (size_t)c->n * sg->nrot * sg->tiles_u * sg->tiles_v;
+  if (sg->items > (size_t)INT32_MAX) return fail(c, PTK_ERR_LIMIT, "too many search work items");
+  // The tiled kernel decodes multiplicities from its map (at most 16 points per
+  // pixel): a rotated pattern stacks at most 4 distinct offsets on one pixel,
+  // so patterns whose offsets repeat more than 4 times use the direct kernel.
+  const size_t tsmem = search_tiled_smem(c->max_R);
+  sg->tiled = c->cfg.search_method != PTK_SEARCH_EXACT_DIRECT && c->max_dup <= 4 && c->max_R <= 112 &&
+              tsmem <= 227 * 1024;
+  if (sg->tiled) {
+    sg->smem = tsmem;
+    const int occ = search_tiled_occupancy(sg->smem, c->max_R);
+    sg->grid = c->num_sms * (occ > 0 ? occ : 1);
+    return PTK_OK;
+  }
   const int span = 2 * c->max_R + kTileU;
   sg->smem = search_smem_bytes(c->max_P, span * span);
   if (sg->smem > 227 * 1024) return fail(c, PTK_ERR_LIMIT, "pattern too large for the shared-memory search tile");
-  sg->items = (size_t)c->n * sg->nrot * sg->tiles_u * sg->tiles_v;
-  if (sg->items > (size_t)INT32_MAX) return fail(c, PTK_ERR_LIMIT, "too many search work items");
   const int occ = search_occupancy(sg->smem);
   sg->grid = c->num_sms * (occ > 0 ? occ : 1);
   return PTK_OK;
@@ -365,7 +393,8 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s) {
   p.tiles_v = sg.tiles_v;
   p.best = c->d_best;
   p.max_items = (int)c->best_cap;
-  launch_search(p, sg.grid, sg.smem, s);
+  if (sg.tiled) launch_search_tiled(p, c->max_R, sg.grid, sg.smem, s);
+  else launch_search(p, sg.grid, sg.smem, s);
   FinalizeLaunch f;
   f.g = c->g;
   f.list = list;
@@ -389,8 +418,19 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s) {
 }
 
 int enqueue_subpixel(ptk_ctx* c, int method, cudaStream_t s) {
-  if (method != PTK_SUBPIX_POWELL) return fail(c, PTK_ERR_ARG, "subpixel method not available");
-  launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, s);
+  if (method == PTK_SUBPIX_ADJOINT_LM) {
+    if (c->cfg.image_interpolator != PTK_INTERP_CUBIC)
+      return fail(c, PTK_ERR_ARG, "the adjoint LM refinement is implemented for the cubic interpolator");
+    LmParams lp;
+    lp.max_iter = c->cfg.lm_max_iter > 0 ? c->cfg.lm_max_iter : 30;
+    lp.tol = c->cfg.lm_tol > 0.0 ? c->cfg.lm_tol : 1e-6;
+    lp.iters = nullptr;
+    launch_subpix_lm(c->g, frame(c, c->cur_slot), lp, s);
+  } else if (method == PTK_SUBPIX_POWELL) {
+    launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, s);
+  } else {
+    return fail(c, PTK_ERR_ARG, "unknown subpixel method");
+  }
   c->launches += 1;
   return PTK_OK;
 }
@@ -904,8 +944,11 @@ static int objective_common(ptk_ctx* c, const double* X3n, double* f, double* g3
     CK(cudaMalloc(&c->d_gr, sizeof(double) * 3 * n));
   }
   CK(cudaMemcpyAsync(c->d_X, X3n, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
-  launch_objective(c->g, frame(c, c->cur_slot), subpix_params(c), c->d_X, c->d_f, g3n ? c->d_gr : nullptr, c->max_P,
-                   c->stream);
+  if (g3n && c->cfg.subpix_method == PTK_SUBPIX_ADJOINT_LM)
+    launch_grad_f32(c->g, frame(c, c->cur_slot), c->d_X, c->d_f, c->d_gr, c->stream);  // the LM's FP32 adjoint
+  else
+    launch_objective(c->g, frame(c, c->cur_slot), subpix_params(c), c->d_X, c->d_f, g3n ? c->d_gr : nullptr,
+                     c->max_P, c->stream);
   c->launches += 1;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(f, c->d_f, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));

@@ -102,12 +102,24 @@ struct SubpixParams {
   int interp;
 };
 
+struct LmParams {
+  int max_iter;
+  double tol;   // step tolerance in pixels (rotation scaled by the grain radius)
+  int* iters;   // optional per-grain iteration count
+};
+
 // ---- host-side launchers (defined in the kernel files) ------------------
+void launch_subpix_lm(const GrainsDev& g, const FrameDev& cur, const LmParams& lp, cudaStream_t s);
+void launch_grad_f32(const GrainsDev& g, const FrameDev& cur, const double* X, double* f, double* grad,
+                     cudaStream_t s);
 void launch_precompute(const GrainsDev& g, const FrameDev& ref, cudaStream_t s);
 void launch_stage_begin(const GrainsDev& g, int* counts, cudaStream_t s);
 void launch_search(const SearchLaunch& p, int grid, size_t smem, cudaStream_t s);
 size_t search_smem_bytes(int max_points, int max_patch_elems);
 int search_occupancy(size_t smem);
+size_t search_tiled_smem(int max_r);
+int search_tiled_occupancy(size_t smem, int max_r);
+void launch_search_tiled(const SearchLaunch& p, int max_r, int grid, size_t smem, cudaStream_t s);
 void launch_finalize(const FinalizeLaunch& p, int n_grains, cudaStream_t s);
 void launch_end_frame(const GrainsDev& g, int swap_reference, cudaStream_t s);
 void prepare_subpix(int max_points);

@@ -323,7 +323,7 @@ __global__ void k_finalize(FinalizeLaunch p) {
   const int gi = p.list[li];
   GrainsDev& g = p.g;
   if (g.masked[gi]) return;
-  if ((g.flags[gi] & 3) != 0) {  // footprint leaves the frame: not searched
+  if ((g.flags[gi] & 7) != 0) {  // footprint leaves the frame (or the tile layout): not searched
     g.status[gi] |= PTK_ST_OUT_OF_BOUNDS;
     return;
   }

@@ -1,0 +1,274 @@
+// Subpixel refinement by adjoint Levenberg-Marquardt (the differentiation
+// form), replacing Powell in follow_pattern_subpixel_xyR
+// (src/p-tracker.cpp:1090-1128).  No reference counterpart.
+//
+// Objective: the reference's 1 - NCC(X) (src/p-tracker.cpp:1018-1088, W = 1,
+// i.e. overflow_stiffness 0) written as a least-squares problem,
+//     F(X) = sum_i r_i^2 = 2 (1 - NCC),   r_i = a_i/|a| - b_i(X)/|b(X)|,
+// with a the centred reference values and b the centred cubic samples of the
+// current frame at the pattern points moved by X = (dx, dy, drot).  With
+// g_i = dv_i/dX (cubic derivatives chained through the rotation),
+// gbar = mean g, n = |b|, c = sum b_i g_i / n:
+//     J^T J = (sum g g^T - P gbar gbar^T - c c^T) / n^2
+//     J^T r = -(sum a_i g_i / |a| - c NCC) / n
+// so one pass over the points accumulates 21 sums.  Samples, derivatives and
+// sums are FP32 (values centred on mean0 to avoid cancellation); the 3x3
+// damped normal equations are solved in FP64 and X and the cumulative grain
+// state accumulate in FP64.
+//
+// One warp per grain (4 grains per 128-thread block), shuffle reductions only.
+#include "ptk_internal.cuh"
+
+namespace ptk {
+
+namespace {
+
+constexpr int kLmWarps = 4;
+constexpr int kNSums = 18;
+
+// exact uint16 -> float: bits of 2^23 + v, minus 2^23
+__device__ __forceinline__ float u16f(unsigned v) { return __int_as_float(0x4B000000 | v) - 8388608.0f; }
+
+// Catmull-Rom weights of the reference's CubicInterpolate (src/interpol.cpp:42-53)
+// and their derivatives.
+__device__ __forceinline__ void cr_weights(float t, float w[4], float dw[4]) {
+  const float t2 = t * t, t3 = t2 * t;
+  w[0] = -0.5f * t3 + t2 - 0.5f * t;
+  w[1] = 1.5f * t3 - 2.5f * t2 + 1.0f;
+  w[2] = -1.5f * t3 + 2.0f * t2 + 0.5f * t;
+  w[3] = 0.5f * t3 - 0.5f * t2;
+  dw[0] = -1.5f * t2 + 2.0f * t - 0.5f;
+  dw[1] = 4.5f * t2 - 5.0f * t;
+  dw[2] = -4.5f * t2 + 4.0f * t + 0.5f;
+  dw[3] = 1.5f * t2 - t;
+}
+
+struct LmGrain {
+  int b, P;
+  int ix0, iy0;       // integer part of refcoord + d
+  float fx, fy;       // fractional part
+  double drot;
+  float mean0;
+  double norm_a;      // |a| = sqrt(C0C0)
+};
+
+struct LmEval {
+  double F, ncc;
+  double H[6];  // xx, xy, xr, yy, yr, rr
+  double gv[3];
+  bool clamped;
+};
+
+// Sums over the grain's points at X (all lanes return the same values).
+__device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain& o, const double X[3], int lane) {
+  double sr, cr;
+  sincos(o.drot + X[2], &sr, &cr);
+  const float c = (float)cr, s = (float)sr;
+  const float bx = o.fx + (float)X[0], by = o.fy + (float)X[1];
+  float S[kNSums];
+#pragma unroll
+  for (int k = 0; k < kNSums; ++k) S[k] = 0.0f;
+  bool clamped = false;
+  for (int i = lane; i < o.P; i += 32) {
+    const short2 q = g.pat0[o.b + i];
+    const float x = (float)q.x, y = (float)q.y;
+    const float px = bx + c * x + s * y;
+    const float py = by - s * x + c * y;
+    const float fpx = floorf(px), fpy = floorf(py);
+    const float tx = px - fpx, ty = py - fpy;
+    int ix = o.ix0 + (int)fpx, iy = o.iy0 + (int)fpy;
+    if (ix < 1 || iy < 1 || ix + 2 >= cur.dimx || iy + 2 >= cur.dimy) {
+      clamped = true;
+      ix = min(max(ix, 1), cur.dimx - 3);
+      iy = min(max(iy, 1), cur.dimy - 3);
+    }
+    float wx[4], dwx[4], wy[4], dwy[4];
+    cr_weights(tx, wx, dwx);
+    cr_weights(ty, wy, dwy);
+    float v = 0.f, gx = 0.f, gy = 0.f;
+    const uint16_t* row = cur.pix + (size_t)(iy - 1) * cur.pitch + (ix - 1);
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const uint16_t* rp = row + (size_t)jj * cur.pitch;
+      const float p0 = u16f(__ldg(rp)), p1 = u16f(__ldg(rp + 1)), p2 = u16f(__ldg(rp + 2)), p3 = u16f(__ldg(rp + 3));
+      const float hx = wx[0] * p0 + wx[1] * p1 + wx[2] * p2 + wx[3] * p3;
+      const float dhx = dwx[0] * p0 + dwx[1] * p1 + dwx[2] * p2 + dwx[3] * p3;
+      v += wy[jj] * hx;
+      gx += wy[jj] * dhx;
+      gy += dwy[jj] * hx;
+    }
+    const float gr = gx * (-s * x + c * y) + gy * (-c * x - s * y);
+    const float vc = v - o.mean0;
+    const float a = u16f(g.w0[o.b + i]) - o.mean0;
+    S[0] += vc;
+    S[1] += vc * vc;
+    S[2] += a * vc;
+    S[3] += gx;
+    S[4] += gy;
+    S[5] += gr;
+    S[6] += gx * gx;
+    S[7] += gx * gy;
+    S[8] += gx * gr;
+    S[9] += gy * gy;
+    S[10] += gy * gr;
+    S[11] += gr * gr;
+    S[12] += vc * gx;
+    S[13] += vc * gy;
+    S[14] += vc * gr;
+    S[15] += a * gx;
+    S[16] += a * gy;
+    S[17] += a * gr;
+  }
+  double T[kNSums];
+#pragma unroll
+  for (int k = 0; k < 18; ++k) {
+    double t = (double)S[k];
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+    T[k] = t;
+  }
+  LmEval e;
+  e.clamped = __any_sync(0xffffffffu, clamped);
+  const double P = (double)o.P;
+  const double mv = T[0] / P;
+  const double n2 = T[1] - P * mv * mv;  // sum b^2
+  const double n = sqrt(n2);
+  // sum a = 0 up to rounding, so sum a b = sum a vc
+  e.ncc = T[2] / (o.norm_a * n);
+  e.F = 2.0 * (1.0 - e.ncc);
+  const double gb[3] = {T[3] / P, T[4] / P, T[5] / P};
+  const double cc[3] = {(T[12] - mv * T[3]) / n, (T[13] - mv * T[4]) / n, (T[14] - mv * T[5]) / n};
+  const double gg[6] = {T[6], T[7], T[8], T[9], T[10], T[11]};
+  const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int k = 0; k < 6; ++k) e.H[k] = (gg[k] - P * gb[ia[k]] * gb[ib[k]] - cc[ia[k]] * cc[ib[k]]) / n2;
+  const double ga[3] = {T[15] / o.norm_a, T[16] / o.norm_a, T[17] / o.norm_a};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) e.gv[k] = -(ga[k] - cc[k] * e.ncc) / n;
+  return e;
+}
+
+// (H + lambda diag H) d = -gv, symmetric 3x3 by Cramer's rule in FP64.
+__device__ bool lm_solve(const double H[6], const double gv[3], double lambda, double d[3]) {
+  const double a = H[0] * (1.0 + lambda), b = H[1], c = H[2];
+  const double e = H[3] * (1.0 + lambda), f = H[4];
+  const double i = H[5] * (1.0 + lambda);
+  const double A = e * i - f * f, B = c * f - b * i, Cc = b * f - c * e;
+  const double det = a * A + b * B + c * Cc;
+  if (!(fabs(det) > 0.0) || !isfinite(det)) return false;
+  const double D = a * i - c * c, E = b * c - a * f, I = a * e - b * b;
+  const double r0 = -gv[0], r1 = -gv[1], r2 = -gv[2];
+  d[0] = (A * r0 + B * r1 + Cc * r2) / det;
+  d[1] = (B * r0 + D * r1 + E * r2) / det;
+  d[2] = (Cc * r0 + E * r1 + I * r2) / det;
+  return isfinite(d[0]) && isfinite(d[1]) && isfinite(d[2]);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kLmWarps * 32) k_subpix_lm(GrainsDev g, FrameDev cur, LmParams lp) {
+  const int lane = threadIdx.x & 31;
+  const int gi = blockIdx.x * kLmWarps + (threadIdx.x >> 5);
+  if (gi >= g.n) return;
+  if (g.masked[gi] || (g.flags[gi] & 3)) return;
+  LmGrain o;
+  o.b = g.pstart[gi];
+  o.P = g.pstart[gi + 1] - o.b;
+  if (o.P <= 0) return;
+  const double xr = (double)g.refx[gi] + g.dx[gi];
+  const double yr = (double)g.refy[gi] + g.dy[gi];
+  const double fxr = floor(xr), fyr = floor(yr);
+  o.ix0 = (int)fxr;
+  o.iy0 = (int)fyr;
+  o.fx = (float)(xr - fxr);
+  o.fy = (float)(yr - fyr);
+  o.drot = g.drot[gi];
+  o.mean0 = (float)g.mean0[gi];
+  o.norm_a = sqrt(g.c0c0[gi]);
+  const double rscale = g.radius[gi] > 1.0 ? g.radius[gi] : 1.0;  // rotation step in pixels at the rim
+
+  double X[3] = {0.0, 0.0, 0.0};
+  LmEval cur_e = lm_eval(g, cur, o, X, lane);
+  bool clamped = cur_e.clamped;
+  double lambda = 1e-3;
+  int it = 0;
+  if (isfinite(cur_e.F)) {
+    for (it = 0; it < lp.max_iter; ++it) {
+      double d[3];
+      if (!lm_solve(cur_e.H, cur_e.gv, lambda, d)) {
+        lambda *= 10.0;
+        if (lambda > 1e8) break;
+        continue;
+      }
+      const double step = fmax(fmax(fabs(d[0]), fabs(d[1])), fabs(d[2]) * rscale);
+      if (step < lp.tol) break;
+      const double Xn[3] = {X[0] + d[0], X[1] + d[1], X[2] + d[2]};
+      const LmEval ne = lm_eval(g, cur, o, Xn, lane);
+      if (isfinite(ne.F) && ne.F < cur_e.F) {
+        X[0] = Xn[0];
+        X[1] = Xn[1];
+        X[2] = Xn[2];
+        cur_e = ne;
+        clamped = clamped || ne.clamped;
+        lambda = fmax(lambda * 0.1, 1e-12);
+      } else {
+        lambda *= 10.0;
+        if (lambda > 1e8) break;
+      }
+    }
+  }
+  if (lane == 0) {
+    g.ncc_subpix[gi] = 1.0 - 0.5 * cur_e.F;
+    g.upix[gi] += X[0];
+    g.vpix[gi] += X[1];
+    g.rot_inc[gi] += X[2];
+    g.dx[gi] += X[0];
+    g.dy[gi] += X[1];
+    g.drot[gi] += X[2];
+    if (clamped) g.status[gi] |= PTK_ST_SUBPIX_CLAMPED;
+    if (lp.iters) lp.iters[gi] = it;
+  }
+}
+
+// F = 1 - NCC and its gradient from the FP32 adjoint sums (for checks).
+__global__ void __launch_bounds__(kLmWarps * 32) k_grad_f32(GrainsDev g, FrameDev cur, const double* Xall, double* f,
+                                                           double* grad) {
+  const int lane = threadIdx.x & 31;
+  const int gi = blockIdx.x * kLmWarps + (threadIdx.x >> 5);
+  if (gi >= g.n) return;
+  LmGrain o;
+  o.b = g.pstart[gi];
+  o.P = g.pstart[gi + 1] - o.b;
+  if (o.P <= 0) return;
+  const double xr = (double)g.refx[gi] + g.dx[gi];
+  const double yr = (double)g.refy[gi] + g.dy[gi];
+  const double fxr = floor(xr), fyr = floor(yr);
+  o.ix0 = (int)fxr;
+  o.iy0 = (int)fyr;
+  o.fx = (float)(xr - fxr);
+  o.fy = (float)(yr - fyr);
+  o.drot = g.drot[gi];
+  o.mean0 = (float)g.mean0[gi];
+  o.norm_a = sqrt(g.c0c0[gi]);
+  const double X[3] = {Xall[3 * gi], Xall[3 * gi + 1], Xall[3 * gi + 2]};
+  const LmEval e = lm_eval(g, cur, o, X, lane);
+  if (lane == 0) {
+    f[gi] = 1.0 - e.ncc;
+    // d(1 - NCC)/dX = (1/2) dF/dX = J^T r
+    grad[3 * gi] = e.gv[0];
+    grad[3 * gi + 1] = e.gv[1];
+    grad[3 * gi + 2] = e.gv[2];
+  }
+}
+
+void launch_subpix_lm(const GrainsDev& g, const FrameDev& cur, const LmParams& lp, cudaStream_t s) {
+  if (g.n <= 0) return;
+  k_subpix_lm<<<(g.n + kLmWarps - 1) / kLmWarps, kLmWarps * 32, 0, s>>>(g, cur, lp);
+}
+
+void launch_grad_f32(const GrainsDev& g, const FrameDev& cur, const double* X, double* f, double* grad,
+                     cudaStream_t s) {
+  if (g.n <= 0) return;
+  k_grad_f32<<<(g.n + kLmWarps - 1) / kLmWarps, kLmWarps * 32, 0, s>>>(g, cur, X, f, grad);
+}
+
+}  // namespace ptk

@@ -76,10 +76,11 @@ def test_pixel_stage_8bit(ptk, wl, oracle, cuda_device, pair_cache):
     assert n >= pair["rec"].shape[0] - 1
 
 
-def test_pixel_stage_16bit(ptk, wl, oracle, cuda_device, pair_cache):
+@pytest.mark.parametrize("method", [0, 2], ids=["tiled", "direct"])
+def test_pixel_stage_16bit(ptk, wl, oracle, cuda_device, pair_cache, method):
     pair = pair_cache("small16", 7)
     opts = _opts(wl, pair)
-    g = _gpu(ptk, pair, opts)
+    g = _gpu(ptk, pair, opts, search_method=method)
     g.precompute()
     g.search(0)
     c = _cpu(oracle, pair, opts)
@@ -142,13 +143,14 @@ def _rescue_pair(wl, seed, disp=7.0):
     return wl.make_pair(p, seed=seed)
 
 
-def test_rescue_levels(ptk, wl, oracle, cuda_device):
+@pytest.mark.parametrize("method", [0, 2], ids=["tiled", "direct"])
+def test_rescue_levels(ptk, wl, oracle, cuda_device, method):
     pair = _rescue_pair(wl, 21)
     z0 = (2, 2, 2, 2, 2, 0.01)
     z1 = (5, 5, 5, 5, 2, 0.01)
     z2 = (9, 9, 9, 9, 3, 0.01)
     opts = dict(zones=[z0, z1, z2], rescue_level=2, NCC_min=0.8, NCC_min_super=0.75, subpixel=0)
-    g = _gpu(ptk, pair, opts)
+    g = _gpu(ptk, pair, opts, search_method=method)
     g.precompute()
     g.search(0)
     g.search(1)
@@ -295,13 +297,18 @@ def test_no_rotation_mode(ptk, wl, oracle, cuda_device, pair_cache):
     assert_pixel_parity(g.get_grains(), c.get_grains(), c.top2())
 
 
-def test_custom_patterns(ptk, wl, oracle, cuda_device, pair_cache):
+@pytest.mark.parametrize("dups", [1, 3, 9], ids=["unique", "few_repeats", "many_repeats"])
+def test_custom_patterns(ptk, wl, oracle, cuda_device, pair_cache, dups):
+    """Sparse random patterns (many multiplicity runs per column, exercising the
+    tiled kernel's entry-by-entry path) and repeated offsets (beyond 4 repeats
+    the direct kernel is used)."""
     pair = pair_cache("tiny", 5)
-    rng = np.random.default_rng(3)
+    rng = np.random.default_rng(3 + dups)
     pats = []
     for _ in range(pair["rec"].shape[0]):
         k = rng.integers(20, 120)
-        pats.append(np.stack([rng.integers(-8, 9, k), rng.integers(-8, 9, k)], 1).astype(np.int32))
+        base = np.stack([rng.integers(-8, 9, k), rng.integers(-8, 9, k)], 1).astype(np.int32)
+        pats.append(np.concatenate([base] + [base[:5]] * (dups - 1)) if dups > 1 else base)
     opts = _opts(wl, pair)
     g = _gpu(ptk, pair, opts, pattern=("patterns", pats))
     g.precompute()
