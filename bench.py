@@ -289,6 +289,25 @@ def main() -> int:
         clocks = sampler.stop()
         gpu_rec = t.get_grains()
 
+        # ---- differentiation form: same exact search, adjoint-LM subpixel ------
+        t.configure(subpix_method=ptk.SUBPIX_ADJOINT_LM)
+        for _ in range(args.warmup):
+            t.restore_grains()
+            t.track_frame(1)
+        lm_ms = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            t.restore_grains()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t.track_frame(1)
+            e1.record(stream)
+            e1.synchronize()
+            lm_ms += e0.elapsed_time(e1)
+        lm_rec = t.get_grains()
+        t.configure(subpix_method=ptk.SUBPIX_POWELL)
+
         # ---- roofline: the pixel search stage alone (k_search dominates) ----
         zone = opts["zones"][0]
         search_ms = []
@@ -326,7 +345,8 @@ def main() -> int:
     ms_step = total_ms / args.steps
     e2e_step = statistics.mean(e2e_ms)
     s_ms = statistics.median(search_ms)
-    ms_step, e2e_step, s_ms = reduce_max([ms_step, e2e_step, s_ms], world, device="cuda")
+    lm_step = lm_ms / args.steps
+    ms_step, e2e_step, s_ms, lm_step = reduce_max([ms_step, e2e_step, s_ms, lm_step], world, device="cuda")
 
     if rank == 0:
         sys.path.insert(0, str(ROOT / "oracle"))
@@ -360,6 +380,17 @@ def main() -> int:
             "accuracy": {"median_abs_err_px_vs_truth": float(np.median(truth_err)),
                          "max_abs_err_px_vs_truth": float(truth_err.max())},
             "clocks": clocks,
+            "forms": {
+                "plain": {"value": aggregate_rate(n, world, ms_step), "ms_per_step": ms_step,
+                          "search": "exact integer/FP64", "subpixel": "FP64 Powell"},
+                "exact_search+adjoint_lm": {"value": aggregate_rate(n, world, lm_step), "ms_per_step": lm_step,
+                                            "search": "exact integer/FP64",
+                                            "subpixel": "adjoint LM (FP32 samples, FP64 3x3 solve)",
+                                            "max_abs_err_px_vs_plain": float(np.abs(lm_rec[:, 4:6] -
+                                                                                    gpu_rec[:, 4:6]).max()),
+                                            "max_abs_err_rad_vs_plain": float(np.abs(lm_rec[:, 6] -
+                                                                                     gpu_rec[:, 6]).max())},
+            },
         }
         if not args.no_cpu_baseline:
             idx = sample_indices(n, args.cpu_sample)

@@ -4,9 +4,9 @@
     libptk_synth.so  seeded synthetic frame generator (host, OpenMP)
 
 Every .cu file is compiled by nvcc for sm_100a only
-(-gencode arch=compute_100a,code=sm_100a); the subpixel and remap kernels are
-compiled with -fmad=false so their FP64 arithmetic follows the reference's
-operation order without fused multiply-adds.  Objects go to _build/ next to
+(-gencode arch=compute_100a,code=sm_100a); the remap kernels are compiled with
+-fmad=false so their FP64 arithmetic repeats the CPU restatement's operations
+exactly (the remap is checked bit for bit).  Objects go to _build/ next to
 this file; a source is recompiled only when it or a header is newer than its
 object.  Run `python p-tracker_b200/build.py` or call build().
 """
@@ -27,7 +27,7 @@ INCLUDE = ROOT / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-O3", "--expt-relaxed-constexpr"]
-NO_FMA = {"ptk_subpix.cu", "ptk_remap.cu"}
+NO_FMA = {"ptk_remap.cu"}
 CU_SOURCES = ["ptk_search.cu", "ptk_search_tiled.cu", "ptk_subpix_lm.cu", "ptk_subpix.cu", "ptk_remap.cu", "ptk_api.cu", "ptk_noalloc.cu"]
 CXX_SOURCES = ["grainfile.cpp"]
 

@@ -427,7 +427,8 @@ int enqueue_subpixel(ptk_ctx* c, int method, cudaStream_t s) {
     lp.iters = nullptr;
     launch_subpix_lm(c->g, frame(c, c->cur_slot), lp, s);
   } else if (method == PTK_SUBPIX_POWELL) {
-    launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, s);
+    launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, c->max_R,
+                         s);
   } else {
     return fail(c, PTK_ERR_ARG, "unknown subpixel method");
   }
@@ -886,7 +887,7 @@ int ptk_track_frame(ptk_ctx* c, int num_image) {
       SearchGeom sg;
       if ((rc = search_geometry(c, l, &sg))) return rc;
     }
-    prepare_subpix(c->max_P);
+    prepare_subpix(c->max_P, c->max_R);
     const int64_t before = c->launches;
     CK(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeRelaxed));
     rc = enqueue_frame(c, pre, swap, c->cap_stream);

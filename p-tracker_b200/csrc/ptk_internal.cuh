@@ -122,9 +122,9 @@ int search_tiled_occupancy(size_t smem, int max_r);
 void launch_search_tiled(const SearchLaunch& p, int max_r, int grid, size_t smem, cudaStream_t s);
 void launch_finalize(const FinalizeLaunch& p, int n_grains, cudaStream_t s);
 void launch_end_frame(const GrainsDev& g, int swap_reference, cudaStream_t s);
-void prepare_subpix(int max_points);
+void prepare_subpix(int max_points, int max_r);
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& ref,
-                          const SubpixParams& sp, int max_points, cudaStream_t s);
+                          const SubpixParams& sp, int max_points, int max_r, cudaStream_t s);
 void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const double* X,
                       double* f, double* grad, int max_points, cudaStream_t s);
 void launch_widen_u8(const uint8_t* src, size_t src_pitch, uint16_t* dst, int dst_pitch, int dimx, int dimy,

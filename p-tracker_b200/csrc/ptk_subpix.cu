@@ -1,11 +1,12 @@
 // Subpixel refinement on sm_100a: the NCC objective through image
 // interpolation, its adjoint gradient, and a per-grain Powell minimiser.
 //
-// This file is compiled with -fmad=false: the objective follows the
-// reference's FP64 operations one for one (src/p-tracker.cpp:1018-1088,
-// src/interpol.cpp:19-144) so that, apart from the order of the sums over
-// pattern points (a block reduction here), the device evaluates the same
-// numbers as the reference.
+// The objective follows the reference's FP64 operations (src/p-tracker.cpp:
+// 1018-1088, src/interpol.cpp:19-144); the order of the sums over pattern
+// points (a block reduction here) and fused multiply-adds change values only
+// in the last bits.  Inside Powell, the objective is evaluated in one pass
+// with the samples centred on mean0 and the frame region under the grain
+// staged in shared memory.
 //
 // One CTA of kSubpixThreads refines one grain.  The Powell driver
 // (follow_pattern_subpixel_xyR, src/p-tracker.cpp:1090-1128; the minimiser
@@ -283,6 +284,88 @@ __device__ ObjGrain load_grain(const GrainsDev& g, int gi) {
   return o;
 }
 
+// Current-frame region around a grain, staged once in shared memory for the
+// objective evaluations of its Powell run (uint16, row-major).
+struct Patch {
+  const uint16_t* pix;
+  int x0, y0, w, h;
+};
+
+__device__ __forceinline__ double patch_or_frame(const Patch& pt, const FrameDev& f, int x, int y) {
+  return (double)pt.pix[(y - pt.y0) * pt.w + (x - pt.x0)];
+}
+
+// Same objective as `objective` in one pass: the samples are centred on mean0,
+// so C11 = sum (v - m0)^2 - P mean(v - m0)^2 and C01 = sum a (v - m0) - mean(v - m0) sum a
+// (sum a = S0 - P mean0) carry no harmful cancellation; one block reduction of
+// three values per evaluation.  Cubic samples whose 4x4 support lies in the
+// staged patch read shared memory.
+template <int NT>
+__device__ double objective_fast(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const ObjGrain& o,
+                                 const Patch& pt, double suma, const double X[3], double* red3, bool* clamped) {
+  const double xpix1 = o.xref + X[0];
+  const double ypix1 = o.yref + X[1];
+  double s1, c1;
+  sincos(o.drot + X[2], &s1, &c1);
+  double S1 = 0.0, S2 = 0.0, S3 = 0.0;
+  for (int i = threadIdx.x; i < o.P; i += NT) {
+    const short2 q = g.pat0[o.b + i];
+    const double x = (double)q.x, y = (double)q.y;
+    const double xs = xpix1 + c1 * x + s1 * y;
+    const double ys = ypix1 - s1 * x + c1 * y;
+    double v;
+    const int ix = (int)floor(xs), iy = (int)floor(ys);
+    if (sp.interp == PTK_INTERP_CUBIC && ix - 1 >= pt.x0 && iy - 1 >= pt.y0 && ix + 2 < pt.x0 + pt.w &&
+        iy + 2 < pt.y0 + pt.h) {
+      const double x01 = xs - (double)ix, y01 = ys - (double)iy;
+      double arr[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int xx = ix - 1 + k;
+        arr[k] = cubic1(patch_or_frame(pt, cur, xx, iy - 1), patch_or_frame(pt, cur, xx, iy),
+                        patch_or_frame(pt, cur, xx, iy + 1), patch_or_frame(pt, cur, xx, iy + 2), y01);
+      }
+      v = cubic1(arr[0], arr[1], arr[2], arr[3], x01);
+    } else {
+      v = interp(cur, sp.interp, xs, ys, clamped);
+    }
+    const double vc = v - o.mean0;
+    const double a = (double)g.w0[o.b + i] - o.mean0;
+    S1 += vc;
+    S2 += vc * vc;
+    S3 += a * vc;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    S1 += __shfl_xor_sync(0xffffffffu, S1, off);
+    S2 += __shfl_xor_sync(0xffffffffu, S2, off);
+    S3 += __shfl_xor_sync(0xffffffffu, S3, off);
+  }
+  const int w = threadIdx.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    red3[3 * w] = S1;
+    red3[3 * w + 1] = S2;
+    red3[3 * w + 2] = S3;
+  }
+  __syncthreads();
+  S1 = S2 = S3 = 0.0;
+#pragma unroll
+  for (int k = 0; k < NT / 32; ++k) {
+    S1 += red3[3 * k];
+    S2 += red3[3 * k + 1];
+    S3 += red3[3 * k + 2];
+  }
+  const double P = (double)o.P;
+  const double mvc = S1 / P;
+  const double c11 = S2 - P * mvc * mvc;
+  const double c01 = S3 - mvc * suma;
+  const double ncc = c01 / sqrt(o.c0c0 * c11);
+  double W = 1.0;
+  const double disp = sqrt(X[0] * X[0] + X[1] * X[1]);
+  if (disp > sp.disp_max) W = sp.stiffness * (disp - sp.disp_max) + 1.0;
+  return (1.0 - ncc) * W;
+}
+
 // --- Powell on the device, block-uniform ----------------------------------
 template <int NT>
 struct PowellEval {
@@ -290,13 +373,14 @@ struct PowellEval {
   const FrameDev* cur;
   const SubpixParams* sp;
   const ObjGrain* o;
-  double* vals;
+  const Patch* pt;
+  double suma;
   double* red;
   bool* clamped;
   int nfev;
   __device__ double operator()(const double X[3]) {
     ++nfev;
-    return objective<NT>(*g, *cur, *sp, *o, X, vals, red, clamped);
+    return objective_fast<NT>(*g, *cur, *sp, *o, *pt, suma, X, red, clamped);
   }
 };
 
@@ -453,18 +537,51 @@ __device__ void powell_minimize(F& f, double p[3], const double step[3], double 
 }  // namespace
 
 // follow_pattern_subpixel_xyR (src/p-tracker.cpp:1090-1128) for every grain.
-__global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, FrameDev cur, SubpixParams sp) {
+__global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, FrameDev cur, SubpixParams sp,
+                                                                    int patch_cap) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ double red[kSubpixThreads / 32];
-  __shared__ int s_clamped;
+  __shared__ double red[3 * (kSubpixThreads / 32)];
+  __shared__ int s_clamped, s_bb[4];
   const int gi = blockIdx.x;
   if (g.masked[gi] || (g.flags[gi] & 3)) return;
   const ObjGrain o = load_grain(g, gi);
   if (o.P <= 0 || o.P > kMaxPatternPoints) return;
-  double* vals = reinterpret_cast<double*>(smem);
+  // stage the frame region under the pattern, with a margin for the Powell steps
+  if (threadIdx.x == 0) {
+    s_clamped = 0;
+    s_bb[0] = s_bb[2] = 1 << 30;
+    s_bb[1] = s_bb[3] = -(1 << 30);
+  }
+  __syncthreads();
+  int xmn = 1 << 30, xmx = -(1 << 30), ymn = 1 << 30, ymx = -(1 << 30);
+  for (int i = threadIdx.x; i < o.P; i += kSubpixThreads) {
+    const short2 q = g.pat0[o.b + i];
+    xmn = min(xmn, (int)q.x);
+    xmx = max(xmx, (int)q.x);
+    ymn = min(ymn, (int)q.y);
+    ymx = max(ymx, (int)q.y);
+  }
+  atomicMin(&s_bb[0], xmn);
+  atomicMax(&s_bb[1], xmx);
+  atomicMin(&s_bb[2], ymn);
+  atomicMax(&s_bb[3], ymx);
+  __syncthreads();
+  constexpr int kMargin = 6;
+  const int cx = (int)floor(o.xref), cy = (int)floor(o.yref);
+  int px0 = max(cx + s_bb[0] - kMargin, 0), py0 = max(cy + s_bb[2] - kMargin, 0);
+  int px1 = min(cx + s_bb[1] + kMargin + 2, cur.dimx), py1 = min(cy + s_bb[3] + kMargin + 2, cur.dimy);
+  int pw = max(px1 - px0, 0), ph = max(py1 - py0, 0);
+  if (pw * ph > patch_cap) ph = pw > 0 ? min(ph, patch_cap / pw) : 0;  // never expected: host sizes the cap
+  uint16_t* s_patch = reinterpret_cast<uint16_t*>(smem);
+  for (int e = threadIdx.x; e < pw * ph; e += kSubpixThreads) {
+    const int yy = e / pw, xx = e - yy * pw;
+    s_patch[e] = cur.pix[(size_t)(py0 + yy) * cur.pitch + (px0 + xx)];
+  }
+  __syncthreads();
+  const Patch pt{s_patch, px0, py0, pw, ph};
+  const double suma = (double)g.s0[gi] - (double)o.P * o.mean0;
   bool clamped = false;
-  if (threadIdx.x == 0) s_clamped = 0;
-  PowellEval<kSubpixThreads> f{&g, &cur, &sp, &o, vals, red, &clamped, 0};
+  PowellEval<kSubpixThreads> f{&g, &cur, &sp, &o, &pt, suma, red, &clamped, 0};
   double X[3] = {0.0, 0.0, 0.0};
   double fret;
   powell_minimize(f, X, sp.init_dir, sp.tol, &fret);
@@ -514,10 +631,15 @@ __global__ void __launch_bounds__(kSubpixThreads) k_objective(GrainsDev g, Frame
   if (threadIdx.x == 0) f[gi] = val;
 }
 
-void prepare_subpix(int max_points) {
+static size_t powell_patch_bytes(int max_r) {
+  const size_t side = (size_t)(2 * max_r + 1 + 2 * 6 + 2);
+  return side * side * sizeof(uint16_t);
+}
+
+void prepare_subpix(int max_points, int max_r) {
   static size_t powell_bytes = 0, objective_bytes = 0;
-  const size_t a = (size_t)max_points * sizeof(double);
-  if (a > powell_bytes) {
+  const size_t a = powell_patch_bytes(max_r);
+  if (a > powell_bytes && a <= 227 * 1024) {
     cudaFuncSetAttribute(k_subpix_powell, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a);
     powell_bytes = a;
   }
@@ -529,17 +651,18 @@ void prepare_subpix(int max_points) {
 }
 
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& /*ref*/, const SubpixParams& sp,
-                          int max_points, cudaStream_t s) {
+                          int max_points, int max_r, cudaStream_t s) {
   if (g.n <= 0) return;
-  prepare_subpix(max_points);
-  const size_t smem = (size_t)max_points * sizeof(double);
-  k_subpix_powell<<<g.n, kSubpixThreads, smem, s>>>(g, cur, sp);
+  prepare_subpix(max_points, max_r);
+  size_t smem = powell_patch_bytes(max_r);
+  if (smem > 227 * 1024) smem = 227 * 1024;  // samples outside the staged region read the frame
+  k_subpix_powell<<<g.n, kSubpixThreads, smem, s>>>(g, cur, sp, (int)(smem / sizeof(uint16_t)));
 }
 
 void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const double* X, double* f,
                       double* grad, int max_points, cudaStream_t s) {
   if (g.n <= 0) return;
-  prepare_subpix(max_points);
+  prepare_subpix(max_points, 0);
   const size_t smem = (size_t)max_points * sizeof(double) * (grad ? 3 : 1);
   k_objective<<<g.n, kSubpixThreads, smem, s>>>(g, cur, sp, X, f, grad);
 }
