@@ -93,6 +93,14 @@ struct ptk_ctx {
   SearchBest* d_best{nullptr};
   size_t best_cap{0};
 
+  // BF16 tensor-core search scratch (PTK_SEARCH_BF16)
+  unsigned char* d_bf_slots{nullptr};  // per-CTA weight slots
+  size_t bf_slots_bytes{0};
+  float* d_c11{nullptr};
+  int2* d_topk{nullptr};
+  SearchBest* d_rescored{nullptr};
+  size_t bf_cap{0};  // (list entries x tiles) the per-tile buffers hold
+
   // distortion
   double disto[14]{};
   bool have_disto{false};
@@ -323,6 +331,7 @@ struct SearchGeom {
   int grid;
   size_t items;
   bool tiled;  // register-tiled exact kernel (else the direct one)
+  bool bf16;   // BF16 tensor-core candidate search + exact rescoring
 };
 
 int search_geometry(ptk_ctx* c, int level, SearchGeom* sg) {
@@ -334,6 +343,17 @@ int search_geometry(ptk_ctx* c, int level, SearchGeom* sg) {
   sg->tiles_v = (sg->nv + kTileV - 1) / kTileV;
   sg->items = (size_t)c->n * sg->nrot * sg->tiles_u * sg->tiles_v;
   if (sg->items > (size_t)INT32_MAX) return fail(c, PTK_ERR_LIMIT, "too many search work items");
+  // The BF16 form covers footprints up to 95 px and 32 rotation steps; other
+  // geometries take the exact kernels (same results, exact ranking).
+  sg->bf16 = c->cfg.search_method == PTK_SEARCH_BF16 && bf16_supported(c->max_R, sg->nrot);
+  if (sg->bf16) {
+    prepare_search_bf16();
+    sg->tiled = false;
+    sg->smem = 0;
+    sg->grid = c->num_sms;
+    sg->items = (size_t)c->n * sg->tiles_u * sg->tiles_v;
+    return PTK_OK;
+  }
   // The tiled kernel decodes multiplicities from its map (at most 16 points per
   // pixel): a rotated pattern stacks at most 4 distinct offsets on one pixel,
   // so patterns whose offsets repeat more than 4 times use the direct kernel.
@@ -364,11 +384,48 @@ int ensure_best(ptk_ctx* c, size_t items) {
   return PTK_OK;
 }
 
+// Per-tile buffers of the BF16 search for `items` (list entries x tiles) and
+// the weight slots of `grid` CTAs.
+int ensure_bf16(ptk_ctx* c, size_t items, int grid) {
+  const size_t slots = (size_t)grid * bf16_slot_bytes(c->max_R);
+  if (slots > c->bf_slots_bytes) {
+    cudaFree(c->d_bf_slots);
+    c->d_bf_slots = nullptr;
+    c->bf_slots_bytes = 0;
+    CK(cudaMalloc(&c->d_bf_slots, slots));
+    c->bf_slots_bytes = slots;
+    invalidate(c);
+  }
+  if (items > c->bf_cap) {
+    cudaFree(c->d_c11);
+    cudaFree(c->d_topk);
+    cudaFree(c->d_rescored);
+    c->d_c11 = nullptr;
+    c->d_topk = nullptr;
+    c->d_rescored = nullptr;
+    c->bf_cap = 0;
+    CK(cudaMalloc(&c->d_c11, sizeof(float) * kTileU * kTileV * items));
+    CK(cudaMalloc(&c->d_topk, sizeof(int2) * kBf16KeepMax * items));
+    CK(cudaMalloc(&c->d_rescored, sizeof(SearchBest) * kBf16KeepMax * items));
+    c->bf_cap = items;
+    invalidate(c);
+  }
+  return PTK_OK;
+}
+
+int ensure_search_scratch(ptk_ctx* c, const SearchGeom& sg) {
+  return sg.bf16 ? ensure_bf16(c, sg.items, sg.grid) : ensure_best(c, sg.items);
+}
+
+// Kernels one search level launches (finalize included).
+int level_launches(const SearchGeom& sg) { return sg.bf16 ? 4 : 2; }
+
 int enqueue_search(ptk_ctx* c, int level, cudaStream_t s) {
   SearchGeom sg;
   int rc = search_geometry(c, level, &sg);
   if (rc) return rc;
-  if (c->best_cap < sg.items) return fail(c, PTK_ERR_STATE, "search scratch not prepared");
+  if (sg.bf16 ? (c->bf_cap < sg.items || !c->d_bf_slots) : (c->best_cap < sg.items))
+    return fail(c, PTK_ERR_STATE, "search scratch not prepared");
   if (level == 0) {
     launch_stage_begin(c->g, c->d_counts, s);
     c->launches += 1;
@@ -377,6 +434,31 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s) {
   const int* count = c->d_counts + level;
   CK(cudaMemsetAsync(c->d_work, 0, sizeof(int), s));
   const ptk_zone& z = c->cfg.zone[level];
+  if (sg.bf16) {
+    Bf16Launch b;
+    b.g = c->g;
+    b.cur = frame(c, c->cur_slot);
+    b.list = list;
+    b.list_count = count;
+    b.work_next = c->d_work;
+    b.steps = c->d_steps[level];
+    b.nrot = sg.nrot;
+    b.left = z.left;
+    b.right = z.right;
+    b.up = z.up;
+    b.down = z.down;
+    b.tiles_u = sg.tiles_u;
+    b.tiles_v = sg.tiles_v;
+    b.keep = std::min(std::max(c->cfg.topk, 1), kBf16KeepMax);
+    b.max_items = (int)sg.items;
+    b.scratch = c->d_bf_slots;
+    b.slot_bytes = bf16_slot_bytes(c->max_R);
+    b.c11 = c->d_c11;
+    b.topk = c->d_topk;
+    b.rescored = c->d_rescored;
+    b.error = c->d_counts + 3;
+    launch_search_bf16(b, sg.grid, s);
+  }
   SearchLaunch p;
   p.g = c->g;
   p.cur = frame(c, c->cur_slot);
@@ -393,27 +475,32 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s) {
   p.tiles_v = sg.tiles_v;
   p.best = c->d_best;
   p.max_items = (int)c->best_cap;
-  if (sg.tiled) launch_search_tiled(p, c->max_R, sg.grid, sg.smem, s);
-  else launch_search(p, sg.grid, sg.smem, s);
+  if (sg.bf16) {
+    // rescored records: [list entry][tile][kBf16KeepMax]
+  } else if (sg.tiled) {
+    launch_search_tiled(p, c->max_R, sg.grid, sg.smem, s);
+  } else {
+    launch_search(p, sg.grid, sg.smem, s);
+  }
   FinalizeLaunch f;
   f.g = c->g;
   f.list = list;
   f.list_count = count;
   f.steps = c->d_steps[level];
-  f.nrot = sg.nrot;
+  f.nrot = sg.bf16 ? kBf16KeepMax : sg.nrot;  // records per tile
   f.left = z.left;
   f.up = z.up;
   f.nu = sg.nu;
   f.nv = sg.nv;
   f.tiles = sg.tiles_u * sg.tiles_v;
-  f.best = c->d_best;
+  f.best = sg.bf16 ? c->d_rescored : c->d_best;
   f.level = level;
   f.NCC_min = c->cfg.NCC_min;
   f.NCC_min_super = c->cfg.NCC_min_super;
   f.out_list = level == 0 ? c->d_lists : c->d_lists + c->n;
   f.out_count = c->d_counts + (level == 0 ? 1 : 2);
   launch_finalize(f, c->n, s);
-  c->launches += 2;
+  c->launches += level_launches(sg);
   return PTK_OK;
 }
 
@@ -437,13 +524,23 @@ int enqueue_subpixel(ptk_ctx* c, int method, cudaStream_t s) {
 }
 
 int prepare_searches(ptk_ctx* c) {
-  size_t need = 0;
+  size_t need = 0, need_bf = 0;
+  int grid_bf = 0;
   for (int level = 0; level < 3; ++level) {
     if (level > c->cfg.rescue_level) break;
     SearchGeom sg;
     int rc = search_geometry(c, level, &sg);
     if (rc) return rc;
-    need = std::max(need, sg.items);
+    if (sg.bf16) {
+      need_bf = std::max(need_bf, sg.items);
+      grid_bf = std::max(grid_bf, sg.grid);
+    } else {
+      need = std::max(need, sg.items);
+    }
+  }
+  if (need_bf) {
+    int rc = ensure_bf16(c, need_bf, grid_bf);
+    if (rc) return rc;
   }
   return ensure_best(c, need ? need : 1);
 }
@@ -553,6 +650,10 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_lists);
   cudaFree(c->d_work);
   cudaFree(c->d_best);
+  cudaFree(c->d_bf_slots);
+  cudaFree(c->d_c11);
+  cudaFree(c->d_topk);
+  cudaFree(c->d_rescored);
   cudaFree(c->d_map);
   cudaFree(c->d_X);
   cudaFree(c->d_f);
@@ -826,7 +927,7 @@ int ptk_search(ptk_ctx* c, int level) {
   if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
   SearchGeom sg;
   if ((rc = search_geometry(c, level, &sg))) return rc;
-  if ((rc = ensure_best(c, sg.items))) return rc;
+  if ((rc = ensure_search_scratch(c, sg))) return rc;
   if ((rc = enqueue_search(c, level, c->stream))) return rc;
   CK(cudaGetLastError());
   return PTK_OK;
@@ -907,7 +1008,11 @@ int ptk_track_frame(ptk_ctx* c, int num_image) {
   // launches of one frame: precompute, stage_begin, (search, finalize) per level,
   // subpixel, end_frame
   int64_t nk = (pre ? 1 : 0) + 1;
-  for (int l = 0; l <= c->cfg.rescue_level && l < 3; ++l) nk += (l == 0 ? 3 : 2);
+  for (int l = 0; l <= c->cfg.rescue_level && l < 3; ++l) {
+    SearchGeom sg;
+    if ((rc = search_geometry(c, l, &sg))) return rc;
+    nk += (l == 0 ? 1 : 0) + level_launches(sg);
+  }
   if (c->cfg.subpixel) nk += 1;
   c->launches += nk;
   if (swap) {
@@ -1008,6 +1113,12 @@ void* ptk_get_stream(ptk_ctx* c) { return c ? static_cast<void*>(c->stream) : nu
 int ptk_synchronize(ptk_ctx* c) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
   CK(cudaStreamSynchronize(c->stream));
+  int flag = 0;  // set by a device wait that gave up (BF16 search)
+  CK(cudaMemcpy(&flag, c->d_counts + 3, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    CK(cudaMemset(c->d_counts + 3, 0, sizeof(int)));
+    return fail(c, PTK_ERR_TIMEOUT, "a tensor-core search wait gave up");
+  }
   return PTK_OK;
 }
 

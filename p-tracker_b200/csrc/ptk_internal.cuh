@@ -94,6 +94,29 @@ struct FinalizeLaunch {
   int* out_count;
 };
 
+// BF16 tensor-core search: kept candidates per tile (upper bound of `keep`).
+constexpr int kBf16KeepMax = 8;
+
+struct Bf16Launch {
+  GrainsDev g;
+  FrameDev cur;
+  const int* list;
+  const int* list_count;
+  int* work_next;           // work-queue head over list entries (zeroed before launch)
+  const double* steps;
+  int nrot;
+  int left, right, up, down;
+  int tiles_u, tiles_v;
+  int keep;                 // candidates per tile rescored exactly (1..kBf16KeepMax)
+  int max_items;            // list capacity x tiles: grid of the per-tile kernels
+  unsigned char* scratch;   // per-CTA BF16 weight slots
+  size_t slot_bytes;
+  float* c11;               // [list entry][tile][32 x 32] window variance
+  int2* topk;               // [list entry][tile][kBf16KeepMax] kept (u, v), INT_MIN when none
+  SearchBest* rescored;     // [list entry][tile][kBf16KeepMax] exact best per kept candidate
+  int* error;               // set when a bounded wait gave up
+};
+
 struct SubpixParams {
   double tol;
   double init_dir[3];
@@ -121,6 +144,10 @@ size_t search_tiled_smem(int max_r);
 int search_tiled_occupancy(size_t smem, int max_r);
 void launch_search_tiled(const SearchLaunch& p, int max_r, int grid, size_t smem, cudaStream_t s);
 void launch_finalize(const FinalizeLaunch& p, int n_grains, cudaStream_t s);
+bool bf16_supported(int max_r, int nrot);
+size_t bf16_slot_bytes(int max_r);
+void prepare_search_bf16();
+void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s);
 void launch_end_frame(const GrainsDev& g, int swap_reference, cudaStream_t s);
 void prepare_subpix(int max_points, int max_r);
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& ref,

@@ -1,0 +1,857 @@
+// BF16 tensor-core integer-pixel + rotation-step search (the precision form)
+// on sm_100a.
+//
+// Same result contract as the exact search (src/p-tracker.cpp:659-1016): the
+// grain moves to the first strict NCC maximum above 0 over (rotation step,
+// x offset, y offset), ranked on exact integer sums.  The tensor cores only
+// decide WHERE to look; every value that reaches the acceptance rule is exact.
+//
+//  1. k_window_stats (CUDA cores): per candidate (u, v) of a 32x32 tile, the
+//     window variance C11 = S11 - S1^2 / P of the current frame under
+//     pattern0_rotated, from row prefix sums over the pattern's runs of equal
+//     multiplicity (S1 exact in integers, S11 in FP32 - it only normalises
+//     the ranking).
+//  2. k_search_bf16 (tcgen05): the cross terms for every rotation step r at
+//     every candidate,
+//         D_r(u, v) = sum_i (I0_i - mean0) * I1(X + u + q_r,i.x, Y + v + q_r,i.y),
+//     in BF16 with FP32 accumulation in tensor memory, and per candidate the
+//     approximate score max_r D_r / sqrt(C11).  The best `keep` candidates of
+//     each tile are written out.
+//  3. k_rescore_bf16 (CUDA cores, exact integers): every rotation step at each
+//     kept candidate, with the exact search's sums and NCC expression, giving
+//     per-candidate best records in the reference's order; the level's usual
+//     finalize applies the acceptance rule to them.
+//
+// Tensor-core formulation of step 2 (one work item = one grain, persistent
+// CTAs, one per SM, 256 threads):
+//   * A operand (M = 128 = 4 x-shifts j by 32 rotation slots r, K = 16
+//     footprint columns): the rotated patterns' centred reference values,
+//     scattered per rotation into float maps and stored in BF16 in the CTA's
+//     own scratch slot as [footprint row][8-column block][rotation][8 values]
+//     (512 bytes per row block).  In shared memory each row has 3 zero blocks
+//     in front, so row m = 32 j + r of a core-matrix group reads block
+//     (a + j): consecutive 8-row groups are 128 bytes apart (SBO) and the two
+//     K halves 512 bytes apart (LBO), i.e. the x-shift by 8 j columns costs
+//     nothing but the descriptor.  Rows are brought in with bulk async copies
+//     (cp.async.bulk, no multicast).
+//   * B operand (N = 256 = 32 y offsets by 8 x offsets, K = 16 image
+//     columns): the current frame in a Hankel layout - per image row and
+//     8-column block, 8 entries of 16 bytes, entry s holding the 8 pixels that
+//     start s columns into the block - so the 8 x offsets of a core matrix are
+//     16 bytes apart, K halves 128 bytes apart (LBO) and y offsets one image
+//     row apart (SBO).
+//   * For footprint row y and chunk c, D[32 j + r][8 v + s] accumulates
+//     W_r(y, f) * I(y + v, f + 24 - 8 j + s): candidate x offset 24 - 8 j + s.
+//     One MMA (M=128, N=256, K=16) covers the whole 32 x 32 x 32 tile; a
+//     grain's tile takes (footprint rows) x (chunks) MMAs, issued by one thread
+//     per strip of rows and committed to an mbarrier.
+//   * The epilogue reads the 128 x 256 FP32 accumulator with tcgen05.ld
+//     (warp w: lanes 32 (w % 4).., columns 128 (w / 4)..), takes the maximum
+//     over rotation lanes per candidate with a warp max-reduction, divides by
+//     sqrt(C11) and keeps the best candidates.
+//
+// Pattern rotation (all three kernels) is rotate_pixel_pattern's
+// (src/p-tracker.cpp:615-621) result bit for bit: an FP32 estimate decides the
+// rounding, and the FP64 expression is evaluated whenever the estimate lies
+// within 1e-3 of a half-integer (the estimate's error is below 2e-5 for the
+// offsets allowed here).
+//
+// Limits (else the exact kernels run): pattern extent within +-47 px
+// (footprint side <= 95), at most 32 rotation steps.
+#include <cuda_bf16.h>
+
+#include <climits>
+
+#include "ptk_internal.cuh"
+
+namespace ptk {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kNRot = 32;         // rotation slots of the A operand
+constexpr int kMaxFoot = 96;      // footprint side limit (2 * half + 1 < 96)
+constexpr int kTmemCols = 256;    // 128 lanes x 256 FP32 columns: the whole tile
+constexpr int kSmemBudget = 200 * 1024;
+constexpr long kWaitLimit = 1L << 22;
+
+// window statistics: 512 threads, prefix rows of 128 entries, runs per row
+constexpr int kStatsThreads = 512;
+constexpr int kPrefRow = 128;
+constexpr int kRunCap = kMaxFoot;
+constexpr size_t kPrefBytes = (size_t)(kMaxFoot + kTileV - 1) * kPrefRow * 8;
+constexpr size_t kStatsSmem = kPrefBytes + 2 * (size_t)kMaxFoot * kRunCap * 4;
+
+// A and B operand formats: BF16 x BF16 -> FP32, both K-major, M = 128, N = 256.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
+                            ((uint32_t)(128 >> 4) << 24);
+
+struct Geom {
+  int half;  // footprint covers offsets [-half, half] in x and y
+  int fw;    // footprint side
+  int nbf;   // 8-column blocks of the footprint
+  int nch;   // 16-column MMA chunks (footprint + 24 columns of shift)
+  int wb;    // weight blocks per row in shared memory (3 leading zero blocks)
+  int hb;    // Hankel blocks per image row
+  int rs;    // footprint rows per strip
+};
+
+__host__ __device__ inline Geom geom_of(int half) {
+  Geom g;
+  g.half = half;
+  g.fw = 2 * half + 1;
+  g.nbf = (g.fw + 7) / 8;
+  g.nch = (g.nbf + 3 + 1) / 2;
+  g.wb = 2 * g.nch + 3;
+  g.hb = 2 * g.nch;
+  const int per_row = g.wb * 512 + g.hb * 128;
+  int rs = (kSmemBudget - 31 * g.hb * 128) / per_row;
+  if (rs > g.fw) rs = g.fw;
+  g.rs = rs < 1 ? 1 : rs;
+  return g;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// tcgen05 shared-memory matrix descriptor: K-major, no swizzle, version 1.
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+// Bounded wait on an mbarrier phase; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  uint32_t done = 0;
+  for (long it = 0; it < kWaitLimit && !done; ++it) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+  }
+  return done != 0;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// 1-D bulk async copy global -> shared (16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(mbar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// rotate_pixel_pattern (src/p-tracker.cpp:615-621): FP64 without contraction,
+// round half away from zero - identical to the exact search's rotation.
+__device__ __forceinline__ short2 rotate_round_b(short2 p, double c, double s) {
+  const double px = (double)p.x, py = (double)p.y;
+  const double xr = __dadd_rn(__dmul_rn(c, px), __dmul_rn(s, py));
+  const double yr = __dadd_rn(__dmul_rn(-s, px), __dmul_rn(c, py));
+  return make_short2((short)round(xr), (short)round(yr));
+}
+
+// Small integer <-> float without the conversion pipe (|v| < 2^22).
+__device__ __forceinline__ float small_i2f(int v) { return __int_as_float(0x4B400000 + v) - 12582912.0f; }
+
+// rotate_round_b's result for |p.x|, |p.y| <= 1024: the FP32 estimate
+// (error < 3e-4 at that size) rounds to nearest unless it lies within 1e-3 of
+// a half-integer, where the FP64 expression decides.
+__device__ __forceinline__ short2 rotate_round_fast(short2 p, float cf, float sf, double c, double s) {
+  const float pxf = small_i2f(p.x), pyf = small_i2f(p.y);
+  const float xf = fmaf(cf, pxf, sf * pyf);
+  const float yf = fmaf(cf, pyf, -(sf * pxf));
+  const float mx = xf + 12582912.0f, my = yf + 12582912.0f;  // rint in the low mantissa bits
+  const float rx = mx - 12582912.0f, ry = my - 12582912.0f;
+  if (fabsf(xf - rx) < 0.499f && fabsf(yf - ry) < 0.499f)
+    return make_short2((short)(__float_as_int(mx) - 0x4B400000), (short)(__float_as_int(my) - 0x4B400000));
+  return rotate_round_b(p, c, s);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// float <-> int keys whose signed order is the float order (finite values)
+__device__ __forceinline__ int f2key(float f) {
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+__device__ __forceinline__ float key2f(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7FFFFFFF); }
+
+__device__ __forceinline__ bool better_b(double ncc, int idx, double bn, int bi) {
+  return ncc > 0.0 && (ncc > bn || (ncc == bn && idx < bi));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// 1. Window variance under pattern0_rotated for every candidate of a tile.
+//    The pattern's multiplicity map is split into row runs of equal
+//    multiplicity; the frame patch gets row prefix sums of I (uint32, exact)
+//    and I^2 (FP32).  Candidate (u, v) then costs two lookups per run:
+//    S1 = sum_runs m * (P1[y + v][x1 + u + 1] - P1[y + v][x0 + u]).
+//    lane = x offset u, warp w = y offsets 2w, 2w + 1.
+__global__ void __launch_bounds__(kStatsThreads) k_window_stats(Bf16Launch p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_bb[4];
+  __shared__ int s_nrun[kMaxFoot];
+  const int item = blockIdx.x;
+  const int tiles = p.tiles_u * p.tiles_v;
+  const int li = item / tiles, t = item - li * tiles;
+  if (li >= *p.list_count) return;
+  const int tu = t / p.tiles_v, tv = t - tu * p.tiles_v;
+  const int gi = p.list[li];
+  const GrainsDev& g = p.g;
+  const int b = g.pstart[gi], P = g.pstart[gi + 1] - b;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int kWarps = kStatsThreads / 32;
+  if (g.masked[gi] || (g.flags[gi] & 2) || P <= 0 || P > kMaxPatternPoints) return;
+  if (tid == 0) {
+    s_bb[0] = s_bb[2] = INT_MAX;
+    s_bb[1] = s_bb[3] = INT_MIN;
+  }
+  __syncthreads();
+  {
+    int xmn = INT_MAX, xmx = INT_MIN, ymn = INT_MAX, ymx = INT_MIN;
+    for (int i = tid; i < P; i += kStatsThreads) {
+      const short2 q = g.pat0[b + i];
+      xmn = min(xmn, (int)q.x);
+      xmx = max(xmx, (int)q.x);
+      ymn = min(ymn, (int)q.y);
+      ymx = max(ymx, (int)q.y);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      xmn = min(xmn, __shfl_xor_sync(0xffffffffu, xmn, o));
+      xmx = max(xmx, __shfl_xor_sync(0xffffffffu, xmx, o));
+      ymn = min(ymn, __shfl_xor_sync(0xffffffffu, ymn, o));
+      ymx = max(ymx, __shfl_xor_sync(0xffffffffu, ymx, o));
+    }
+    if (lane == 0) {
+      atomicMin(&s_bb[0], xmn);
+      atomicMax(&s_bb[1], xmx);
+      atomicMin(&s_bb[2], ymn);
+      atomicMax(&s_bb[3], ymx);
+    }
+  }
+  __syncthreads();
+  const int bx0 = s_bb[0], by0 = s_bb[2];
+  const int bw = s_bb[1] - bx0 + 1, bh = s_bb[3] - by0 + 1;
+  if (bw >= kMaxFoot || bh >= kMaxFoot) return;  // excluded by the host's geometry check
+  int* mmap = reinterpret_cast<int*>(smem);  // bh x bw multiplicities (aliased by the prefix rows later)
+  uint32_t* run_a = reinterpret_cast<uint32_t*>(smem + kPrefBytes);  // [y][k]: x0 | m << 16
+  uint32_t* run_b = run_a + kMaxFoot * kRunCap;                          // [y][k]: x1
+  for (int e = tid; e < bw * bh; e += kStatsThreads) mmap[e] = 0;
+  __syncthreads();
+  for (int i = tid; i < P; i += kStatsThreads) {
+    const short2 q = g.pat0[b + i];
+    atomicAdd(&mmap[(q.y - by0) * bw + (q.x - bx0)], 1);
+  }
+  __syncthreads();
+  // runs of equal multiplicity, one warp per row (starts and ends paired by rank)
+  for (int y = warp; y < bh; y += kWarps) {
+    const int* row = mmap + y * bw;
+    int ns = 0, ne = 0;
+    for (int x0 = 0; x0 < bw; x0 += 32) {
+      const int x = x0 + lane;
+      const int m = x < bw ? row[x] : 0;
+      const int ml = (x >= 1 && x <= bw) ? row[x - 1] : 0;
+      const int mr = (x + 1 < bw) ? row[x + 1] : 0;
+      const bool st = m != 0 && m != ml, en = m != 0 && m != mr;
+      const unsigned bs = __ballot_sync(0xffffffffu, st), be = __ballot_sync(0xffffffffu, en);
+      const unsigned below = (1u << lane) - 1u;
+      if (st) run_a[y * kRunCap + ns + __popc(bs & below)] = (uint32_t)x | ((uint32_t)m << 16);
+      if (en) run_b[y * kRunCap + ne + __popc(be & below)] = (uint32_t)x;
+      ns += __popc(bs);
+      ne += __popc(be);
+    }
+    if (lane == 0) s_nrun[y] = ns;
+  }
+  __syncthreads();
+  // prefix rows: pref[rho][x] = (sum of I, sum of I^2) over columns < x
+  const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
+  const int u0 = -p.left + tu * kTileU, v0 = -p.up + tv * kTileV;
+  const int X0 = g.refx[gi] + gdx + bx0 + u0, Y0 = g.refy[gi] + gdy + by0 + v0;
+  const int pc = bw + kTileU - 1;  // patch columns; prefix entries 0..pc
+  uint2* pref = reinterpret_cast<uint2*>(smem);
+  for (int rho = warp; rho < bh + kTileV - 1; rho += kWarps) {
+    const int Y = Y0 + rho;
+    const bool rowin = Y >= 0 && Y < p.cur.dimy;
+    uint32_t s[4];
+    float q[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int x = 4 * lane + j, X = X0 + x;
+      uint32_t v = 0;
+      if (rowin && x < pc && X >= 0 && X < p.cur.dimx) v = p.cur.pix[(size_t)Y * p.cur.pitch + X];
+      const float vf = small_i2f((int)v);
+      s[j] = v + (j ? s[j - 1] : 0u);
+      q[j] = vf * vf + (j ? q[j - 1] : 0.0f);
+    }
+    uint32_t ts = s[3];
+    float tq = q[3];
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t os = __shfl_up_sync(0xffffffffu, ts, o);
+      const float oq = __shfl_up_sync(0xffffffffu, tq, o);
+      if (lane >= o) {
+        ts += os;
+        tq += oq;
+      }
+    }
+    const uint32_t es = ts - s[3];
+    const float eq = tq - q[3];
+    uint2* prow = pref + rho * kPrefRow;
+    if (lane == 0) prow[0] = make_uint2(0u, 0u);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int x = 4 * lane + j;
+      if (x + 1 < kPrefRow) prow[x + 1] = make_uint2(es + s[j], __float_as_uint(eq + q[j]));
+    }
+  }
+  __syncthreads();
+  const int u = lane;
+  uint32_t S1[2] = {0u, 0u};
+  float S11[2] = {0.0f, 0.0f};
+  for (int y = 0; y < bh; ++y) {
+    const int nr = s_nrun[y];
+    for (int k = 0; k < nr; ++k) {
+      const uint32_t a = run_a[y * kRunCap + k];
+      const int x0 = (int)(a & 0xffffu), x1 = (int)run_b[y * kRunCap + k];
+      const uint32_t m = a >> 16;
+      const float mf = small_i2f((int)m);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const uint2* prow = pref + (y + 2 * warp + j) * kPrefRow;
+        const uint2 hi = prow[x1 + u + 1], lo = prow[x0 + u];
+        S1[j] += m * (hi.x - lo.x);
+        S11[j] = fmaf(mf, __uint_as_float(hi.y) - __uint_as_float(lo.y), S11[j]);
+      }
+    }
+  }
+  float* out = p.c11 + (size_t)item * (kTileU * kTileV);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const double c11 = (double)S11[j] - (double)S1[j] * (double)S1[j] / (double)P;
+    out[(2 * warp + j) * kTileU + u] = (float)c11;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2. Tensor-core cross terms and the kept candidates of every tile.
+__global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
+  extern __shared__ __align__(128) unsigned char smem_bf[];
+  unsigned char* smem = smem_bf;
+  __shared__ __align__(8) unsigned long long s_mbar;   // MMA completion
+  __shared__ __align__(8) unsigned long long s_wbar;   // weight-row bulk copies
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_li, s_err, s_n2, s_big, s_bb[4];
+  __shared__ double2 s_cs[kNRot];
+  __shared__ float2 s_csf[kNRot];
+  __shared__ float s_cv[8 * kBf16KeepMax];
+  __shared__ int s_ci[8 * kBf16KeepMax];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t mbar = smem_u32(&s_mbar), wbar = smem_u32(&s_wbar);
+  uint4* slot = reinterpret_cast<uint4*>(p.scratch + (size_t)blockIdx.x * p.slot_bytes);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(wbar));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    s_err = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = s_tmem;
+  uint32_t parity = 0, wparity = 0;
+
+  const GrainsDev& g = p.g;
+  const int count = *p.list_count;
+  const int tiles = p.tiles_u * p.tiles_v;
+  const int keep = p.keep;
+
+  for (;;) {
+    __syncthreads();  // every thread is done with the previous grain's shared state
+    if (tid == 0) {
+      s_li = atomicAdd(p.work_next, 1);
+      s_n2 = 0;
+      s_big = 0;
+      s_bb[0] = s_bb[2] = INT_MAX;
+      s_bb[1] = s_bb[3] = INT_MIN;
+    }
+    __syncthreads();
+    const int li = s_li;
+    if (li >= count || s_err) break;
+    const int gi = p.list[li];
+    const int b = g.pstart[gi], P = g.pstart[gi + 1] - b;
+    int2* topk_g = p.topk + (size_t)li * tiles * kBf16KeepMax;
+    if (g.masked[gi] || (g.flags[gi] & 2) || P <= 0 || P > kMaxPatternPoints) {
+      for (int e = tid; e < tiles * kBf16KeepMax; e += kThreads) topk_g[e] = make_int2(INT_MIN, INT_MIN);
+      continue;
+    }
+    // footprint half-extent from the pattern's largest norm; rotation cos/sin
+    const double base_rot = g.refrot[gi] + g.drot[gi];  // total_rot = base_rot + step, as the exact search
+    {
+      int n2 = 0;
+      for (int i = tid; i < P; i += kThreads) {
+        const short2 q = g.pat[b + i];
+        n2 = max(n2, (int)q.x * q.x + (int)q.y * q.y);
+      }
+      atomicMax(&s_n2, n2);
+      if (tid < p.nrot) {
+        double sr, cr;
+        sincos(base_rot + p.steps[tid], &sr, &cr);
+        s_cs[tid] = make_double2(cr, sr);
+        s_csf[tid] = make_float2((float)cr, (float)sr);
+      }
+    }
+    __syncthreads();
+    const Geom G = geom_of((int)ceil(sqrt((double)s_n2)) + 1);
+    if (G.fw >= kMaxFoot) {  // excluded by the host's geometry check
+      if (tid == 0) atomicOr(&g.flags[gi], 4);
+      for (int e = tid; e < tiles * kBf16KeepMax; e += kThreads) topk_g[e] = make_int2(INT_MIN, INT_MIN);
+      continue;
+    }
+    const float mean0 = (float)g.mean0[gi];
+    const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
+
+    // ---- phase 1: BF16 weights of every rotation into the scratch slot,
+    //      as many rotations per pass as float maps fit in shared memory
+    float* fmap = reinterpret_cast<float*>(smem);
+    const int fw2 = G.fw * G.fw;
+    const int nb_max = max(1, min(p.nrot, kSmemBudget / (fw2 * 4)));
+    const int rows = G.fw * G.nbf;
+    int xmn = INT_MAX, xmx = INT_MIN, ymn = INT_MAX, ymx = INT_MIN;
+    bool big = false;
+    for (int r0 = 0; r0 < p.nrot; r0 += nb_max) {
+      const int nb = min(nb_max, p.nrot - r0);
+      for (int e = tid; e < nb * fw2; e += kThreads) fmap[e] = 0.0f;
+      __syncthreads();
+      for (int i = tid; i < P; i += kThreads) {
+        const short2 q0 = g.pat[b + i];
+        const float w = small_i2f((int)g.w0[b + i]) - mean0;
+        for (int k = 0; k < nb; ++k) {
+          const float2 cf = s_csf[r0 + k];
+          const double2 cd = s_cs[r0 + k];
+          const short2 q = rotate_round_fast(q0, cf.x, cf.y, cd.x, cd.y);
+          xmn = min(xmn, (int)q.x);
+          xmx = max(xmx, (int)q.x);
+          ymn = min(ymn, (int)q.y);
+          ymx = max(ymx, (int)q.y);
+          const int fx = q.x + G.half, fy = q.y + G.half;
+          if (fx >= 0 && fy >= 0 && fx < G.fw && fy < G.fw)
+            atomicAdd(&fmap[k * fw2 + fy * G.fw + fx], w);
+          else
+            big = true;
+        }
+      }
+      __syncthreads();
+      for (int e = tid; e < nb * rows; e += kThreads) {
+        const int rem = e / nb, k = e - rem * nb;
+        const int y = rem / G.nbf, af = rem - y * G.nbf;
+        const float* src = fmap + k * fw2 + y * G.fw + 8 * af;
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = (8 * af + j < G.fw) ? src[j] : 0.0f;
+        slot[(size_t)rem * kNRot + r0 + k] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
+                                                        pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
+      }
+      __syncthreads();
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      xmn = min(xmn, __shfl_xor_sync(0xffffffffu, xmn, o));
+      xmx = max(xmx, __shfl_xor_sync(0xffffffffu, xmx, o));
+      ymn = min(ymn, __shfl_xor_sync(0xffffffffu, ymn, o));
+      ymx = max(ymx, __shfl_xor_sync(0xffffffffu, ymx, o));
+    }
+    if (lane == 0) {
+      atomicMin(&s_bb[0], xmn);
+      atomicMax(&s_bb[1], xmx);
+      atomicMin(&s_bb[2], ymn);
+      atomicMax(&s_bb[3], ymx);
+    }
+    if (big) s_big = 1;
+    unsigned char* sW = smem;
+    unsigned char* sH = smem + (size_t)G.rs * G.wb * 512;
+    const uint32_t wbase = smem_u32(sW), hbase = smem_u32(sH);
+    // zero blocks of every weight row (3 in front, the rest after the footprint)
+    for (int e = tid; e < G.rs * (G.wb - G.nbf) * kNRot; e += kThreads) {
+      const int yl = e / ((G.wb - G.nbf) * kNRot), rem = e - yl * ((G.wb - G.nbf) * kNRot);
+      const int zb = rem >> 5, r = rem & 31;
+      const int a = zb < 3 ? zb : zb + G.nbf;
+      reinterpret_cast<uint4*>(sW)[((size_t)yl * G.wb + a) * kNRot + r] = make_uint4(0, 0, 0, 0);
+    }
+    // slot rows (generic stores) are read next by the bulk-copy engine
+    asm volatile("fence.proxy.async;" ::: "memory");
+    __syncthreads();
+    if (s_big) {  // cannot happen for |offset| < half; guarded all the same
+      if (tid == 0) atomicOr(&g.flags[gi], 4);
+      for (int e = tid; e < tiles * kBf16KeepMax; e += kThreads) topk_g[e] = make_int2(INT_MIN, INT_MIN);
+      continue;
+    }
+    const int bbx0 = s_bb[0], bbx1 = s_bb[1], bby0 = s_bb[2], bby1 = s_bb[3];
+    const float sub = 8388608.0f + rintf(mean0);  // pixel v -> (2^23 + v) - sub = v - ishift, exactly
+    const uint32_t row_bytes = (uint32_t)G.nbf * 512;
+
+    for (int t = 0; t < tiles; ++t) {
+      const int tu = t / p.tiles_v, tv = t - tu * p.tiles_v;
+      const int u0 = -p.left + tu * kTileU, u1 = min(u0 + kTileU - 1, p.right);
+      const int v0 = -p.up + tv * kTileV, v1 = min(v0 + kTileV - 1, p.down);
+      int2* topk = topk_g + (size_t)t * kBf16KeepMax;
+      {  // the union of the rotated footprints over the tile's candidates must stay in the frame
+        const int ax0 = g.refx[gi] + gdx + bbx0 + u0, ax1 = g.refx[gi] + gdx + bbx1 + u1;
+        const int ay0 = g.refy[gi] + gdy + bby0 + v0, ay1 = g.refy[gi] + gdy + bby1 + v1;
+        if (ax0 < 0 || ay0 < 0 || ax1 >= p.cur.dimx || ay1 >= p.cur.dimy) {
+          if (tid == 0) atomicOr(&g.flags[gi], 1);
+          if (tid < kBf16KeepMax) topk[tid] = make_int2(INT_MIN, INT_MIN);
+          continue;
+        }
+      }
+      // image origin of footprint column 0 at candidate (u0, v0)
+      const int Xi = g.refx[gi] + gdx - G.half + u0, Yi = g.refy[gi] + gdy - G.half + v0;
+      for (int ys = 0; ys < G.fw; ys += G.rs) {
+        const int nr = min(G.rs, G.fw - ys);
+        if (tid == 0) {  // weight rows ys .. ys + nr - 1 by bulk copies
+          mbar_expect_tx(wbar, (uint32_t)nr * row_bytes);
+          for (int yl = 0; yl < nr; ++yl)
+            bulk_g2s(wbase + (uint32_t)((yl * G.wb + 3) * 512), slot + (size_t)(ys + yl) * G.nbf * kNRot, row_bytes,
+                     wbar);
+        }
+        // Hankel image rows ys .. ys + nr + 30
+        const int Y0 = Yi + ys, hx1 = Xi + 8 * G.hb + 6;
+        const bool inside = Y0 >= 0 && Y0 + nr + 30 < p.cur.dimy && Xi >= 0 && hx1 < p.cur.dimx;
+        for (int e = tid; e < (nr + 31) * G.hb; e += kThreads) {
+          const int rho = e / G.hb, a = e - rho * G.hb;
+          const int Y = Y0 + rho, Xa = Xi + 8 * a;
+          float px[15];
+          if (inside) {
+            const uint16_t* src = p.cur.pix + (size_t)Y * p.cur.pitch + Xa;
+#pragma unroll
+            for (int k = 0; k < 15; ++k) px[k] = __int_as_float(0x4B000000 | (int)__ldg(src + k)) - sub;
+          } else {
+            const bool rowin = Y >= 0 && Y < p.cur.dimy;
+            const uint16_t* src = p.cur.pix + (size_t)(rowin ? Y : 0) * p.cur.pitch;
+#pragma unroll
+            for (int k = 0; k < 15; ++k) {
+              const int X = Xa + k;
+              px[k] = (rowin && X >= 0 && X < p.cur.dimx) ? __int_as_float(0x4B000000 | (int)__ldg(src + X)) - sub
+                                                          : 0.0f;
+            }
+          }
+          uint32_t E[7], O[7];
+#pragma unroll
+          for (int k = 0; k < 7; ++k) {
+            E[k] = pack_bf16x2(px[2 * k], px[2 * k + 1]);
+            O[k] = pack_bf16x2(px[2 * k + 1], px[2 * k + 2]);
+          }
+          uint4* dst = reinterpret_cast<uint4*>(sH + (size_t)e * 128);
+#pragma unroll
+          for (int s = 0; s < 8; ++s) {
+            const int h = s >> 1;
+            dst[s] = (s & 1) ? make_uint4(O[h], O[h + 1], O[h + 2], O[h + 3])
+                             : make_uint4(E[h], E[h + 1], E[h + 2], E[h + 3]);
+          }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+          if (!mbar_wait(wbar, wparity)) {
+            s_err = 1;
+            atomicOr(p.error, 1);
+          } else {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            for (int yl = 0; yl < nr; ++yl)
+              for (int c = 0; c < G.nch; ++c) {
+                const uint64_t ad = make_desc(wbase + (uint32_t)((yl * G.wb + 2 * c) * 512), 512, 128);
+                const uint64_t bd =
+                    make_desc(hbase + (uint32_t)((yl * G.hb + 2 * c) * 128), 128, (uint32_t)(G.hb * 128));
+                mma_bf16(tmem, ad, bd, (ys == 0 && yl == 0 && c == 0) ? 0u : 1u);
+              }
+            mma_commit(mbar);
+          }
+        }
+        wparity ^= 1u;
+        __syncthreads();
+        if (s_err) break;
+        const bool ok = mbar_wait(mbar, parity);
+        parity ^= 1u;
+        if (!ok && tid == 0) {
+          s_err = 1;
+          atomicOr(p.error, 1);
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        __syncthreads();
+        if (s_err) break;
+      }
+      if (s_err) break;
+
+      // ---- epilogue: max over rotations, normalise, keep the best candidates
+      const int q = warp & 3, h = warp >> 2;  // TMEM lane quadrant (x shift j) and column half
+      const float* c11 = p.c11 + ((size_t)li * tiles + t) * (kTileU * kTileV);
+      float sc[4];
+#pragma unroll
+      for (int ch = 0; ch < 4; ++ch) {
+        uint32_t rv[32];
+        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(128 * h + 32 * ch), rv);
+        int mine = INT_MIN;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          const int key = lane < p.nrot ? f2key(__uint_as_float(rv[k])) : INT_MIN;
+          const int m = __reduce_max_sync(0xffffffffu, key);
+          if (lane == k) mine = m;
+        }
+        // this lane's candidate: accumulator column 128 h + 32 ch + lane
+        const int ul = 24 - 8 * q + (lane & 7), vl = 16 * h + 4 * ch + (lane >> 3);
+        float s = -INFINITY;
+        if (u0 + ul <= u1 && v0 + vl <= v1) {
+          const float var = c11[vl * kTileU + ul];
+          if (var > 0.0f) s = key2f(mine) * rsqrtf(var);
+        }
+        sc[ch] = s;
+      }
+      // per-warp best `keep`, then the block's best `keep` among them
+      for (int k = 0; k < keep; ++k) {
+        float bv = -INFINITY;
+        int bc = -1;
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch)
+          if (sc[ch] > bv) {
+            bv = sc[ch];
+            bc = ch;
+          }
+        const int key = (bc >= 0) ? f2key(bv) : INT_MIN;
+        const int mkey = __reduce_max_sync(0xffffffffu, key);
+        const unsigned who = __ballot_sync(0xffffffffu, key == mkey && bc >= 0);
+        const int wl = who ? __ffs(who) - 1 : -1;
+        int packed = -1;
+        if (lane == wl) {
+          const int ul = 24 - 8 * q + (lane & 7), vl = 16 * h + 4 * bc + (lane >> 3);
+          packed = (ul << 8) | vl;
+#pragma unroll
+          for (int ch = 0; ch < 4; ++ch)
+            if (ch == bc) sc[ch] = -INFINITY;
+        }
+        packed = __shfl_sync(0xffffffffu, packed, wl >= 0 ? wl : 0);
+        if (lane == 0) {
+          s_cv[warp * kBf16KeepMax + k] = wl >= 0 ? key2f(mkey) : -INFINITY;
+          s_ci[warp * kBf16KeepMax + k] = wl >= 0 ? packed : -1;
+        }
+      }
+      __syncthreads();
+      if (warp == 0) {
+        // 8 warps x 8 entries: this lane holds entries lane and lane + 32
+        const bool used0 = (lane & (kBf16KeepMax - 1)) < keep;
+        float cv0 = used0 ? s_cv[lane] : -INFINITY, cv1 = used0 ? s_cv[lane + 32] : -INFINITY;
+        int ci0 = used0 ? s_ci[lane] : -1, ci1 = used0 ? s_ci[lane + 32] : -1;
+        for (int k = 0; k < kBf16KeepMax; ++k) {
+          const bool sel = cv1 > cv0;
+          const float bv = sel ? cv1 : cv0;
+          const int bi = sel ? ci1 : ci0;
+          const int key = bi >= 0 ? f2key(bv) : INT_MIN;
+          const int mkey = __reduce_max_sync(0xffffffffu, key);
+          const unsigned who = __ballot_sync(0xffffffffu, key == mkey && bi >= 0);
+          const int wl = who ? __ffs(who) - 1 : -1;
+          int packed = -1;
+          if (lane == wl) {
+            packed = bi;
+            if (sel) {
+              cv1 = -INFINITY;
+              ci1 = -1;
+            } else {
+              cv0 = -INFINITY;
+              ci0 = -1;
+            }
+          }
+          packed = __shfl_sync(0xffffffffu, packed, wl >= 0 ? wl : 0);
+          if (lane == 0)
+            topk[k] = (k < keep && wl >= 0 && packed >= 0) ? make_int2(u0 + (packed >> 8), v0 + (packed & 0xff))
+                                                            : make_int2(INT_MIN, INT_MIN);
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncthreads();
+    }
+    if (s_err) break;
+  }
+  __syncthreads();
+  if (s_err && tid == 0) {  // one more bounded wait on the last armed copy and MMA phases
+    mbar_wait(wbar, wparity ^ 1u);
+    mbar_wait(mbar, parity ^ 1u);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+}
+
+// ---------------------------------------------------------------------------
+// 3. Exact rescoring: every rotation step at each kept candidate of a tile,
+//    with the exact search's integer sums and NCC expression.  One block per
+//    (grain, tile); warp w takes rotation steps w, w + 8, ..., its lanes the
+//    pattern points, all kept candidates at once.
+__global__ void __launch_bounds__(256) k_rescore_bf16(Bf16Launch p) {
+  __shared__ double s_bn[8][kBf16KeepMax];
+  __shared__ int s_bi[8][kBf16KeepMax];
+  const int item = blockIdx.x;
+  const int tiles = p.tiles_u * p.tiles_v;
+  const int li = item / tiles;
+  if (li >= *p.list_count) return;
+  const int gi = p.list[li];
+  const GrainsDev& g = p.g;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  SearchBest* rec = p.rescored + (size_t)item * kBf16KeepMax;
+  const int b = g.pstart[gi], P = g.pstart[gi + 1] - b;
+  const bool skip = g.masked[gi] || (g.flags[gi] & 7) || P <= 0 || P > kMaxPatternPoints;
+  const int2* cand = p.topk + (size_t)item * kBf16KeepMax;
+  const int NU = p.left + p.right + 1, NV = p.up + p.down + 1;
+  int nk = 0;
+  int base[kBf16KeepMax];  // pixel index of each kept candidate's anchor, -1 when none
+  int uv[kBf16KeepMax];    // (u + left) * NV + (v + up): the candidate's order index without the rotation
+  const int gdx = skip ? 0 : (int)round(g.dx[gi]), gdy = skip ? 0 : (int)round(g.dy[gi]);
+#pragma unroll
+  for (int k = 0; k < kBf16KeepMax; ++k) {
+    const int2 c = skip ? make_int2(INT_MIN, INT_MIN) : cand[k];
+    const bool ok = k < p.keep && c.x != INT_MIN;
+    base[k] = ok ? (g.refy[gi] + gdy + c.y) * p.cur.pitch + (g.refx[gi] + gdx + c.x) : -1;
+    uv[k] = ok ? (c.x + p.left) * NV + (c.y + p.up) : 0;
+    nk += ok ? 1 : 0;
+  }
+  if (skip || nk == 0) {
+    if (tid < kBf16KeepMax) rec[tid] = SearchBest{0.0, INT_MAX, 0};
+    return;
+  }
+  const long long Pl = P, S0 = g.s0[gi];
+  const double den1 = (double)(Pl * g.s00[gi] - S0 * S0);
+  const int pitch = p.cur.pitch;
+  const double base_rot = g.refrot[gi] + g.drot[gi];
+  double bn[kBf16KeepMax];
+  int bi[kBf16KeepMax];
+#pragma unroll
+  for (int k = 0; k < kBf16KeepMax; ++k) {
+    bn[k] = 0.0;
+    bi[k] = INT_MAX;
+  }
+  for (int r = warp; r < p.nrot; r += 8) {
+    double sr, cr;
+    sincos(base_rot + p.steps[r], &sr, &cr);
+    const float cf = (float)cr, sf = (float)sr;
+    unsigned s1[kBf16KeepMax];
+    unsigned long long s11[kBf16KeepMax], s01[kBf16KeepMax];
+#pragma unroll
+    for (int k = 0; k < kBf16KeepMax; ++k) {
+      s1[k] = 0;
+      s11[k] = 0;
+      s01[k] = 0;
+    }
+    for (int i = lane; i < P; i += 32) {
+      const short2 q = rotate_round_fast(g.pat[b + i], cf, sf, cr, sr);
+      const int o = (int)q.y * pitch + (int)q.x;
+      const unsigned w = g.w0[b + i];
+#pragma unroll
+      for (int k = 0; k < kBf16KeepMax; ++k) {
+        if (base[k] < 0) continue;
+        const unsigned val = __ldg(&p.cur.pix[base[k] + o]);
+        s1[k] += val;
+        s11[k] += (unsigned long long)(val * val);
+        s01[k] += (unsigned long long)(w * val);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kBf16KeepMax; ++k) {
+      if (base[k] < 0) continue;
+      unsigned long long a = s1[k], c = s11[k], d = s01[k];
+      for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+        d += __shfl_xor_sync(0xffffffffu, d, o);
+      }
+      const long long S1 = (long long)a, S11 = (long long)c, S01 = (long long)d;
+      const long long num = Pl * S01 - S0 * S1;
+      const long long d2 = Pl * S11 - S1 * S1;
+      const double ncc = (double)num / sqrt(den1 * (double)d2);
+      const int idx = r * NU * NV + uv[k];
+      if (better_b(ncc, idx, bn[k], bi[k])) {
+        bn[k] = ncc;
+        bi[k] = idx;
+      }
+    }
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < kBf16KeepMax; ++k) {
+      s_bn[warp][k] = bn[k];
+      s_bi[warp][k] = bi[k];
+    }
+  }
+  __syncthreads();
+  if (tid < kBf16KeepMax) {
+    double fn = 0.0;
+    int fi = INT_MAX;
+    for (int w = 0; w < 8; ++w)
+      if (better_b(s_bn[w][tid], s_bi[w][tid], fn, fi)) {
+        fn = s_bn[w][tid];
+        fi = s_bi[w][tid];
+      }
+    rec[tid] = SearchBest{fn, fi, 0};
+  }
+}
+
+// ---------------------------------------------------------------------------
+size_t bf16_slot_bytes(int max_r) {
+  const Geom G = geom_of(max_r);
+  return (size_t)G.fw * G.nbf * kNRot * 16;
+}
+
+bool bf16_supported(int max_r, int nrot) { return 2 * max_r + 1 < kMaxFoot && nrot >= 1 && nrot <= kNRot; }
+
+void prepare_search_bf16() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(k_search_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget);
+  cudaFuncSetAttribute(k_window_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStatsSmem);
+  done = true;
+}
+
+void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s) {
+  const int items = p.max_items;
+  k_window_stats<<<items, kStatsThreads, kStatsSmem, s>>>(p);
+  k_search_bf16<<<grid, kThreads, kSmemBudget, s>>>(p);
+  k_rescore_bf16<<<items, 256, 0, s>>>(p);
+}
+
+}  // namespace ptk
