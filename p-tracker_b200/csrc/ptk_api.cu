@@ -350,7 +350,7 @@ int search_geometry(ptk_ctx* c, int level, SearchGeom* sg) {
     prepare_search_bf16();
     sg->tiled = false;
     sg->smem = 0;
-    sg->grid = c->num_sms;
+    sg->grid = 2 * c->num_sms;  // two CTAs per SM: one's fills overlap the other's MMAs
     sg->items = (size_t)c->n * sg->tiles_u * sg->tiles_v;
     return PTK_OK;
   }
@@ -512,6 +512,7 @@ int enqueue_subpixel(ptk_ctx* c, int method, cudaStream_t s) {
     lp.max_iter = c->cfg.lm_max_iter > 0 ? c->cfg.lm_max_iter : 30;
     lp.tol = c->cfg.lm_tol > 0.0 ? c->cfg.lm_tol : 1e-6;
     lp.iters = nullptr;
+    lp.order = c->d_order;
     launch_subpix_lm(c->g, frame(c, c->cur_slot), lp, s);
   } else if (method == PTK_SUBPIX_POWELL) {
     launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, c->max_R,
@@ -583,7 +584,7 @@ int ptk_config_default(ptk_config* cfg) {
   cfg->iraz = 0;
   cfg->subpix_method = PTK_SUBPIX_POWELL;
   cfg->search_method = PTK_SEARCH_EXACT;
-  cfg->topk = 8;
+  cfg->topk = 4;
   cfg->lm_max_iter = 30;
   cfg->lm_tol = 1e-6;
   return PTK_OK;

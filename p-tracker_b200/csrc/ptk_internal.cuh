@@ -129,6 +129,7 @@ struct LmParams {
   int max_iter;
   double tol;   // step tolerance in pixels (rotation scaled by the grain radius)
   int* iters;   // optional per-grain iteration count
+  const int* order;  // grains by decreasing pattern size (one block each), or null for index order
 };
 
 // ---- host-side launchers (defined in the kernel files) ------------------

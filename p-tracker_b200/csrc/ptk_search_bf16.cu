@@ -72,7 +72,7 @@ constexpr int kThreads = 256;
 constexpr int kNRot = 32;         // rotation slots of the A operand
 constexpr int kMaxFoot = 96;      // footprint side limit (2 * half + 1 < 96)
 constexpr int kTmemCols = 256;    // 128 lanes x 256 FP32 columns: the whole tile
-constexpr int kSmemBudget = 200 * 1024;
+constexpr int kSmemBudget = 108 * 1024;  // two CTAs per SM
 constexpr long kWaitLimit = 1L << 22;
 
 // window statistics: 512 threads, prefix rows of 128 entries, runs per row
@@ -369,13 +369,13 @@ __global__ void __launch_bounds__(kStatsThreads) k_window_stats(Bf16Launch p) {
 
 // ---------------------------------------------------------------------------
 // 2. Tensor-core cross terms and the kept candidates of every tile.
-__global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
+__global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
   extern __shared__ __align__(128) unsigned char smem_bf[];
   unsigned char* smem = smem_bf;
   __shared__ __align__(8) unsigned long long s_mbar;   // MMA completion
   __shared__ __align__(8) unsigned long long s_wbar;   // weight-row bulk copies
   __shared__ uint32_t s_tmem;
-  __shared__ int s_li, s_err, s_n2, s_big, s_bb[4];
+  __shared__ int s_li, s_err, s_n2, s_bb[4];
   __shared__ double2 s_cs[kNRot];
   __shared__ float2 s_csf[kNRot];
   __shared__ float s_cv[8 * kBf16KeepMax];
@@ -411,7 +411,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     if (tid == 0) {
       s_li = atomicAdd(p.work_next, 1);
       s_n2 = 0;
-      s_big = 0;
       s_bb[0] = s_bb[2] = INT_MAX;
       s_bb[1] = s_bb[3] = INT_MIN;
     }
@@ -457,8 +456,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     const int fw2 = G.fw * G.fw;
     const int nb_max = max(1, min(p.nrot, kSmemBudget / (fw2 * 4)));
     const int rows = G.fw * G.nbf;
-    int xmn = INT_MAX, xmx = INT_MIN, ymn = INT_MAX, ymx = INT_MIN;
-    bool big = false;
     for (int r0 = 0; r0 < p.nrot; r0 += nb_max) {
       const int nb = min(nb_max, p.nrot - r0);
       for (int e = tid; e < nb * fw2; e += kThreads) fmap[e] = 0.0f;
@@ -470,15 +467,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
           const float2 cf = s_csf[r0 + k];
           const double2 cd = s_cs[r0 + k];
           const short2 q = rotate_round_fast(q0, cf.x, cf.y, cd.x, cd.y);
-          xmn = min(xmn, (int)q.x);
-          xmx = max(xmx, (int)q.x);
-          ymn = min(ymn, (int)q.y);
-          ymx = max(ymx, (int)q.y);
-          const int fx = q.x + G.half, fy = q.y + G.half;
-          if (fx >= 0 && fy >= 0 && fx < G.fw && fy < G.fw)
-            atomicAdd(&fmap[k * fw2 + fy * G.fw + fx], w);
-          else
-            big = true;
+          // |q| <= ceil(|p|) = half - 1: always inside the footprint
+          const unsigned fx = (unsigned)(q.x + G.half), fy = (unsigned)(q.y + G.half);
+          if (fx < (unsigned)G.fw && fy < (unsigned)G.fw) atomicAdd(&fmap[k * fw2 + fy * G.fw + fx], w);
         }
       }
       __syncthreads();
@@ -494,19 +485,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
       }
       __syncthreads();
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      xmn = min(xmn, __shfl_xor_sync(0xffffffffu, xmn, o));
-      xmx = max(xmx, __shfl_xor_sync(0xffffffffu, xmx, o));
-      ymn = min(ymn, __shfl_xor_sync(0xffffffffu, ymn, o));
-      ymx = max(ymx, __shfl_xor_sync(0xffffffffu, ymx, o));
-    }
-    if (lane == 0) {
-      atomicMin(&s_bb[0], xmn);
-      atomicMax(&s_bb[1], xmx);
-      atomicMin(&s_bb[2], ymn);
-      atomicMax(&s_bb[3], ymx);
-    }
-    if (big) s_big = 1;
     unsigned char* sW = smem;
     unsigned char* sH = smem + (size_t)G.rs * G.wb * 512;
     const uint32_t wbase = smem_u32(sW), hbase = smem_u32(sH);
@@ -520,14 +498,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     // slot rows (generic stores) are read next by the bulk-copy engine
     asm volatile("fence.proxy.async;" ::: "memory");
     __syncthreads();
-    if (s_big) {  // cannot happen for |offset| < half; guarded all the same
-      if (tid == 0) atomicOr(&g.flags[gi], 4);
-      for (int e = tid; e < tiles * kBf16KeepMax; e += kThreads) topk_g[e] = make_int2(INT_MIN, INT_MIN);
-      continue;
-    }
-    const int bbx0 = s_bb[0], bbx1 = s_bb[1], bby0 = s_bb[2], bby1 = s_bb[3];
+    // Bounding box of the rotated patterns: +-(half - 1) bounds it; the exact
+    // union over the rotation steps (which decides out-of-frame grains, as in
+    // the exact search) is computed only when that bound reaches the edge.
+    int bbx0 = 1 - G.half, bbx1 = G.half - 1, bby0 = 1 - G.half, bby1 = G.half - 1;
+    bool exact_bb = false;
     const float sub = 8388608.0f + rintf(mean0);  // pixel v -> (2^23 + v) - sub = v - ishift, exactly
-    const uint32_t row_bytes = (uint32_t)G.nbf * 512;
 
     for (int t = 0; t < tiles; ++t) {
       const int tu = t / p.tiles_v, tv = t - tu * p.tiles_v;
@@ -535,9 +511,42 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
       const int v0 = -p.up + tv * kTileV, v1 = min(v0 + kTileV - 1, p.down);
       int2* topk = topk_g + (size_t)t * kBf16KeepMax;
       {  // the union of the rotated footprints over the tile's candidates must stay in the frame
-        const int ax0 = g.refx[gi] + gdx + bbx0 + u0, ax1 = g.refx[gi] + gdx + bbx1 + u1;
-        const int ay0 = g.refy[gi] + gdy + bby0 + v0, ay1 = g.refy[gi] + gdy + bby1 + v1;
-        if (ax0 < 0 || ay0 < 0 || ax1 >= p.cur.dimx || ay1 >= p.cur.dimy) {
+        const int X = g.refx[gi] + gdx, Y = g.refy[gi] + gdy;
+        bool oob = X + bbx0 + u0 < 0 || Y + bby0 + v0 < 0 || X + bbx1 + u1 >= p.cur.dimx ||
+                   Y + bby1 + v1 >= p.cur.dimy;
+        if (oob && !exact_bb) {
+          int xmn = INT_MAX, xmx = INT_MIN, ymn = INT_MAX, ymx = INT_MIN;
+          for (int i = tid; i < P; i += kThreads) {
+            const short2 q0 = g.pat[b + i];
+            for (int r = 0; r < p.nrot; ++r) {
+              const short2 q = rotate_round_fast(q0, s_csf[r].x, s_csf[r].y, s_cs[r].x, s_cs[r].y);
+              xmn = min(xmn, (int)q.x);
+              xmx = max(xmx, (int)q.x);
+              ymn = min(ymn, (int)q.y);
+              ymx = max(ymx, (int)q.y);
+            }
+          }
+          for (int o = 16; o > 0; o >>= 1) {
+            xmn = min(xmn, __shfl_xor_sync(0xffffffffu, xmn, o));
+            xmx = max(xmx, __shfl_xor_sync(0xffffffffu, xmx, o));
+            ymn = min(ymn, __shfl_xor_sync(0xffffffffu, ymn, o));
+            ymx = max(ymx, __shfl_xor_sync(0xffffffffu, ymx, o));
+          }
+          if (lane == 0) {
+            atomicMin(&s_bb[0], xmn);
+            atomicMax(&s_bb[1], xmx);
+            atomicMin(&s_bb[2], ymn);
+            atomicMax(&s_bb[3], ymx);
+          }
+          __syncthreads();
+          bbx0 = s_bb[0];
+          bbx1 = s_bb[1];
+          bby0 = s_bb[2];
+          bby1 = s_bb[3];
+          exact_bb = true;
+          oob = X + bbx0 + u0 < 0 || Y + bby0 + v0 < 0 || X + bbx1 + u1 >= p.cur.dimx || Y + bby1 + v1 >= p.cur.dimy;
+        }
+        if (oob) {
           if (tid == 0) atomicOr(&g.flags[gi], 1);
           if (tid < kBf16KeepMax) topk[tid] = make_int2(INT_MIN, INT_MIN);
           continue;
@@ -547,11 +556,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
       const int Xi = g.refx[gi] + gdx - G.half + u0, Yi = g.refy[gi] + gdy - G.half + v0;
       for (int ys = 0; ys < G.fw; ys += G.rs) {
         const int nr = min(G.rs, G.fw - ys);
-        if (tid == 0) {  // weight rows ys .. ys + nr - 1 by bulk copies
-          mbar_expect_tx(wbar, (uint32_t)nr * row_bytes);
-          for (int yl = 0; yl < nr; ++yl)
-            bulk_g2s(wbase + (uint32_t)((yl * G.wb + 3) * 512), slot + (size_t)(ys + yl) * G.nbf * kNRot, row_bytes,
-                     wbar);
+        if (warp == 0) {  // weight rows ys .. ys + nr - 1: the live rotation rows of each block, bulk copies
+          if (lane == 0) mbar_expect_tx(wbar, (uint32_t)(nr * G.nbf * p.nrot * 16));
+          __syncwarp();
+          for (int e = lane; e < nr * G.nbf; e += 32) {
+            const int yl = e / G.nbf, af = e - yl * G.nbf;
+            bulk_g2s(wbase + (uint32_t)((yl * G.wb + 3 + af) * 512), slot + ((size_t)(ys + yl) * G.nbf + af) * kNRot,
+                     (uint32_t)p.nrot * 16, wbar);
+          }
         }
         // Hankel image rows ys .. ys + nr + 30
         const int Y0 = Yi + ys, hx1 = Xi + 8 * G.hb + 6;

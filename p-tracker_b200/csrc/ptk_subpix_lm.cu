@@ -16,14 +16,18 @@
 // damped normal equations are solved in FP64 and X and the cumulative grain
 // state accumulate in FP64.
 //
-// One warp per grain (4 grains per 128-thread block), shuffle reductions only.
+// One 128-thread block per grain, grains in decreasing pattern size (the
+// level-0 order) so that the large ones start first; the iteration stops when
+// the step is below the tolerance, or after two rejected steps in a row once
+// a step was accepted (the FP32 sums' noise floor: further steps only
+// re-sample it).
 #include "ptk_internal.cuh"
 
 namespace ptk {
 
 namespace {
 
-constexpr int kLmWarps = 4;
+constexpr int kLmThreads = 128;
 constexpr int kNSums = 18;
 
 // exact uint16 -> float: bits of 2^23 + v, minus 2^23
@@ -59,8 +63,11 @@ struct LmEval {
   bool clamped;
 };
 
-// Sums over the grain's points at X (all lanes return the same values).
-__device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain& o, const double X[3], int lane) {
+// Sums over the grain's points at X, reduced over the block in a fixed order
+// (every thread returns the same values).
+__device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain& o, const double X[3],
+                          double (*part)[kNSums]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double sr, cr;
   sincos(o.drot + X[2], &sr, &cr);
   const float c = (float)cr, s = (float)sr;
@@ -69,7 +76,7 @@ __device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain
 #pragma unroll
   for (int k = 0; k < kNSums; ++k) S[k] = 0.0f;
   bool clamped = false;
-  for (int i = lane; i < o.P; i += 32) {
+  for (int i = tid; i < o.P; i += kLmThreads) {
     const short2 q = g.pat0[o.b + i];
     const float x = (float)q.x, y = (float)q.y;
     const float px = bx + c * x + s * y;
@@ -119,15 +126,24 @@ __device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain
     S[16] += a * gy;
     S[17] += a * gr;
   }
-  double T[kNSums];
+  // warp sums in FP64, then the warps' partial sums in index order
 #pragma unroll
-  for (int k = 0; k < 18; ++k) {
+  for (int k = 0; k < kNSums; ++k) {
     double t = (double)S[k];
     for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+    if (lane == 0) part[warp][k] = t;
+  }
+  const int any_clamped = __syncthreads_or(clamped ? 1 : 0);
+  double T[kNSums];
+#pragma unroll
+  for (int k = 0; k < kNSums; ++k) {
+    double t = part[0][k];
+    for (int w = 1; w < kLmThreads / 32; ++w) t += part[w][k];
     T[k] = t;
   }
+  __syncthreads();  // part[] is rewritten by the next evaluation
   LmEval e;
-  e.clamped = __any_sync(0xffffffffu, clamped);
+  e.clamped = any_clamped != 0;
   const double P = (double)o.P;
   const double mv = T[0] / P;
   const double n2 = T[1] - P * mv * mv;  // sum b^2
@@ -165,10 +181,9 @@ __device__ bool lm_solve(const double H[6], const double gv[3], double lambda, d
 
 }  // namespace
 
-__global__ void __launch_bounds__(kLmWarps * 32) k_subpix_lm(GrainsDev g, FrameDev cur, LmParams lp) {
-  const int lane = threadIdx.x & 31;
-  const int gi = blockIdx.x * kLmWarps + (threadIdx.x >> 5);
-  if (gi >= g.n) return;
+__global__ void __launch_bounds__(kLmThreads) k_subpix_lm(GrainsDev g, FrameDev cur, LmParams lp) {
+  __shared__ double part[kLmThreads / 32][kNSums];
+  const int gi = lp.order ? lp.order[blockIdx.x] : (int)blockIdx.x;
   if (g.masked[gi] || (g.flags[gi] & 3)) return;
   LmGrain o;
   o.b = g.pstart[gi];
@@ -187,10 +202,10 @@ __global__ void __launch_bounds__(kLmWarps * 32) k_subpix_lm(GrainsDev g, FrameD
   const double rscale = g.radius[gi] > 1.0 ? g.radius[gi] : 1.0;  // rotation step in pixels at the rim
 
   double X[3] = {0.0, 0.0, 0.0};
-  LmEval cur_e = lm_eval(g, cur, o, X, lane);
+  LmEval cur_e = lm_eval(g, cur, o, X, part);
   bool clamped = cur_e.clamped;
   double lambda = 1e-3;
-  int it = 0;
+  int it = 0, accepted = 0, rejected_run = 0;
   if (isfinite(cur_e.F)) {
     for (it = 0; it < lp.max_iter; ++it) {
       double d[3];
@@ -202,7 +217,7 @@ __global__ void __launch_bounds__(kLmWarps * 32) k_subpix_lm(GrainsDev g, FrameD
       const double step = fmax(fmax(fabs(d[0]), fabs(d[1])), fabs(d[2]) * rscale);
       if (step < lp.tol) break;
       const double Xn[3] = {X[0] + d[0], X[1] + d[1], X[2] + d[2]};
-      const LmEval ne = lm_eval(g, cur, o, Xn, lane);
+      const LmEval ne = lm_eval(g, cur, o, Xn, part);
       if (isfinite(ne.F) && ne.F < cur_e.F) {
         X[0] = Xn[0];
         X[1] = Xn[1];
@@ -210,13 +225,16 @@ __global__ void __launch_bounds__(kLmWarps * 32) k_subpix_lm(GrainsDev g, FrameD
         cur_e = ne;
         clamped = clamped || ne.clamped;
         lambda = fmax(lambda * 0.1, 1e-12);
+        ++accepted;
+        rejected_run = 0;
       } else {
         lambda *= 10.0;
         if (lambda > 1e8) break;
+        if (++rejected_run >= 2 && accepted > 0) break;
       }
     }
   }
-  if (lane == 0) {
+  if (threadIdx.x == 0) {
     g.ncc_subpix[gi] = 1.0 - 0.5 * cur_e.F;
     g.upix[gi] += X[0];
     g.vpix[gi] += X[1];
@@ -230,11 +248,10 @@ __global__ void __launch_bounds__(kLmWarps * 32) k_subpix_lm(GrainsDev g, FrameD
 }
 
 // F = 1 - NCC and its gradient from the FP32 adjoint sums (for checks).
-__global__ void __launch_bounds__(kLmWarps * 32) k_grad_f32(GrainsDev g, FrameDev cur, const double* Xall, double* f,
-                                                           double* grad) {
-  const int lane = threadIdx.x & 31;
-  const int gi = blockIdx.x * kLmWarps + (threadIdx.x >> 5);
-  if (gi >= g.n) return;
+__global__ void __launch_bounds__(kLmThreads) k_grad_f32(GrainsDev g, FrameDev cur, const double* Xall, double* f,
+                                                        double* grad) {
+  __shared__ double part[kLmThreads / 32][kNSums];
+  const int gi = blockIdx.x;
   LmGrain o;
   o.b = g.pstart[gi];
   o.P = g.pstart[gi + 1] - o.b;
@@ -250,8 +267,8 @@ __global__ void __launch_bounds__(kLmWarps * 32) k_grad_f32(GrainsDev g, FrameDe
   o.mean0 = (float)g.mean0[gi];
   o.norm_a = sqrt(g.c0c0[gi]);
   const double X[3] = {Xall[3 * gi], Xall[3 * gi + 1], Xall[3 * gi + 2]};
-  const LmEval e = lm_eval(g, cur, o, X, lane);
-  if (lane == 0) {
+  const LmEval e = lm_eval(g, cur, o, X, part);
+  if (threadIdx.x == 0) {
     f[gi] = 1.0 - e.ncc;
     // d(1 - NCC)/dX = (1/2) dF/dX = J^T r
     grad[3 * gi] = e.gv[0];
@@ -262,13 +279,13 @@ __global__ void __launch_bounds__(kLmWarps * 32) k_grad_f32(GrainsDev g, FrameDe
 
 void launch_subpix_lm(const GrainsDev& g, const FrameDev& cur, const LmParams& lp, cudaStream_t s) {
   if (g.n <= 0) return;
-  k_subpix_lm<<<(g.n + kLmWarps - 1) / kLmWarps, kLmWarps * 32, 0, s>>>(g, cur, lp);
+  k_subpix_lm<<<g.n, kLmThreads, 0, s>>>(g, cur, lp);
 }
 
 void launch_grad_f32(const GrainsDev& g, const FrameDev& cur, const double* X, double* f, double* grad,
                      cudaStream_t s) {
   if (g.n <= 0) return;
-  k_grad_f32<<<(g.n + kLmWarps - 1) / kLmWarps, kLmWarps * 32, 0, s>>>(g, cur, X, f, grad);
+  k_grad_f32<<<g.n, kLmThreads, 0, s>>>(g, cur, X, f, grad);
 }
 
 }  // namespace ptk
