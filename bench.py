@@ -1,16 +1,27 @@
 """Benchmark of the per-grain tracking path: grains per second per frame pair.
 
 One step = one frame pair tracked through the whole per-frame pipeline of
-particle_tracking (precompute, exact pixel + rotation search, Powell subpixel,
-increments) for every grain of the workload.  Default workload: the 16-bit
-5616x3744 pair with 2000 bimodal grains (search +-15 px, 21 rotation steps),
-seeded synthetic data.
+particle_tracking (precompute, integer pixel + rotation search, subpixel
+refinement, increments) for every grain of the workload.  Default workload:
+the 16-bit 5616x3744 pair with 2000 bimodal grains (search +-15 px, 21
+rotation steps), seeded synthetic data.
 
-  value  device-resident: frames already in HBM, grain state restored on the
-         device before each step; L2 flushed (256 MiB write) before every
-         timed step; CUDA events on the context stream.
-  e2e    through the C ABI with pinned host buffers: both frames and the grain
-         records uploaded, the frame tracked, the records read back, every step.
+Forms, all on the same pair:
+  headline  BF16 tensor-core candidate ranking (tcgen05) with exact integer
+            rescoring of the kept candidates, then the adjoint
+            Levenberg-Marquardt subpixel refinement;
+  plain     exact integer search + FP64 Powell (the reference's method);
+  exact_search+adjoint_lm.
+
+  value  headline, device-resident: frames already in HBM, grain state
+         restored on the device before each step; L2 flushed (256 MiB write)
+         before every timed step; CUDA events on the context stream.
+  e2e    headline through the C ABI with pinned host buffers: both frames and
+         the grain records uploaded, the frame tracked, the records read back,
+         every step.
+  roofline  k_search_bf16 timed with CUDA events between the search kernels
+         (ptk_search_timed): 6 flops per pattern-pixel-candidate, against the
+         measured dense BF16 peak; its tensor-core flops reported beside.
 
 Multi-GPU (torchrun): one process per GPU; grains are independent, so each rank
 tracks its own pair (different seed) with no data-path collective; time is the
@@ -204,6 +215,22 @@ def run_reference_arm(args, rank: int, world: int):
     return 0
 
 
+def gemm_flops(rec: np.ndarray, nrot_slots: int = 32) -> float:
+    """Tensor-core flops of one BF16 search launch over the 32x32 candidate
+    tile of each grain: footprint rows x 16-column chunks MMAs of
+    M=128 (4 x-shifts x 32 rotation slots) x N=256 x K=16, footprint and
+    rotation-slot padding included (grain_diameter 1.0 patterns: half-extent =
+    radius + 1)."""
+    total = 0.0
+    for r in rec[:, 3]:
+        half = max(int(r), 1) + 1
+        fw = 2 * half + 1
+        nbf = (fw + 7) // 8
+        nch = (nbf + 4) // 2
+        total += fw * nch * 2.0 * 128 * 256 * 16
+    return total
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -211,7 +238,6 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg2")
-    ap.add_argument("--form", default="plain", choices=["plain"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-sample", type=int, default=48)
     ap.add_argument("--cpu-sample", type=int, default=48)
@@ -240,7 +266,9 @@ def main() -> int:
     n = pair["rec"].shape[0]
     opts = wl.tracker_options(p)
     stream = torch.cuda.Stream()
-    t = ptk.Tracker(p["dimx"], p["dimy"], rescue_level=opts["rescue_level"], NCC_min=opts["NCC_min"], iraz=1 << 30)
+    head = dict(search_method=ptk.SEARCH_BF16, subpix_method=ptk.SUBPIX_ADJOINT_LM)
+    t = ptk.Tracker(p["dimx"], p["dimy"], rescue_level=opts["rescue_level"], NCC_min=opts["NCC_min"], iraz=1 << 30,
+                    **head)
     t.set_stream(stream.cuda_stream)
     for lvl, z in enumerate(opts["zones"]):
         if z is not None:
@@ -259,12 +287,35 @@ def main() -> int:
         if world > 1:
             dist.barrier()
 
-    # ---- value: device-resident steps --------------------------------------
-    with torch.cuda.stream(stream):
+    def time_frames(steps):
+        """Device-resident frames: grain state restored on the device, L2
+        flushed, then one frame timed with events on the context stream."""
         for _ in range(args.warmup):
             t.restore_grains()
             t.track_frame(1)
         stream.synchronize()
+        total = 0.0
+        l0 = t.launches()
+        for _ in range(steps):
+            flush.zero_()
+            t.restore_grains()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t.track_frame(1)
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total / steps, t.launches() - l0
+
+    def pixel_stage():
+        t.restore_grains()
+        t.precompute()
+        t.search(0)
+        return t.get_grains()
+
+    with torch.cuda.stream(stream):
+        # ---- headline: BF16 tensor-core search + exact rescoring + adjoint LM
         barrier()
         try:
             pr = torch.cuda.get_device_properties(local)
@@ -272,58 +323,32 @@ def main() -> int:
         except Exception:
             gpu_id = str(local)
         sampler = ClockSampler(gpu_id if rank == 0 else None)
-        launches0 = t.launches()
-        total_ms = 0.0
-        for _ in range(args.steps):
-            flush.zero_()
-            t.restore_grains()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            t.track_frame(1)
-            e1.record(stream)
-            e1.synchronize()
-            total_ms += e0.elapsed_time(e1)
-        launches = t.launches() - launches0
+        ms_step, launches = time_frames(args.steps)
         barrier()
-        clocks = sampler.stop()
-        gpu_rec = t.get_grains()
+        head_rec = t.get_grains()
 
-        # ---- differentiation form: same exact search, adjoint-LM subpixel ------
-        t.configure(subpix_method=ptk.SUBPIX_ADJOINT_LM)
-        for _ in range(args.warmup):
-            t.restore_grains()
-            t.track_frame(1)
-        lm_ms = 0.0
-        for _ in range(args.steps):
-            flush.zero_()
-            t.restore_grains()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            t.track_frame(1)
-            e1.record(stream)
-            e1.synchronize()
-            lm_ms += e0.elapsed_time(e1)
-        lm_rec = t.get_grains()
-        t.configure(subpix_method=ptk.SUBPIX_POWELL)
-
-        # ---- roofline: the pixel search stage alone (k_search dominates) ----
-        zone = opts["zones"][0]
-        search_ms = []
+        # ---- per-kernel roofline of the BF16 search (CUDA events between its kernels)
+        kms = []
         for _ in range(max(3, args.steps // 2)):
             flush.zero_()
             t.restore_grains()
             t.precompute()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            t.search(0)
-            e1.record(stream)
-            e1.synchronize()
-            search_ms.append(e0.elapsed_time(e1))
+            kms.append(t.search_timed(0))
+        kms = np.median(np.array(kms), axis=0).tolist()
+        bf16_pix = pixel_stage()
 
-        # ---- e2e through the C ABI with host buffers --------------------------
+        # ---- the other forms on the same pair
+        t.configure(search_method=ptk.SEARCH_EXACT, subpix_method=ptk.SUBPIX_POWELL)
+        plain_ms, _ = time_frames(args.steps)
+        plain_rec = t.get_grains()
+        exact_pix = pixel_stage()
+        t.configure(subpix_method=ptk.SUBPIX_ADJOINT_LM)
+        lm_ms, _ = time_frames(args.steps)
+        lm_rec = t.get_grains()
+        t.configure(**head)
+        clocks = sampler.stop()  # sampled over the timed frames of all three forms
+
+        # ---- e2e: the headline form through the C ABI with host buffers
         e2e_ms = []
         rec_host = pair["rec"]
         for it in range(args.warmup + args.e2e_steps):
@@ -342,54 +367,64 @@ def main() -> int:
             if it >= args.warmup:
                 e2e_ms.append(e0.elapsed_time(e1))
 
-    ms_step = total_ms / args.steps
     e2e_step = statistics.mean(e2e_ms)
-    s_ms = statistics.median(search_ms)
-    lm_step = lm_ms / args.steps
-    ms_step, e2e_step, s_ms, lm_step = reduce_max([ms_step, e2e_step, s_ms, lm_step], world, device="cuda")
+    ms_step, e2e_step, plain_ms, lm_ms = reduce_max([ms_step, e2e_step, plain_ms, lm_ms], world, device="cuda")
 
     if rank == 0:
-        sys.path.insert(0, str(ROOT / "oracle"))
-        import bind
-        steps_list = bind.rotation_steps(zone[5], zone[4]) if bind.PORT_SO.exists() else None
-        nrot = len(steps_list) if steps_list is not None else 2 * zone[4] + 1
-        ppc = search_ppc(t, pair["rec"], zone, nrot)
-        flops = 6.0 * ppc
+        zone = opts["zones"][0]
+        nsteps = 0
+        drot = -abs(zone[5] * zone[4])
+        while drot <= abs(zone[5] * zone[4]):  # the reference's rotation loop (double)
+            nsteps += 1
+            drot += zone[5]
+        ppc = search_ppc(t, pair["rec"], zone, nsteps)
         peaks = measured_peaks()
-        achieved = flops / (s_ms * 1e-3) / 1e12
-        truth_err = np.abs(gpu_rec[:, 4:6] - pair["truth"][:, :2])
+        k_search_ms = kms[2]
+        alg = 6.0 * ppc / (k_search_ms * 1e-3) / 1e12
+        gemm = gemm_flops(pair["rec"]) / (k_search_ms * 1e-3) / 1e12
+        truth_err = np.abs(head_rec[:, 4:6] - pair["truth"][:, :2])
+        agree = np.all(bf16_pix[:, 4:7] == exact_pix[:, 4:7], axis=1)
         frame_bytes = pair["ref"].nbytes + pair["cur"].nbytes
         nn = n
         block = 16 * 8 * nn + 2 * 8 * nn + ((12 * nn + 15) // 16) * 16 + ((2 * nn + 15) // 16) * 16
         line = {
             "metric": METRIC, "value": aggregate_rate(n, world, ms_step), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int64+f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 ranking (f32 accumulate) + int64 exact rescoring + f32/f64 adjoint LM",
+            "data": "synthetic",
             "config": {"workload": f"{args.workload}: {p['dimx']}x{p['dimy']} "
                                    f"{'u16' if p['maxval'] > 255 else 'u8'}, {n} grains per GPU, search +-{zone[0]} px,"
-                                   f" {nrot} rotation steps, Powell subpixel",
-                       "form": "plain (exact integer search + FP64 Powell)", "grains_per_gpu": n,
-                       "l2": "flushed (256 MiB write) before each timed step", "parallelism": f"grain shards x{world}"},
+                                   f" {nsteps} rotation steps",
+                       "form": "BF16 tensor-core search + exact rescoring + adjoint LM (headline)",
+                       "grains_per_gpu": n, "l2": "flushed (256 MiB write) before each timed step",
+                       "parallelism": f"grain shards x{world}"},
             "e2e": {"value": aggregate_rate(n, world, e2e_step), "unit": UNIT,
                     "h2d_bytes_per_step": int(frame_bytes + block), "d2h_bytes_per_step": int(block)},
             "gpu_launches": int(launches),
-            "roofline": {"kernel": "k_search (pixel + rotation stage)", "bound": "tensor", "achieved": achieved,
-                         "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
-                         "traffic": None, "algorithmic_flop_per_launch": flops, "ppc_per_launch": int(ppc),
-                         "launch_ms": s_ms, "peak_source": peaks["source"] + " bf16 dense (burst)"},
+            "roofline": {"kernel": "k_search_bf16 (tcgen05 candidate ranking)", "bound": "tensor",
+                         "achieved": alg, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                         "frac": alg / peaks["bf16_tflops"], "traffic": None,
+                         "algorithmic_flop_per_launch": 6.0 * ppc, "ppc_per_launch": int(ppc),
+                         "tensor_flop_per_launch": gemm_flops(pair["rec"]), "tensor_tflops": gemm,
+                         "tensor_frac": gemm / peaks["bf16_tflops"], "launch_ms": k_search_ms,
+                         "search_kernels_ms": {"k_window_stats": kms[0], "k_weights_bf16": kms[1],
+                                               "k_search_bf16": kms[2], "k_rescore_bf16": kms[3]},
+                         "peak_source": peaks["source"] + " bf16 dense (burst)"},
             "accuracy": {"median_abs_err_px_vs_truth": float(np.median(truth_err)),
-                         "max_abs_err_px_vs_truth": float(truth_err.max())},
+                         "max_abs_err_px_vs_truth": float(truth_err.max()),
+                         "integer_argmax_agreement_vs_exact_search": float(agree.mean()),
+                         "max_abs_err_px_vs_plain": float(np.abs(head_rec[:, 4:6] - plain_rec[:, 4:6]).max()),
+                         "max_abs_err_rad_vs_plain": float(np.abs(head_rec[:, 6] - plain_rec[:, 6]).max())},
             "clocks": clocks,
             "forms": {
-                "plain": {"value": aggregate_rate(n, world, ms_step), "ms_per_step": ms_step,
+                "bf16_search+adjoint_lm": {"value": aggregate_rate(n, world, ms_step), "ms_per_step": ms_step},
+                "plain": {"value": aggregate_rate(n, world, plain_ms), "ms_per_step": plain_ms,
                           "search": "exact integer/FP64", "subpixel": "FP64 Powell"},
-                "exact_search+adjoint_lm": {"value": aggregate_rate(n, world, lm_step), "ms_per_step": lm_step,
-                                            "search": "exact integer/FP64",
-                                            "subpixel": "adjoint LM (FP32 samples, FP64 3x3 solve)",
+                "exact_search+adjoint_lm": {"value": aggregate_rate(n, world, lm_ms), "ms_per_step": lm_ms,
                                             "max_abs_err_px_vs_plain": float(np.abs(lm_rec[:, 4:6] -
-                                                                                    gpu_rec[:, 4:6]).max()),
-                                            "max_abs_err_rad_vs_plain": float(np.abs(lm_rec[:, 6] -
-                                                                                     gpu_rec[:, 6]).max())},
+                                                                                    plain_rec[:, 4:6]).max())},
+                "speedup_headline_vs_plain": plain_ms / ms_step,
             },
         }
         if not args.no_cpu_baseline:
@@ -397,10 +432,14 @@ def main() -> int:
             threads = cpu_threads()
             kind, times, cpu_rec = cpu_track(pair, wl, idx, threads, steps=1)
             cpu_value = len(idx) / times[0]
-            dpos = np.abs(gpu_rec[idx][:, 4:6] - cpu_rec[:, 4:6])
             line["cpu_baseline"] = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": kind,
                                     "sample": f"{len(idx)} of {n} grains (evenly spaced), full frame pipeline"}
-            line["accuracy"]["max_abs_err_px_vs_fp64_oracle"] = float(dpos.max())
+            line["accuracy"]["max_abs_err_px_vs_fp64_oracle"] = float(np.abs(head_rec[idx][:, 4:6] -
+                                                                             cpu_rec[:, 4:6]).max())
+            line["accuracy"]["max_abs_err_rad_vs_fp64_oracle"] = float(np.abs(head_rec[idx][:, 6] -
+                                                                              cpu_rec[:, 6]).max())
+            line["accuracy"]["plain_max_abs_err_px_vs_fp64_oracle"] = float(np.abs(plain_rec[idx][:, 4:6] -
+                                                                                   cpu_rec[:, 4:6]).max())
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -159,6 +159,13 @@ int ptk_read_frame(ptk_ctx* ctx, int slot, uint16_t* out);
  * ptk_subpixel replaces follow_pattern_subpixel_xyR (src/p-tracker.cpp:1090-1128). */
 int ptk_precompute(ptk_ctx* ctx);
 int ptk_search(ptk_ctx* ctx, int level);
+/* Profiling aid (no reference counterpart): ptk_search(level) with CUDA events
+ * recorded on the context stream between its search kernels; synchronizes and
+ * writes each kernel's duration in milliseconds to kernel_ms, in launch order -
+ * PTK_SEARCH_BF16: window statistics, weights, tensor-core search, rescoring
+ * (4 values); exact forms: the search kernel (1 value).  *n_kernels receives
+ * the count; max_kernels bounds what is written. */
+int ptk_search_timed(ptk_ctx* ctx, int level, float* kernel_ms, int max_kernels, int* n_kernels);
 int ptk_subpixel(ptk_ctx* ctx, int method);
 /* Increments upix = dx - dx_prev ... and, when num_image - iref >= iraz, the
  * reference change (src/p-tracker.cpp:577-611). */

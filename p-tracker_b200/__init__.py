@@ -77,6 +77,7 @@ _SIGS = {
     "ptk_read_frame": (C.c_int, [_P, C.c_int, _P]),
     "ptk_precompute": (C.c_int, [_P]),
     "ptk_search": (C.c_int, [_P, C.c_int]),
+    "ptk_search_timed": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "ptk_subpixel": (C.c_int, [_P, C.c_int]),
     "ptk_end_frame": (C.c_int, [_P, C.c_int]),
     "ptk_track_frame": (C.c_int, [_P, C.c_int]),
@@ -299,6 +300,14 @@ class Tracker:
 
     def search(self, level: int = 0):
         self._check(self._L.ptk_search(self.h, level), self.h)
+
+    def search_timed(self, level: int = 0) -> list:
+        """The level's search with CUDA events between its kernels: per-kernel
+        milliseconds in launch order (see ptk_search_timed)."""
+        ms = (C.c_float * 8)()
+        n = C.c_int(0)
+        self._check(self._L.ptk_search_timed(self.h, level, ms, 8, C.byref(n)), self.h)
+        return [float(ms[k]) for k in range(n.value)]
 
     def subpixel(self, method: int = SUBPIX_POWELL):
         self._check(self._L.ptk_subpixel(self.h, method), self.h)

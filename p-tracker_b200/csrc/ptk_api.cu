@@ -94,8 +94,11 @@ struct ptk_ctx {
   size_t best_cap{0};
 
   // BF16 tensor-core search scratch (PTK_SEARCH_BF16)
-  unsigned char* d_bf_slots{nullptr};  // per-CTA weight slots
-  size_t bf_slots_bytes{0};
+  int* d_bf_half{nullptr};             // per grain footprint half-extent
+  size_t* d_bf_wofs{nullptr};          // per grain weight-slot offset (16-byte units)
+  unsigned char* d_bf_wslots{nullptr};  // BF16 weights of every rotation step, per grain
+  size_t bf_wslots_bytes{0};
+  bool bf_geom_dirty{true};            // patterns changed since the slots were laid out
   float* d_c11{nullptr};
   int2* d_topk{nullptr};
   SearchBest* d_rescored{nullptr};
@@ -292,6 +295,7 @@ int upload_patterns(ptk_ctx* c) {
     }
   }
   c->max_dup = max_dup;
+  c->bf_geom_dirty = true;
   c->patterns_ok = true;
   for (int i = 0; i < n; ++i)
     if (c->h_pat[i].empty()) c->patterns_ok = false;
@@ -384,16 +388,39 @@ int ensure_best(ptk_ctx* c, size_t items) {
   return PTK_OK;
 }
 
-// Per-tile buffers of the BF16 search for `items` (list entries x tiles) and
-// the weight slots of `grid` CTAs.
-int ensure_bf16(ptk_ctx* c, size_t items, int grid) {
-  const size_t slots = (size_t)grid * bf16_slot_bytes(c->max_R);
-  if (slots > c->bf_slots_bytes) {
-    cudaFree(c->d_bf_slots);
-    c->d_bf_slots = nullptr;
-    c->bf_slots_bytes = 0;
-    CK(cudaMalloc(&c->d_bf_slots, slots));
-    c->bf_slots_bytes = slots;
+// Per-tile buffers of the BF16 search for `items` (list entries x tiles), and
+// the per-grain weight slots: footprint half-extent ceil(max |offset|) + 1 of
+// each pattern and the slot offsets, laid out once per pattern set.
+int ensure_bf16(ptk_ctx* c, size_t items) {
+  if (c->bf_geom_dirty) {
+    const int n = c->n;
+    std::vector<int> half(n > 0 ? n : 1, 1);
+    std::vector<size_t> wofs(n > 0 ? n : 1, 0);
+    size_t total = 0;
+    for (int i = 0; i < n; ++i) {
+      long long m2 = 0;
+      for (const short2& q : c->h_pat[i]) m2 = std::max(m2, (long long)q.x * q.x + (long long)q.y * q.y);
+      half[i] = (int)std::ceil(std::sqrt((double)m2)) + 1;
+      wofs[i] = total;
+      total += bf16_weight_entries(half[i]);
+    }
+    cudaFree(c->d_bf_half);
+    cudaFree(c->d_bf_wofs);
+    c->d_bf_half = nullptr;
+    c->d_bf_wofs = nullptr;
+    CK(cudaMalloc(&c->d_bf_half, sizeof(int) * half.size()));
+    CK(cudaMalloc(&c->d_bf_wofs, sizeof(size_t) * wofs.size()));
+    CK(cudaMemcpy(c->d_bf_half, half.data(), sizeof(int) * half.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_bf_wofs, wofs.data(), sizeof(size_t) * wofs.size(), cudaMemcpyHostToDevice));
+    const size_t bytes = std::max<size_t>(total, 1) * 16;
+    if (bytes > c->bf_wslots_bytes) {
+      cudaFree(c->d_bf_wslots);
+      c->d_bf_wslots = nullptr;
+      c->bf_wslots_bytes = 0;
+      CK(cudaMalloc(&c->d_bf_wslots, bytes));
+      c->bf_wslots_bytes = bytes;
+    }
+    c->bf_geom_dirty = false;
     invalidate(c);
   }
   if (items > c->bf_cap) {
@@ -414,17 +441,17 @@ int ensure_bf16(ptk_ctx* c, size_t items, int grid) {
 }
 
 int ensure_search_scratch(ptk_ctx* c, const SearchGeom& sg) {
-  return sg.bf16 ? ensure_bf16(c, sg.items, sg.grid) : ensure_best(c, sg.items);
+  return sg.bf16 ? ensure_bf16(c, sg.items) : ensure_best(c, sg.items);
 }
 
 // Kernels one search level launches (finalize included).
-int level_launches(const SearchGeom& sg) { return sg.bf16 ? 4 : 2; }
+int level_launches(const SearchGeom& sg) { return sg.bf16 ? 5 : 2; }
 
-int enqueue_search(ptk_ctx* c, int level, cudaStream_t s) {
+int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = nullptr) {
   SearchGeom sg;
   int rc = search_geometry(c, level, &sg);
   if (rc) return rc;
-  if (sg.bf16 ? (c->bf_cap < sg.items || !c->d_bf_slots) : (c->best_cap < sg.items))
+  if (sg.bf16 ? (c->bf_cap < sg.items || c->bf_geom_dirty) : (c->best_cap < sg.items))
     return fail(c, PTK_ERR_STATE, "search scratch not prepared");
   if (level == 0) {
     launch_stage_begin(c->g, c->d_counts, s);
@@ -451,13 +478,14 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s) {
     b.tiles_v = sg.tiles_v;
     b.keep = std::min(std::max(c->cfg.topk, 1), kBf16KeepMax);
     b.max_items = (int)sg.items;
-    b.scratch = c->d_bf_slots;
-    b.slot_bytes = bf16_slot_bytes(c->max_R);
+    b.half = c->d_bf_half;
+    b.wofs = c->d_bf_wofs;
+    b.wslots = c->d_bf_wslots;
     b.c11 = c->d_c11;
     b.topk = c->d_topk;
     b.rescored = c->d_rescored;
     b.error = c->d_counts + 3;
-    launch_search_bf16(b, sg.grid, s);
+    launch_search_bf16(b, sg.grid, s, ev);
   }
   SearchLaunch p;
   p.g = c->g;
@@ -477,10 +505,11 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s) {
   p.max_items = (int)c->best_cap;
   if (sg.bf16) {
     // rescored records: [list entry][tile][kBf16KeepMax]
-  } else if (sg.tiled) {
-    launch_search_tiled(p, c->max_R, sg.grid, sg.smem, s);
   } else {
-    launch_search(p, sg.grid, sg.smem, s);
+    if (ev) cudaEventRecord(ev[0], s);
+    if (sg.tiled) launch_search_tiled(p, c->max_R, sg.grid, sg.smem, s);
+    else launch_search(p, sg.grid, sg.smem, s);
+    if (ev) cudaEventRecord(ev[1], s);
   }
   FinalizeLaunch f;
   f.g = c->g;
@@ -526,7 +555,6 @@ int enqueue_subpixel(ptk_ctx* c, int method, cudaStream_t s) {
 
 int prepare_searches(ptk_ctx* c) {
   size_t need = 0, need_bf = 0;
-  int grid_bf = 0;
   for (int level = 0; level < 3; ++level) {
     if (level > c->cfg.rescue_level) break;
     SearchGeom sg;
@@ -534,13 +562,12 @@ int prepare_searches(ptk_ctx* c) {
     if (rc) return rc;
     if (sg.bf16) {
       need_bf = std::max(need_bf, sg.items);
-      grid_bf = std::max(grid_bf, sg.grid);
     } else {
       need = std::max(need, sg.items);
     }
   }
   if (need_bf) {
-    int rc = ensure_bf16(c, need_bf, grid_bf);
+    int rc = ensure_bf16(c, need_bf);
     if (rc) return rc;
   }
   return ensure_best(c, need ? need : 1);
@@ -651,7 +678,9 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_lists);
   cudaFree(c->d_work);
   cudaFree(c->d_best);
-  cudaFree(c->d_bf_slots);
+  cudaFree(c->d_bf_half);
+  cudaFree(c->d_bf_wofs);
+  cudaFree(c->d_bf_wslots);
   cudaFree(c->d_c11);
   cudaFree(c->d_topk);
   cudaFree(c->d_rescored);
@@ -931,6 +960,38 @@ int ptk_search(ptk_ctx* c, int level) {
   if ((rc = ensure_search_scratch(c, sg))) return rc;
   if ((rc = enqueue_search(c, level, c->stream))) return rc;
   CK(cudaGetLastError());
+  return PTK_OK;
+}
+
+int ptk_search_timed(ptk_ctx* c, int level, float* kernel_ms, int max_kernels, int* n_kernels) {
+  if (!c || level < 0 || level > 2 || !n_kernels || (max_kernels > 0 && !kernel_ms))
+    return fail(c, PTK_ERR_ARG, "bad argument");
+  int rc = check_ready(c, true);
+  if (rc) return rc;
+  if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
+  SearchGeom sg;
+  if ((rc = search_geometry(c, level, &sg))) return rc;
+  if ((rc = ensure_search_scratch(c, sg))) return rc;
+  cudaEvent_t ev[5] = {};
+  const int nev = sg.bf16 ? 5 : 2;
+  for (int k = 0; k < nev; ++k) {
+    cudaError_t e = cudaEventCreate(&ev[k]);
+    if (e != cudaSuccess) {
+      for (int j = 0; j < k; ++j) cudaEventDestroy(ev[j]);
+      return cuda_fail(c, e, "cudaEventCreate");
+    }
+  }
+  rc = enqueue_search(c, level, c->stream, ev);
+  cudaError_t e = rc ? cudaSuccess : cudaStreamSynchronize(c->stream);
+  *n_kernels = nev - 1;
+  for (int k = 0; !rc && e == cudaSuccess && k + 1 < nev; ++k) {
+    float ms = 0.0f;
+    e = cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+    if (k < max_kernels) kernel_ms[k] = ms;
+  }
+  for (int k = 0; k < nev; ++k) cudaEventDestroy(ev[k]);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(c, e, "search timing");
   return PTK_OK;
 }
 

@@ -109,8 +109,9 @@ struct Bf16Launch {
   int tiles_u, tiles_v;
   int keep;                 // candidates per tile rescored exactly (1..kBf16KeepMax)
   int max_items;            // list capacity x tiles: grid of the per-tile kernels
-  unsigned char* scratch;   // per-CTA BF16 weight slots
-  size_t slot_bytes;
+  const int* half;          // per grain: footprint half-extent ceil(max |offset|) + 1
+  const size_t* wofs;       // per grain: offset of its weight slot in wslots (16-byte units)
+  unsigned char* wslots;    // BF16 weights of every rotation step, per grain
   float* c11;               // [list entry][tile][32 x 32] window variance
   int2* topk;               // [list entry][tile][kBf16KeepMax] kept (u, v), INT_MIN when none
   SearchBest* rescored;     // [list entry][tile][kBf16KeepMax] exact best per kept candidate
@@ -146,9 +147,10 @@ int search_tiled_occupancy(size_t smem, int max_r);
 void launch_search_tiled(const SearchLaunch& p, int max_r, int grid, size_t smem, cudaStream_t s);
 void launch_finalize(const FinalizeLaunch& p, int n_grains, cudaStream_t s);
 bool bf16_supported(int max_r, int nrot);
-size_t bf16_slot_bytes(int max_r);
+size_t bf16_weight_entries(int half);
 void prepare_search_bf16();
-void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s);
+// ev (optional, 5 events): recorded before the first kernel and after each of the four
+void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent_t* ev = nullptr);
 void launch_end_frame(const GrainsDev& g, int swap_reference, cudaStream_t s);
 void prepare_subpix(int max_points, int max_r);
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& ref,

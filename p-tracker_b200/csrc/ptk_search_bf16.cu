@@ -73,7 +73,14 @@ constexpr int kNRot = 32;         // rotation slots of the A operand
 constexpr int kMaxFoot = 96;      // footprint side limit (2 * half + 1 < 96)
 constexpr int kTmemCols = 256;    // 128 lanes x 256 FP32 columns: the whole tile
 constexpr int kSmemBudget = 108 * 1024;  // two CTAs per SM
+// Kept candidates: the tile's best approximate score and those within 2 % of
+// it (up to `keep`).  On the 5616x3744 2000-grain workload the exact best lies
+// at most 0.05 % below the approximate best.
+constexpr float kKeepRel = 0.02f;
 constexpr long kWaitLimit = 1L << 22;
+// weights kernel: 512 threads, 64 KB of float maps (three blocks per SM)
+constexpr int kWThreads = 512;
+constexpr int kWSmem = 64 * 1024;
 
 // window statistics: 512 threads, prefix rows of 128 entries, runs per row
 constexpr int kStatsThreads = 512;
@@ -368,6 +375,70 @@ __global__ void __launch_bounds__(kStatsThreads) k_window_stats(Bf16Launch p) {
 }
 
 // ---------------------------------------------------------------------------
+// 2a. BF16 weights of every rotation step of a grain (one block per list
+//     entry): the pattern rotated by each step, scattered with the centred
+//     reference values I0 - mean0 into float maps (coinciding points add up),
+//     written to the grain's weight slot as [footprint row][8-column block]
+//     [rotation][8 values].  As many rotations per pass as maps fit in shared
+//     memory.
+__global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double2 s_cs[kNRot];
+  __shared__ float2 s_csf[kNRot];
+  const int li = blockIdx.x;
+  if (li >= *p.list_count) return;
+  const GrainsDev& g = p.g;
+  const int gi = p.list[li];
+  const int b = g.pstart[gi], P = g.pstart[gi + 1] - b;
+  if (g.masked[gi] || (g.flags[gi] & 2) || P <= 0 || P > kMaxPatternPoints) return;
+  const Geom G = geom_of(p.half[gi]);
+  if (G.fw >= kMaxFoot) return;  // excluded by the host's geometry check
+  const int tid = threadIdx.x;
+  uint4* slot = reinterpret_cast<uint4*>(p.wslots) + p.wofs[gi];
+  const double base_rot = g.refrot[gi] + g.drot[gi];  // total_rot = base_rot + step, as the exact search
+  if (tid < p.nrot) {
+    double sr, cr;
+    sincos(base_rot + p.steps[tid], &sr, &cr);
+    s_cs[tid] = make_double2(cr, sr);
+    s_csf[tid] = make_float2((float)cr, (float)sr);
+  }
+  const float mean0 = (float)g.mean0[gi];
+  float* fmap = reinterpret_cast<float*>(smem);
+  const int fw2 = G.fw * G.fw;
+  const int nb_max = max(1, min(p.nrot, kWSmem / (fw2 * 4)));
+  const int rows = G.fw * G.nbf;
+  for (int r0 = 0; r0 < p.nrot; r0 += nb_max) {
+    const int nb = min(nb_max, p.nrot - r0);
+    for (int e = tid; e < nb * fw2; e += kWThreads) fmap[e] = 0.0f;
+    __syncthreads();
+    for (int i = tid; i < P; i += kWThreads) {
+      const short2 q0 = g.pat[b + i];
+      const float w = small_i2f((int)g.w0[b + i]) - mean0;
+      for (int k = 0; k < nb; ++k) {
+        const float2 cf = s_csf[r0 + k];
+        const double2 cd = s_cs[r0 + k];
+        const short2 q = rotate_round_fast(q0, cf.x, cf.y, cd.x, cd.y);
+        // |q| <= ceil(|p|) = half - 1: always inside the footprint
+        const unsigned fx = (unsigned)(q.x + G.half), fy = (unsigned)(q.y + G.half);
+        if (fx < (unsigned)G.fw && fy < (unsigned)G.fw) atomicAdd(&fmap[k * fw2 + fy * G.fw + fx], w);
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < nb * rows; e += kWThreads) {
+      const int rem = e / nb, k = e - rem * nb;
+      const int y = rem / G.nbf, af = rem - y * G.nbf;
+      const float* src = fmap + k * fw2 + y * G.fw + 8 * af;
+      float v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = (8 * af + j < G.fw) ? src[j] : 0.0f;
+      slot[(size_t)rem * kNRot + r0 + k] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
+                                                      pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // 2. Tensor-core cross terms and the kept candidates of every tile.
 __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
   extern __shared__ __align__(128) unsigned char smem_bf[];
@@ -375,14 +446,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
   __shared__ __align__(8) unsigned long long s_mbar;   // MMA completion
   __shared__ __align__(8) unsigned long long s_wbar;   // weight-row bulk copies
   __shared__ uint32_t s_tmem;
-  __shared__ int s_li, s_err, s_n2, s_bb[4];
+  __shared__ int s_li, s_err, s_bb[4];
   __shared__ double2 s_cs[kNRot];
   __shared__ float2 s_csf[kNRot];
   __shared__ float s_cv[8 * kBf16KeepMax];
   __shared__ int s_ci[8 * kBf16KeepMax];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t mbar = smem_u32(&s_mbar), wbar = smem_u32(&s_wbar);
-  uint4* slot = reinterpret_cast<uint4*>(p.scratch + (size_t)blockIdx.x * p.slot_bytes);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -410,7 +480,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
     __syncthreads();  // every thread is done with the previous grain's shared state
     if (tid == 0) {
       s_li = atomicAdd(p.work_next, 1);
-      s_n2 = 0;
       s_bb[0] = s_bb[2] = INT_MAX;
       s_bb[1] = s_bb[3] = INT_MIN;
     }
@@ -424,67 +493,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
       for (int e = tid; e < tiles * kBf16KeepMax; e += kThreads) topk_g[e] = make_int2(INT_MIN, INT_MIN);
       continue;
     }
-    // footprint half-extent from the pattern's largest norm; rotation cos/sin
-    const double base_rot = g.refrot[gi] + g.drot[gi];  // total_rot = base_rot + step, as the exact search
-    {
-      int n2 = 0;
-      for (int i = tid; i < P; i += kThreads) {
-        const short2 q = g.pat[b + i];
-        n2 = max(n2, (int)q.x * q.x + (int)q.y * q.y);
-      }
-      atomicMax(&s_n2, n2);
-      if (tid < p.nrot) {
-        double sr, cr;
-        sincos(base_rot + p.steps[tid], &sr, &cr);
-        s_cs[tid] = make_double2(cr, sr);
-        s_csf[tid] = make_float2((float)cr, (float)sr);
-      }
+    // rotation cos/sin (total_rot = base_rot + step, as the exact search) and
+    // the grain's footprint geometry
+    const double base_rot = g.refrot[gi] + g.drot[gi];
+    if (tid < p.nrot) {
+      double sr, cr;
+      sincos(base_rot + p.steps[tid], &sr, &cr);
+      s_cs[tid] = make_double2(cr, sr);
+      s_csf[tid] = make_float2((float)cr, (float)sr);
     }
-    __syncthreads();
-    const Geom G = geom_of((int)ceil(sqrt((double)s_n2)) + 1);
-    if (G.fw >= kMaxFoot) {  // excluded by the host's geometry check
-      if (tid == 0) atomicOr(&g.flags[gi], 4);
-      for (int e = tid; e < tiles * kBf16KeepMax; e += kThreads) topk_g[e] = make_int2(INT_MIN, INT_MIN);
-      continue;
-    }
+    const Geom G = geom_of(p.half[gi]);
     const float mean0 = (float)g.mean0[gi];
     const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
-
-    // ---- phase 1: BF16 weights of every rotation into the scratch slot,
-    //      as many rotations per pass as float maps fit in shared memory
-    float* fmap = reinterpret_cast<float*>(smem);
-    const int fw2 = G.fw * G.fw;
-    const int nb_max = max(1, min(p.nrot, kSmemBudget / (fw2 * 4)));
-    const int rows = G.fw * G.nbf;
-    for (int r0 = 0; r0 < p.nrot; r0 += nb_max) {
-      const int nb = min(nb_max, p.nrot - r0);
-      for (int e = tid; e < nb * fw2; e += kThreads) fmap[e] = 0.0f;
-      __syncthreads();
-      for (int i = tid; i < P; i += kThreads) {
-        const short2 q0 = g.pat[b + i];
-        const float w = small_i2f((int)g.w0[b + i]) - mean0;
-        for (int k = 0; k < nb; ++k) {
-          const float2 cf = s_csf[r0 + k];
-          const double2 cd = s_cs[r0 + k];
-          const short2 q = rotate_round_fast(q0, cf.x, cf.y, cd.x, cd.y);
-          // |q| <= ceil(|p|) = half - 1: always inside the footprint
-          const unsigned fx = (unsigned)(q.x + G.half), fy = (unsigned)(q.y + G.half);
-          if (fx < (unsigned)G.fw && fy < (unsigned)G.fw) atomicAdd(&fmap[k * fw2 + fy * G.fw + fx], w);
-        }
-      }
-      __syncthreads();
-      for (int e = tid; e < nb * rows; e += kThreads) {
-        const int rem = e / nb, k = e - rem * nb;
-        const int y = rem / G.nbf, af = rem - y * G.nbf;
-        const float* src = fmap + k * fw2 + y * G.fw + 8 * af;
-        float v[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = (8 * af + j < G.fw) ? src[j] : 0.0f;
-        slot[(size_t)rem * kNRot + r0 + k] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
-                                                        pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
-      }
-      __syncthreads();
-    }
+    const uint4* slot = reinterpret_cast<const uint4*>(p.wslots) + p.wofs[gi];
     unsigned char* sW = smem;
     unsigned char* sH = smem + (size_t)G.rs * G.wb * 512;
     const uint32_t wbase = smem_u32(sW), hbase = smem_u32(sH);
@@ -495,8 +516,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
       const int a = zb < 3 ? zb : zb + G.nbf;
       reinterpret_cast<uint4*>(sW)[((size_t)yl * G.wb + a) * kNRot + r] = make_uint4(0, 0, 0, 0);
     }
-    // slot rows (generic stores) are read next by the bulk-copy engine
-    asm volatile("fence.proxy.async;" ::: "memory");
     __syncthreads();
     // Bounding box of the rotated patterns: +-(half - 1) bounds it; the exact
     // union over the rotation steps (which decides out-of-frame grains, as in
@@ -565,39 +584,29 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
                      (uint32_t)p.nrot * 16, wbar);
           }
         }
-        // Hankel image rows ys .. ys + nr + 30
-        const int Y0 = Yi + ys, hx1 = Xi + 8 * G.hb + 6;
-        const bool inside = Y0 >= 0 && Y0 + nr + 30 < p.cur.dimy && Xi >= 0 && hx1 < p.cur.dimx;
-        for (int e = tid; e < (nr + 31) * G.hb; e += kThreads) {
-          const int rho = e / G.hb, a = e - rho * G.hb;
-          const int Y = Y0 + rho, Xa = Xi + 8 * a;
-          float px[15];
-          if (inside) {
-            const uint16_t* src = p.cur.pix + (size_t)Y * p.cur.pitch + Xa;
-#pragma unroll
-            for (int k = 0; k < 15; ++k) px[k] = __int_as_float(0x4B000000 | (int)__ldg(src + k)) - sub;
-          } else {
-            const bool rowin = Y >= 0 && Y < p.cur.dimy;
-            const uint16_t* src = p.cur.pix + (size_t)(rowin ? Y : 0) * p.cur.pitch;
-#pragma unroll
-            for (int k = 0; k < 15; ++k) {
-              const int X = Xa + k;
-              px[k] = (rowin && X >= 0 && X < p.cur.dimx) ? __int_as_float(0x4B000000 | (int)__ldg(src + X)) - sub
-                                                          : 0.0f;
-            }
-          }
-          uint32_t E[7], O[7];
-#pragma unroll
-          for (int k = 0; k < 7; ++k) {
-            E[k] = pack_bf16x2(px[2 * k], px[2 * k + 1]);
-            O[k] = pack_bf16x2(px[2 * k + 1], px[2 * k + 2]);
-          }
-          uint4* dst = reinterpret_cast<uint4*>(sH + (size_t)e * 128);
-#pragma unroll
-          for (int s = 0; s < 8; ++s) {
-            const int h = s >> 1;
-            dst[s] = (s & 1) ? make_uint4(O[h], O[h + 1], O[h + 2], O[h + 3])
-                             : make_uint4(E[h], E[h + 1], E[h + 2], E[h + 3]);
+        // Hankel image rows ys .. ys + nr + 30.  Entry (block a, shift s) of a
+        // row is the 8-pixel window starting at column x = 8 a + s, stored at
+        // byte 16 x: a warp fills one row, 25 windows per pass, lane x loading
+        // pixel x and taking pixels x + 1 .. x + 7 from the next lanes, so the
+        // 16-byte stores of a pass are contiguous.
+        const int Y0 = Yi + ys, nwin = 8 * G.hb;
+        const bool inside = Y0 >= 0 && Y0 + nr + 30 < p.cur.dimy && Xi >= 0 && Xi + nwin + 6 < p.cur.dimx;
+        for (int rho = warp; rho < nr + 31; rho += kThreads / 32) {
+          const int Y = Y0 + rho;
+          const bool rowin = Y >= 0 && Y < p.cur.dimy;
+          const uint16_t* src = p.cur.pix + (size_t)(rowin ? Y : 0) * p.cur.pitch;
+          unsigned char* drow = sH + (size_t)rho * G.hb * 128;
+          for (int x0 = 0; x0 < nwin; x0 += 25) {
+            const int x = x0 + lane, X = Xi + x;
+            float f = 0.0f;
+            if (x < nwin + 7 && (inside || (rowin && X >= 0 && X < p.cur.dimx)))
+              f = __int_as_float(0x4B000000 | (int)__ldg(src + X)) - sub;
+            const float f1 = __shfl_down_sync(0xffffffffu, f, 1);
+            const uint32_t p0 = pack_bf16x2(f, f1);
+            const uint32_t p2 = __shfl_down_sync(0xffffffffu, p0, 2);
+            const uint32_t p4 = __shfl_down_sync(0xffffffffu, p0, 4);
+            const uint32_t p6 = __shfl_down_sync(0xffffffffu, p0, 6);
+            if (lane < 25 && x < nwin) *reinterpret_cast<uint4*>(drow + 16 * x) = make_uint4(p0, p2, p4, p6);
           }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -619,16 +628,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
           }
         }
         wparity ^= 1u;
-        __syncthreads();
-        if (s_err) break;
-        const bool ok = mbar_wait(mbar, parity);
-        parity ^= 1u;
-        if (!ok && tid == 0) {
-          s_err = 1;
-          atomicOr(p.error, 1);
+        // one thread waits for the MMAs; the others rest at the barrier
+        if (tid == 0 && !s_err) {
+          if (!mbar_wait(mbar, parity)) {
+            s_err = 1;
+            atomicOr(p.error, 1);
+          }
+          asm volatile("tcgen05.fence::before_thread_sync;");
         }
-        asm volatile("tcgen05.fence::after_thread_sync;");
+        parity ^= 1u;
         __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
         if (s_err) break;
       }
       if (s_err) break;
@@ -691,13 +701,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
         const bool used0 = (lane & (kBf16KeepMax - 1)) < keep;
         float cv0 = used0 ? s_cv[lane] : -INFINITY, cv1 = used0 ? s_cv[lane + 32] : -INFINITY;
         int ci0 = used0 ? s_ci[lane] : -1, ci1 = used0 ? s_ci[lane + 32] : -1;
+        float top = -INFINITY;
         for (int k = 0; k < kBf16KeepMax; ++k) {
           const bool sel = cv1 > cv0;
           const float bv = sel ? cv1 : cv0;
           const int bi = sel ? ci1 : ci0;
           const int key = bi >= 0 ? f2key(bv) : INT_MIN;
           const int mkey = __reduce_max_sync(0xffffffffu, key);
-          const unsigned who = __ballot_sync(0xffffffffu, key == mkey && bi >= 0);
+          if (k == 0) top = key2f(mkey);
+          // candidates scoring more than kKeepRel below the tile's best are not rescored
+          const bool near = !(top > 0.0f) || key2f(mkey) >= top * (1.0f - kKeepRel);
+          const unsigned who = near ? __ballot_sync(0xffffffffu, key == mkey && bi >= 0) : 0u;
           const int wl = who ? __ffs(who) - 1 : -1;
           int packed = -1;
           if (lane == wl) {
@@ -790,17 +804,22 @@ __global__ void __launch_bounds__(256) k_rescore_bf16(Bf16Launch p) {
       s11[k] = 0;
       s01[k] = 0;
     }
-    for (int i = lane; i < P; i += 32) {
-      const short2 q = rotate_round_fast(g.pat[b + i], cf, sf, cr, sr);
-      const int o = (int)q.y * pitch + (int)q.x;
-      const unsigned w = g.w0[b + i];
+    // two points per lane per pass: both points' loads are in flight together
+    for (int i = lane; i < P; i += 64) {
+      const bool two = i + 32 < P;
+      const short2 qa = rotate_round_fast(g.pat[b + i], cf, sf, cr, sr);
+      const short2 qb = two ? rotate_round_fast(g.pat[b + i + 32], cf, sf, cr, sr) : qa;
+      const int oa = (int)qa.y * pitch + (int)qa.x, ob = (int)qb.y * pitch + (int)qb.x;
+      const unsigned wa = g.w0[b + i], wb = two ? (unsigned)g.w0[b + i + 32] : 0u;
 #pragma unroll
       for (int k = 0; k < kBf16KeepMax; ++k) {
         if (base[k] < 0) continue;
-        const unsigned val = __ldg(&p.cur.pix[base[k] + o]);
-        s1[k] += val;
-        s11[k] += (unsigned long long)(val * val);
-        s01[k] += (unsigned long long)(w * val);
+        const uint16_t* px = p.cur.pix + base[k];
+        const unsigned va = __ldg(px + oa);
+        const unsigned vb = two ? (unsigned)__ldg(px + ob) : 0u;
+        s1[k] += va + vb;
+        s11[k] += (unsigned long long)(va * va) + (unsigned long long)(vb * vb);
+        s01[k] += (unsigned long long)(wa * va) + (unsigned long long)(wb * vb);
       }
     }
 #pragma unroll
@@ -844,9 +863,9 @@ __global__ void __launch_bounds__(256) k_rescore_bf16(Bf16Launch p) {
 }
 
 // ---------------------------------------------------------------------------
-size_t bf16_slot_bytes(int max_r) {
-  const Geom G = geom_of(max_r);
-  return (size_t)G.fw * G.nbf * kNRot * 16;
+size_t bf16_weight_entries(int half) {
+  const Geom G = geom_of(half);
+  return (size_t)G.fw * G.nbf * kNRot;
 }
 
 bool bf16_supported(int max_r, int nrot) { return 2 * max_r + 1 < kMaxFoot && nrot >= 1 && nrot <= kNRot; }
@@ -856,14 +875,21 @@ void prepare_search_bf16() {
   if (done) return;
   cudaFuncSetAttribute(k_search_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget);
   cudaFuncSetAttribute(k_window_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStatsSmem);
+  cudaFuncSetAttribute(k_weights_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, kWSmem);
   done = true;
 }
 
-void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s) {
+void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent_t* ev) {
   const int items = p.max_items;
+  if (ev) cudaEventRecord(ev[0], s);
   k_window_stats<<<items, kStatsThreads, kStatsSmem, s>>>(p);
+  if (ev) cudaEventRecord(ev[1], s);
+  k_weights_bf16<<<p.max_items / (p.tiles_u * p.tiles_v), kWThreads, kWSmem, s>>>(p);
+  if (ev) cudaEventRecord(ev[2], s);
   k_search_bf16<<<grid, kThreads, kSmemBudget, s>>>(p);
+  if (ev) cudaEventRecord(ev[3], s);
   k_rescore_bf16<<<items, 256, 0, s>>>(p);
+  if (ev) cudaEventRecord(ev[4], s);
 }
 
 }  // namespace ptk
