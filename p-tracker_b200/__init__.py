@@ -78,6 +78,9 @@ _SIGS = {
     "ptk_precompute": (C.c_int, [_P]),
     "ptk_search": (C.c_int, [_P, C.c_int]),
     "ptk_search_timed": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
+    "ptk_read_image_file": (C.c_int, [C.c_char_p, _P, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_char_p,
+                                      C.c_int]),
+    "ptk_image_error": (C.c_char_p, []),
     "ptk_subpixel": (C.c_int, [_P, C.c_int]),
     "ptk_end_frame": (C.c_int, [_P, C.c_int]),
     "ptk_track_frame": (C.c_int, [_P, C.c_int]),
@@ -390,5 +393,27 @@ def save_grains_file(path: str, rec13: np.ndarray, from_image: str = "", to_imag
         raise PtkError(rc, f"cannot write {path}")
 
 
+def read_image_file(path: str) -> tuple[np.ndarray, str]:
+    """Grey levels of an image file as the tracking path reads it
+    (ptk_read_image_file): a (rows, columns) uint16 array and the TIFF DateTime
+    (or "dateTime unknown")."""
+    L = lib()
+    w, h = C.c_int(), C.c_int()
+    rc = L.ptk_read_image_file(str(path).encode(), None, 0, C.byref(w), C.byref(h), None, 0)
+    if rc != PTK_OK:
+        raise PtkError(rc, L.ptk_image_error().decode())
+    out = np.zeros((h.value, w.value), dtype=np.uint16)
+    when = C.create_string_buffer(256)
+    rc = L.ptk_read_image_file(str(path).encode(), _ptr(out), out.size, C.byref(w), C.byref(h), when, 256)
+    if rc != PTK_OK:
+        raise PtkError(rc, L.ptk_image_error().decode())
+    return out, when.value.decode()
+
+
+def cli_path() -> Path:
+    """The command-file driver (ptracker_b200), built next to libptk.so."""
+    return Path(__file__).resolve().parent / "ptracker_b200"
+
+
 __all__ = ["Tracker", "Config", "Zone", "Grain", "GRAIN_DTYPE", "COLUMNS", "lib", "synth", "PtkError",
-           "read_grains_file", "save_grains_file", "abi_sizes", "exported_symbols"]
+           "read_grains_file", "save_grains_file", "read_image_file", "cli_path", "abi_sizes", "exported_symbols"]

@@ -2,6 +2,7 @@
 
     libptk.so        C-ABI tracking path (CUDA kernels for sm_100a + host runtime)
     libptk_synth.so  seeded synthetic frame generator (host, OpenMP)
+    ptracker_b200    command-file driver of the tracking procedure (links libptk.so)
 
 Every .cu file is compiled by nvcc for sm_100a only
 (-gencode arch=compute_100a,code=sm_100a); the remap kernels are compiled with
@@ -29,7 +30,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-O3", "--expt-relaxed-constexpr"]
 NO_FMA = {"ptk_remap.cu"}
 CU_SOURCES = ["ptk_search.cu", "ptk_search_tiled.cu", "ptk_search_bf16.cu", "ptk_subpix_lm.cu", "ptk_subpix.cu", "ptk_remap.cu", "ptk_api.cu", "ptk_noalloc.cu"]
-CXX_SOURCES = ["grainfile.cpp"]
+CXX_SOURCES = ["grainfile.cpp", "imageio.cpp"]
 
 
 def _host_cxx() -> str:
@@ -93,9 +94,14 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> dict:
     s = CSRC / "synth.cpp"
     if _stale(synth, [s]):
         _run([cxx, "-O3", "-fopenmp", "-std=c++17", "-fPIC", "-shared", str(s), "-o", str(synth)])
+    cli = HERE / "ptracker_b200"
+    s = CSRC / "ptracker_cli.cpp"
+    if _stale(cli, [s, lib] + hdrs):
+        _run([cxx, "-O2", "-std=c++17", "-I", str(INCLUDE), str(s), "-o", str(cli), "-L", str(HERE), "-lptk",
+              "-Wl,-rpath,$ORIGIN", "-pthread"])
     if verbose:
-        print(f"built {lib} and {synth} ({len(jobs)} objects recompiled)")
-    return {"libptk": str(lib), "libptk_synth": str(synth), "recompiled": len(jobs)}
+        print(f"built {lib}, {synth} and {cli} ({len(jobs)} objects recompiled)")
+    return {"libptk": str(lib), "libptk_synth": str(synth), "cli": str(cli), "recompiled": len(jobs)}
 
 
 if __name__ == "__main__":

@@ -1,0 +1,241 @@
+// Image files of the C ABI (include/ptk.h): the grey levels the tracking path
+// works on, read from disk on the host.
+//
+// The reference reads frames with libtiff's RGBA reader and converts every
+// pixel to one uint16 grey level (src/p-tracker.cpp:86-187):
+//     r, g, b = 8-bit channel * (1 / 255)          (double)
+//     grey    = (uint16)(65535 * (0.299 r + 0.587 g + 0.114 b))
+// with the rows restored to top-down order.  libtiff is not part of this
+// build, so an uncompressed baseline TIFF is decoded here and its samples go
+// through the same 8-bit channels the RGBA reader produces: 8-bit grey v ->
+// (v, v, v) (MinIsWhite: 255 - v), 16-bit grey -> its high byte, 16-bit
+// colour channels -> (v + 128) / 257, 8-bit RGB / RGBA as stored.  Binary
+// PGM (P5) frames are an addition of this build and are returned as stored.
+#include <cctype>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "../../include/ptk.h"
+
+namespace {
+
+struct Reader {
+  std::vector<unsigned char> d;
+  bool le = true;
+  bool ok(size_t off, size_t n) const { return off <= d.size() && n <= d.size() - off; }
+  uint16_t u16(size_t o) const {
+    return le ? (uint16_t)(d[o] | (d[o + 1] << 8)) : (uint16_t)((d[o] << 8) | d[o + 1]);
+  }
+  uint32_t u32(size_t o) const {
+    return le ? (uint32_t)d[o] | ((uint32_t)d[o + 1] << 8) | ((uint32_t)d[o + 2] << 16) | ((uint32_t)d[o + 3] << 24)
+              : ((uint32_t)d[o] << 24) | ((uint32_t)d[o + 1] << 16) | ((uint32_t)d[o + 2] << 8) | (uint32_t)d[o + 3];
+  }
+};
+
+struct Entry {
+  uint16_t type = 0;
+  uint32_t count = 0;
+  size_t at = 0;  // file offset of the first value
+};
+
+size_t type_size(uint16_t t) {
+  switch (t) {
+    case 1: case 2: case 6: case 7: return 1;
+    case 3: case 8: return 2;
+    case 4: case 9: case 11: return 4;
+    case 5: case 10: case 12: return 8;
+    default: return 0;
+  }
+}
+
+// k-th value of an integer entry (BYTE / SHORT / LONG)
+bool value(const Reader& r, const Entry& e, uint32_t k, uint32_t* v) {
+  const size_t s = type_size(e.type);
+  if (k >= e.count || (e.type != 1 && e.type != 3 && e.type != 4)) return false;
+  const size_t o = e.at + (size_t)k * s;
+  if (!r.ok(o, s)) return false;
+  *v = e.type == 1 ? r.d[o] : (e.type == 3 ? r.u16(o) : r.u32(o));
+  return true;
+}
+
+uint16_t grey_of(double R, double G, double B) {
+  const double fact = 1.0 / 255.0;
+  const double rr = R * fact, gg = G * fact, bb = B * fact;
+  return (uint16_t)(65535.0 * (0.299 * rr + 0.587 * gg + 0.114 * bb));
+}
+
+int read_tiff(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, std::string* when,
+              std::string* err) {
+  r.le = r.d[0] == 'I';
+  if (r.u16(2) != 42) return (*err = "not a TIFF file", PTK_ERR_IO);
+  const size_t ifd = r.u32(4);
+  if (!r.ok(ifd, 2)) return (*err = "truncated TIFF header", PTK_ERR_IO);
+  const int n = r.u16(ifd);
+  if (!r.ok(ifd + 2, (size_t)n * 12)) return (*err = "truncated TIFF directory", PTK_ERR_IO);
+  bool have[400] = {};  // baseline tags only (all below 400)
+  Entry ent[400];
+  for (int i = 0; i < n; ++i) {
+    const size_t o = ifd + 2 + (size_t)i * 12;
+    const uint16_t t = r.u16(o);
+    if (t >= 400) continue;
+    Entry e;
+    e.type = r.u16(o + 2);
+    e.count = r.u32(o + 4);
+    const size_t bytes = type_size(e.type) * (size_t)e.count;
+    e.at = bytes <= 4 ? o + 8 : r.u32(o + 8);
+    ent[t] = e;
+    have[t] = true;
+  }
+  auto get = [&](int t, uint32_t dflt) -> uint32_t {
+    uint32_t v = dflt;
+    if (have[t] && !value(r, ent[t], 0, &v)) v = dflt;
+    return v;
+  };
+  const uint32_t w = get(256, 0), h = get(257, 0);
+  const uint32_t spp = get(277, 1), comp = get(259, 1), photo = get(262, 1), planar = get(284, 1);
+  const uint32_t orient = get(274, 1), fmt = get(339, 1);
+  uint32_t bps = 8;
+  if (have[258] && !value(r, ent[258], 0, &bps)) bps = 8;
+  if (w == 0 || h == 0 || w > 65535 || h > 65535) return (*err = "bad TIFF image size", PTK_ERR_IO);
+  if (comp != 1) return (*err = "compressed TIFF is not supported (baseline uncompressed only)", PTK_ERR_IO);
+  if (planar != 1 || orient != 1 || fmt != 1)
+    return (*err = "TIFF layout not supported (chunky, top-left, unsigned samples only)", PTK_ERR_IO);
+  if (bps != 8 && bps != 16) return (*err = "TIFF sample depth must be 8 or 16 bits", PTK_ERR_IO);
+  const bool grey = photo == 0 || photo == 1;
+  if (!(grey && spp >= 1) && !(photo == 2 && spp >= 3))
+    return (*err = "TIFF photometric interpretation not supported (grey or RGB)", PTK_ERR_IO);
+  if (!have[273] || !have[279]) return (*err = "TIFF without strips", PTK_ERR_IO);
+  *dimx = (int)w;
+  *dimy = (int)h;
+  if (have[306]) {
+    const Entry& e = ent[306];
+    if (r.ok(e.at, e.count)) {
+      std::string s(reinterpret_cast<const char*>(&r.d[e.at]), e.count);
+      const size_t z = s.find('\0');
+      *when = z == std::string::npos ? s : s.substr(0, z);
+    }
+  }
+  if (!out) return PTK_OK;
+  if (capacity < (size_t)w * h) return (*err = "output buffer too small", PTK_ERR_ARG);
+  // the strips, concatenated, hold the rows top-down
+  const size_t bpp = (size_t)spp * (bps / 8), row_bytes = bpp * w;
+  std::vector<unsigned char> pix;
+  pix.reserve(row_bytes * h);
+  for (uint32_t k = 0; k < ent[273].count; ++k) {
+    uint32_t off = 0, len = 0;
+    if (!value(r, ent[273], k, &off) || !value(r, ent[279], k, &len) || !r.ok(off, len))
+      return (*err = "truncated TIFF strip", PTK_ERR_IO);
+    pix.insert(pix.end(), r.d.begin() + off, r.d.begin() + off + len);
+  }
+  if (pix.size() < row_bytes * h) return (*err = "TIFF strips shorter than the image", PTK_ERR_IO);
+  auto sample = [&](size_t o) -> uint32_t {
+    return bps == 8 ? pix[o] : (r.le ? (uint32_t)(pix[o] | (pix[o + 1] << 8)) : (uint32_t)((pix[o] << 8) | pix[o + 1]));
+  };
+  for (uint32_t y = 0; y < h; ++y)
+    for (uint32_t x = 0; x < w; ++x) {
+      const size_t o = (size_t)y * row_bytes + (size_t)x * bpp;
+      double R, G, B;
+      if (grey) {
+        uint32_t v = sample(o);
+        if (bps == 16) v >>= 8;  // the RGBA reader keeps the high byte of 16-bit grey
+        if (photo == 0) v = 255 - v;
+        R = G = B = v;
+      } else {
+        uint32_t c[3];
+        for (int k = 0; k < 3; ++k) {
+          c[k] = sample(o + k * (bps / 8));
+          if (bps == 16) c[k] = (c[k] + 128) / 257;
+        }
+        R = c[0];
+        G = c[1];
+        B = c[2];
+      }
+      out[(size_t)y * w + x] = grey_of(R, G, B);
+    }
+  return PTK_OK;
+}
+
+int read_pgm(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, std::string* err) {
+  size_t p = 2;
+  auto next = [&](long* v) -> bool {
+    while (p < r.d.size()) {
+      if (r.d[p] == '#') {
+        while (p < r.d.size() && r.d[p] != '\n') ++p;
+      } else if (std::isspace(r.d[p])) {
+        ++p;
+      } else {
+        break;
+      }
+    }
+    long x = 0;
+    bool any = false;
+    while (p < r.d.size() && r.d[p] >= '0' && r.d[p] <= '9') {
+      x = x * 10 + (r.d[p++] - '0');
+      any = true;
+      if (x > 1000000) return false;
+    }
+    *v = x;
+    return any;
+  };
+  long w, h, maxv;
+  if (!next(&w) || !next(&h) || !next(&maxv) || w <= 0 || h <= 0 || w > 65535 || h > 65535 || maxv <= 0 ||
+      maxv > 65535)
+    return (*err = "bad PGM header", PTK_ERR_IO);
+  ++p;  // the single whitespace after maxval
+  *dimx = (int)w;
+  *dimy = (int)h;
+  if (!out) return PTK_OK;
+  if (capacity < (size_t)w * h) return (*err = "output buffer too small", PTK_ERR_ARG);
+  const size_t bpp = maxv < 256 ? 1 : 2;
+  if (!r.ok(p, (size_t)w * h * bpp)) return (*err = "truncated PGM data", PTK_ERR_IO);
+  for (size_t i = 0; i < (size_t)w * h; ++i)
+    out[i] = bpp == 1 ? r.d[p + i] : (uint16_t)((r.d[p + 2 * i] << 8) | r.d[p + 2 * i + 1]);
+  return PTK_OK;
+}
+
+thread_local std::string g_image_error;
+
+}  // namespace
+
+extern "C" {
+
+int ptk_read_image_file(const char* path, uint16_t* out, size_t capacity, int* dimx, int* dimy, char* datetime,
+                        int datetime_len) {
+  if (!path || !dimx || !dimy) return PTK_ERR_ARG;
+  Reader r;
+  {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) {
+      g_image_error = std::string("cannot open ") + path;
+      return PTK_ERR_IO;
+    }
+    r.d.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+  }
+  std::string when = "dateTime unknown", err;
+  int rc;
+  if (r.d.size() >= 8 && ((r.d[0] == 'I' && r.d[1] == 'I') || (r.d[0] == 'M' && r.d[1] == 'M'))) {
+    rc = read_tiff(r, out, capacity, dimx, dimy, &when, &err);
+  } else if (r.d.size() >= 2 && r.d[0] == 'P' && r.d[1] == '5') {
+    rc = read_pgm(r, out, capacity, dimx, dimy, &err);
+  } else {
+    rc = PTK_ERR_IO;
+    err = "unknown image format (uncompressed TIFF or binary PGM)";
+  }
+  if (rc) {
+    g_image_error = std::string(path) + ": " + err;
+    return rc;
+  }
+  if (datetime && datetime_len > 0) {
+    std::strncpy(datetime, when.c_str(), (size_t)datetime_len - 1);
+    datetime[datetime_len - 1] = '\0';
+  }
+  return PTK_OK;
+}
+
+const char* ptk_image_error(void) { return g_image_error.c_str(); }
+
+}  // extern "C"
