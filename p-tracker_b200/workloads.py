@@ -51,7 +51,7 @@ PRESETS["cfg5"] = dict(dimx=5616, dimy=3744, maxval=65535, n=5000, mix=[(1.0, 8.
                        density=0.02, amp=(60.0 * 256, 220.0 * 256), bg=10.0 * 256, noise=2.0 * 256, disp=0.0,
                        rot=0.0, zone=15, num_rot=10, inc_rot=0.005, rescue_zone=40, frames=50, shear=60.0,
                        rot_walk=0.01, jump=25.0, jump_frac=0.03,
-                       disto=(-2e-9, 1e-16))
+                       disto=(-2e-9, 1e-16), gap=20.0)  # 5000 grains fit; a jump may overlap a neighbour by <= 5 px
 
 
 def _threads() -> int:
@@ -74,7 +74,7 @@ def place(p: dict, seed: int, n: int | None = None):
     margin = max(p["zone"], p.get("rescue_zone", 0)) + p["disp"] + 6.0 + p.get("jump", 0.0) + p.get("shear", 0.0) * 0.5
     if p.get("disto"):
         margin += 40.0
-    gap = 2.0 * p["disp"] + 6.0 + (2.0 * p.get("jump", 0.0) if p.get("jump") else 0.0)
+    gap = p.get("gap", 2.0 * p["disp"] + 6.0 + (2.0 * p.get("jump", 0.0) if p.get("jump") else 0.0))
     got = L.ptk_synth_place(C.c_int(p["dimx"]), C.c_int(p["dimy"]), C.c_int(n), C.c_int(len(mix)), _dp(w),
                             _dp(rlo), _dp(rhi), C.c_double(p["sig"][0]), C.c_double(p["sig"][1]),
                             C.c_double(margin), C.c_double(gap), C.c_uint64(seed), _dp(cx), _dp(cy), _dp(r),
@@ -189,3 +189,21 @@ def sequence_motion(p: dict, grains: dict, seed: int):
         dyk = dyk + np.where(j, p["jump"] * np.sin(ang), 0.0)
         out.append((dxk, dyk, rot[k]))
     return out, jumpers, jump_frame
+
+
+def make_sequence(name_or_params, seed: int = 1, frames: int | None = None) -> dict:
+    """Frames of a cfg5-style sequence: the preset's grains moved by
+    sequence_motion (shear field, rotation walk, jumps), rendered through the
+    preset's radial distortion when it has one.  Returns the uint16 frames, the
+    start records, the 14 undistor parameters (or None), the motion and the
+    jumpers."""
+    p = dict(PRESETS[name_or_params] if isinstance(name_or_params, str) else name_or_params)
+    if frames is not None:
+        p["frames"] = frames
+    grains = place(p, seed)
+    motion, jumpers, jump_frame = sequence_motion(p, grains, seed)
+    disto = distortion_params(p) if p.get("disto") else None
+    out = [render(p, grains, dx, dy, th, noise_seed=seed * 1000 + k, disto=disto)
+           for k, (dx, dy, th) in enumerate(motion)]
+    return dict(params=p, frames=out, rec=start_records(grains), grains=grains, disto=disto, motion=motion,
+                jumpers=jumpers, jump_frame=jump_frame)
