@@ -96,7 +96,7 @@ typedef struct ptk_config {
   int32_t iraz;                  /* reference change period, default 0        */
   int32_t subpix_method;         /* PTK_SUBPIX_*, default POWELL              */
   int32_t search_method;         /* PTK_SEARCH_*, default EXACT               */
-  int32_t topk;                  /* BF16 search: candidates per 32x32 tile rescored exactly (1..8, default 4) */
+  int32_t topk;                  /* BF16 search: candidates per 32x32 tile rescored exactly, those within 3 % of its best score (1..8, default 8) */
   int32_t lm_max_iter;           /* adjoint LM: iteration cap                 */
   double lm_tol;                 /* adjoint LM: step tolerance (pixels)       */
 } ptk_config;

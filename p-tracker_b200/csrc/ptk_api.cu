@@ -88,7 +88,7 @@ struct ptk_ctx {
 
   // lists: counts[0] = n (level-0 list), counts[1] rescue, counts[2] super-rescue
   int* d_counts{nullptr};
-  int* d_lists{nullptr};  // [rescue n][super n]
+  int* d_lists{nullptr};  // [rescue n][super n][exact re-search n]
   int* d_work{nullptr};
   SearchBest* d_best{nullptr};
   size_t best_cap{0};
@@ -99,7 +99,6 @@ struct ptk_ctx {
   unsigned char* d_bf_wslots{nullptr};  // BF16 weights of every rotation step, per grain
   size_t bf_wslots_bytes{0};
   bool bf_geom_dirty{true};            // patterns changed since the slots were laid out
-  float* d_c11{nullptr};
   int2* d_topk{nullptr};
   SearchBest* d_rescored{nullptr};
   size_t bf_cap{0};  // (list entries x tiles) the per-tile buffers hold
@@ -338,7 +337,7 @@ struct SearchGeom {
   bool bf16;   // BF16 tensor-core candidate search + exact rescoring
 };
 
-int search_geometry(ptk_ctx* c, int level, SearchGeom* sg) {
+int search_geometry(ptk_ctx* c, int level, SearchGeom* sg, bool allow_bf16 = true) {
   const ptk_zone& z = c->cfg.zone[level];
   sg->nrot = (int)c->steps[level].size();
   sg->nu = z.left + z.right + 1;
@@ -349,12 +348,12 @@ int search_geometry(ptk_ctx* c, int level, SearchGeom* sg) {
   if (sg->items > (size_t)INT32_MAX) return fail(c, PTK_ERR_LIMIT, "too many search work items");
   // The BF16 form covers footprints up to 95 px and 32 rotation steps; other
   // geometries take the exact kernels (same results, exact ranking).
-  sg->bf16 = c->cfg.search_method == PTK_SEARCH_BF16 && bf16_supported(c->max_R, sg->nrot);
+  sg->bf16 = allow_bf16 && c->cfg.search_method == PTK_SEARCH_BF16 && bf16_supported(c->max_R, sg->nrot);
   if (sg->bf16) {
     prepare_search_bf16();
     sg->tiled = false;
     sg->smem = 0;
-    sg->grid = 2 * c->num_sms;  // two CTAs per SM: one's fills overlap the other's MMAs
+    sg->grid = c->num_sms;  // one CTA per SM: the whole tensor memory holds both accumulators
     sg->items = (size_t)c->n * sg->tiles_u * sg->tiles_v;
     return PTK_OK;
   }
@@ -424,14 +423,11 @@ int ensure_bf16(ptk_ctx* c, size_t items) {
     invalidate(c);
   }
   if (items > c->bf_cap) {
-    cudaFree(c->d_c11);
     cudaFree(c->d_topk);
     cudaFree(c->d_rescored);
-    c->d_c11 = nullptr;
     c->d_topk = nullptr;
     c->d_rescored = nullptr;
     c->bf_cap = 0;
-    CK(cudaMalloc(&c->d_c11, sizeof(float) * kTileU * kTileV * items));
     CK(cudaMalloc(&c->d_topk, sizeof(int2) * kBf16KeepMax * items));
     CK(cudaMalloc(&c->d_rescored, sizeof(SearchBest) * kBf16KeepMax * items));
     c->bf_cap = items;
@@ -440,18 +436,29 @@ int ensure_bf16(ptk_ctx* c, size_t items) {
   return PTK_OK;
 }
 
-int ensure_search_scratch(ptk_ctx* c, const SearchGeom& sg) {
-  return sg.bf16 ? ensure_bf16(c, sg.items) : ensure_best(c, sg.items);
+// A BF16 level also needs the exact kernels' scratch: the grains it rejects
+// are searched again exactly.
+int ensure_search_scratch(ptk_ctx* c, int level, const SearchGeom& sg) {
+  if (!sg.bf16) return ensure_best(c, sg.items);
+  SearchGeom sx;
+  int rc = search_geometry(c, level, &sx, false);
+  if (rc) return rc;
+  if ((rc = ensure_best(c, sx.items))) return rc;
+  return ensure_bf16(c, sg.items);
 }
 
-// Kernels one search level launches (finalize included).
-int level_launches(const SearchGeom& sg) { return sg.bf16 ? 5 : 2; }
+// Kernels one search level launches (finalizes included): BF16 weights,
+// search, rescore and finalize, then the exact search and finalize of the
+// grains the BF16 pass rejected.
+int level_launches(const SearchGeom& sg) { return sg.bf16 ? 6 : 2; }
 
 int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = nullptr) {
   SearchGeom sg;
   int rc = search_geometry(c, level, &sg);
   if (rc) return rc;
-  if (sg.bf16 ? (c->bf_cap < sg.items || c->bf_geom_dirty) : (c->best_cap < sg.items))
+  SearchGeom sx = sg;  // the exact kernels' geometry (a BF16 level's re-search)
+  if (sg.bf16 && (rc = search_geometry(c, level, &sx, false))) return rc;
+  if ((sg.bf16 && (c->bf_cap < sg.items || c->bf_geom_dirty)) || c->best_cap < sx.items)
     return fail(c, PTK_ERR_STATE, "search scratch not prepared");
   if (level == 0) {
     launch_stage_begin(c->g, c->d_counts, s);
@@ -459,8 +466,19 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
   }
   const int* list = level == 0 ? c->d_order : (level == 1 ? c->d_lists : c->d_lists + c->n);
   const int* count = c->d_counts + level;
-  CK(cudaMemsetAsync(c->d_work, 0, sizeof(int), s));
+  CK(cudaMemsetAsync(c->d_work, 0, 2 * sizeof(int), s));
   const ptk_zone& z = c->cfg.zone[level];
+  FinalizeLaunch f;
+  f.g = c->g;
+  f.steps = c->d_steps[level];
+  f.left = z.left;
+  f.up = z.up;
+  f.nu = sg.nu;
+  f.nv = sg.nv;
+  f.tiles = sg.tiles_u * sg.tiles_v;
+  f.level = level;
+  f.NCC_min = c->cfg.NCC_min;
+  f.NCC_min_super = c->cfg.NCC_min_super;
   if (sg.bf16) {
     Bf16Launch b;
     b.g = c->g;
@@ -481,51 +499,50 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
     b.half = c->d_bf_half;
     b.wofs = c->d_bf_wofs;
     b.wslots = c->d_bf_wslots;
-    b.c11 = c->d_c11;
     b.topk = c->d_topk;
     b.rescored = c->d_rescored;
     b.error = c->d_counts + 3;
     launch_search_bf16(b, sg.grid, s, ev);
+    // The ranking finds the exact best wherever it is a match; a grain the
+    // level rejects (best below the threshold, among candidates that all
+    // match poorly) is searched again exactly, so that its recorded NCC and
+    // its acceptance are the exact search's.
+    f.list = list;
+    f.list_count = count;
+    f.nrot = kBf16KeepMax;  // rescored records per tile
+    f.best = c->d_rescored;
+    f.redo = 1;
+    f.out_list = c->d_lists + 2 * (size_t)c->n;
+    f.out_count = c->d_counts + 4 + level;
+    launch_finalize(f, c->n, s);
+    list = f.out_list;
+    count = f.out_count;
   }
   SearchLaunch p;
   p.g = c->g;
   p.cur = frame(c, c->cur_slot);
   p.list = list;
   p.list_count = count;
-  p.work_next = c->d_work;
+  p.work_next = c->d_work + 1;
   p.steps = c->d_steps[level];
-  p.nrot = sg.nrot;
+  p.nrot = sx.nrot;
   p.left = z.left;
   p.right = z.right;
   p.up = z.up;
   p.down = z.down;
-  p.tiles_u = sg.tiles_u;
-  p.tiles_v = sg.tiles_v;
+  p.tiles_u = sx.tiles_u;
+  p.tiles_v = sx.tiles_v;
   p.best = c->d_best;
   p.max_items = (int)c->best_cap;
-  if (sg.bf16) {
-    // rescored records: [list entry][tile][kBf16KeepMax]
-  } else {
-    if (ev) cudaEventRecord(ev[0], s);
-    if (sg.tiled) launch_search_tiled(p, c->max_R, sg.grid, sg.smem, s);
-    else launch_search(p, sg.grid, sg.smem, s);
-    if (ev) cudaEventRecord(ev[1], s);
-  }
-  FinalizeLaunch f;
-  f.g = c->g;
+  if (ev && !sg.bf16) cudaEventRecord(ev[0], s);
+  if (sx.tiled) launch_search_tiled(p, c->max_R, sx.grid, sx.smem, s);
+  else launch_search(p, sx.grid, sx.smem, s);
+  if (ev && !sg.bf16) cudaEventRecord(ev[1], s);
   f.list = list;
   f.list_count = count;
-  f.steps = c->d_steps[level];
-  f.nrot = sg.bf16 ? kBf16KeepMax : sg.nrot;  // records per tile
-  f.left = z.left;
-  f.up = z.up;
-  f.nu = sg.nu;
-  f.nv = sg.nv;
-  f.tiles = sg.tiles_u * sg.tiles_v;
-  f.best = sg.bf16 ? c->d_rescored : c->d_best;
-  f.level = level;
-  f.NCC_min = c->cfg.NCC_min;
-  f.NCC_min_super = c->cfg.NCC_min_super;
+  f.nrot = sx.nrot;
+  f.best = c->d_best;
+  f.redo = 0;
   f.out_list = level == 0 ? c->d_lists : c->d_lists + c->n;
   f.out_count = c->d_counts + (level == 0 ? 1 : 2);
   launch_finalize(f, c->n, s);
@@ -562,6 +579,9 @@ int prepare_searches(ptk_ctx* c) {
     if (rc) return rc;
     if (sg.bf16) {
       need_bf = std::max(need_bf, sg.items);
+      SearchGeom sx;  // the exact re-search of the grains a BF16 level rejects
+      if ((rc = search_geometry(c, level, &sx, false))) return rc;
+      need = std::max(need, sx.items);
     } else {
       need = std::max(need, sg.items);
     }
@@ -611,7 +631,7 @@ int ptk_config_default(ptk_config* cfg) {
   cfg->iraz = 0;
   cfg->subpix_method = PTK_SUBPIX_POWELL;
   cfg->search_method = PTK_SEARCH_EXACT;
-  cfg->topk = 4;
+  cfg->topk = 8;
   cfg->lm_max_iter = 30;
   cfg->lm_tol = 1e-6;
   return PTK_OK;
@@ -644,10 +664,12 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
     if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(frame)"));
     cudaMemset(c->d_img[k], 0, bytes);
   }
-  e = cudaMalloc(&c->d_counts, 4 * sizeof(int));
+  // counts: [0] grains, [1] rescue list, [2] super-rescue list, [3] error flag,
+  // [4 + level] exact re-search list of a BF16 level
+  e = cudaMalloc(&c->d_counts, 8 * sizeof(int));
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(counts)"));
-  cudaMemset(c->d_counts, 0, 4 * sizeof(int));
-  e = cudaMalloc(&c->d_work, sizeof(int));
+  cudaMemset(c->d_counts, 0, 8 * sizeof(int));
+  e = cudaMalloc(&c->d_work, 2 * sizeof(int));  // work-queue heads of the BF16 and exact kernels
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(work)"));
   for (int l = 0; l < 3; ++l) {
     int rc = build_steps(c, l);
@@ -681,7 +703,6 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_bf_half);
   cudaFree(c->d_bf_wofs);
   cudaFree(c->d_bf_wslots);
-  cudaFree(c->d_c11);
   cudaFree(c->d_topk);
   cudaFree(c->d_rescored);
   cudaFree(c->d_map);
@@ -730,7 +751,7 @@ int ptk_set_grains(ptk_ctx* c, const ptk_grain* grains, int n) {
     c->n = n;
     BlockLayout L(n);
     CK(cudaMalloc(&c->d_block, L.total));
-    CK(cudaMalloc(&c->d_lists, sizeof(int) * 2 * (n > 0 ? n : 1)));
+    CK(cudaMalloc(&c->d_lists, sizeof(int) * 3 * (n > 0 ? n : 1)));
     c->h_pat.assign(n, std::vector<short2>());
     c->patterns_ok = false;
     cudaFree(c->d_best);
@@ -957,7 +978,7 @@ int ptk_search(ptk_ctx* c, int level) {
   if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
   SearchGeom sg;
   if ((rc = search_geometry(c, level, &sg))) return rc;
-  if ((rc = ensure_search_scratch(c, sg))) return rc;
+  if ((rc = ensure_search_scratch(c, level, sg))) return rc;
   if ((rc = enqueue_search(c, level, c->stream))) return rc;
   CK(cudaGetLastError());
   return PTK_OK;
@@ -971,9 +992,9 @@ int ptk_search_timed(ptk_ctx* c, int level, float* kernel_ms, int max_kernels, i
   if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
   SearchGeom sg;
   if ((rc = search_geometry(c, level, &sg))) return rc;
-  if ((rc = ensure_search_scratch(c, sg))) return rc;
+  if ((rc = ensure_search_scratch(c, level, sg))) return rc;
   cudaEvent_t ev[5] = {};
-  const int nev = sg.bf16 ? 5 : 2;
+  const int nev = sg.bf16 ? 4 : 2;
   for (int k = 0; k < nev; ++k) {
     cudaError_t e = cudaEventCreate(&ev[k]);
     if (e != cudaSuccess) {

@@ -90,8 +90,9 @@ struct FinalizeLaunch {
   const SearchBest* best;
   int level;
   double NCC_min, NCC_min_super;
-  int* out_list;   // next-level list (rescue / super-rescue)
+  int* out_list;   // next-level list (rescue / super-rescue), or the re-search list
   int* out_count;
+  int redo;        // 1: rejected grains go to out_list for an exact re-search of this level, unmarked
 };
 
 // BF16 tensor-core search: kept candidates per tile (upper bound of `keep`).
@@ -112,7 +113,6 @@ struct Bf16Launch {
   const int* half;          // per grain: footprint half-extent ceil(max |offset|) + 1
   const size_t* wofs;       // per grain: offset of its weight slot in wslots (16-byte units)
   unsigned char* wslots;    // BF16 weights of every rotation step, per grain
-  float* c11;               // [list entry][tile][32 x 32] window variance
   int2* topk;               // [list entry][tile][kBf16KeepMax] kept (u, v), INT_MIN when none
   SearchBest* rescored;     // [list entry][tile][kBf16KeepMax] exact best per kept candidate
   int* error;               // set when a bounded wait gave up

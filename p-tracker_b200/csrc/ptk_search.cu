@@ -94,12 +94,13 @@ __global__ void k_precompute(GrainsDev g, FrameDev ref) {
 }
 
 // reset() + backup() of every grain at the start of the pixel stage
-// (src/p-tracker.cpp:478-479) and zeroing of the rescue-list counters.
+// (src/p-tracker.cpp:478-479) and zeroing of the list counters.
 __global__ void k_stage_begin(GrainsDev g, int* counts) {
   const int gi = blockIdx.x * blockDim.x + threadIdx.x;
   if (gi == 0) {
     counts[1] = 0;
     counts[2] = 0;
+    counts[4] = counts[5] = counts[6] = 0;  // exact re-search lists of BF16 levels
   }
   if (gi >= g.n) return;
   g.ncc[gi] = 0.0;
@@ -357,21 +358,29 @@ __global__ void k_finalize(FinalizeLaunch p) {
     g.ncc[gi] = bn;
     g.ncc_rescue[gi] = bn;
     accept = !(bn < p.NCC_min);
+  } else if (p.level == 1) {
+    g.ncc_rescue[gi] = bn;
+    accept = !(bn < p.NCC_min_super);
+  } else {
+    g.ncc_rescue[gi] = bn;
+    accept = bn > p.NCC_min_super;
+  }
+  if (!accept && p.redo) {  // decided by the exact re-search of this level
+    p.out_list[atomicAdd(p.out_count, 1)] = gi;
+    return;
+  }
+  if (p.level == 0) {
     if (!accept) {
       p.out_list[atomicAdd(p.out_count, 1)] = gi;
       g.status[gi] |= PTK_ST_RESCUED;
     }
   } else if (p.level == 1) {
-    g.ncc_rescue[gi] = bn;
-    accept = !(bn < p.NCC_min_super);
     if (!accept) {
       p.out_list[atomicAdd(p.out_count, 1)] = gi;
       g.status[gi] |= PTK_ST_SUPER_RESCUED | PTK_ST_FAILED;
     }
-  } else {
-    g.ncc_rescue[gi] = bn;
-    accept = bn > p.NCC_min_super;
-    if (accept) g.status[gi] &= (uint8_t)~PTK_ST_FAILED;
+  } else if (accept) {
+    g.status[gi] &= (uint8_t)~PTK_ST_FAILED;
   }
   if (accept) {
     const double rest_dx = g.dx[gi] - gdx;

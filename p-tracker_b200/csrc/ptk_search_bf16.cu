@@ -6,51 +6,57 @@
 // x offset, y offset), ranked on exact integer sums.  The tensor cores only
 // decide WHERE to look; every value that reaches the acceptance rule is exact.
 //
-//  1. k_window_stats (CUDA cores): per candidate (u, v) of a 32x32 tile, the
-//     window variance C11 = S11 - S1^2 / P of the current frame under
-//     pattern0_rotated, from row prefix sums over the pattern's runs of equal
-//     multiplicity (S1 exact in integers, S11 in FP32 - it only normalises
-//     the ranking).
-//  2. k_search_bf16 (tcgen05): the cross terms for every rotation step r at
-//     every candidate,
-//         D_r(u, v) = sum_i (I0_i - mean0) * I1(X + u + q_r,i.x, Y + v + q_r,i.y),
+//  1. k_weights_bf16: per grain and rotation step r, the pattern rotated as
+//     the exact search rotates it (rotate_pixel_pattern), scattered into two
+//     maps over the footprint: W_r, the centred reference values
+//     I0_i - mean0 (coinciding points add up), and M_r, the multiplicity of
+//     each footprint pixel.  Both are stored in BF16 (M_r exactly).
+//  2. k_search_bf16 (tcgen05): for every rotation step r and candidate
+//     c = (u, v) of a 32 x 32 tile, two correlations with the current frame I1,
+//         D_r(c) = sum_x W_r(x) I1(x + c)              (the NCC's cross term)
+//         S_r(c) = sum_x M_r(x) (I1(x + c) - m)^2      (m = rint(mean0))
 //     in BF16 with FP32 accumulation in tensor memory, and per candidate the
-//     approximate score max_r D_r / sqrt(C11).  The best `keep` candidates of
-//     each tile are written out.
+//     ranking score max_r D_r / sqrt(S_r).  Because the window's variance
+//     under the rotated footprint is S_r minus a non-negative mean term,
+//     D_r / sqrt(S_r) is a lower bound of NCC_r * sqrt(C0C0) that no footprint
+//     difference between rotation steps can inflate, and it is tight when the
+//     window's mean is close to the reference pattern's.  The best candidates
+//     of each tile (within kKeepRel of its best score) are written out.
 //  3. k_rescore_bf16 (CUDA cores, exact integers): every rotation step at each
 //     kept candidate, with the exact search's sums and NCC expression, giving
 //     per-candidate best records in the reference's order; the level's usual
 //     finalize applies the acceptance rule to them.
 //
 // Tensor-core formulation of step 2 (one work item = one grain, persistent
-// CTAs, one per SM, 256 threads):
-//   * A operand (M = 128 = 4 x-shifts j by 32 rotation slots r, K = 16
-//     footprint columns): the rotated patterns' centred reference values,
-//     scattered per rotation into float maps and stored in BF16 in the CTA's
-//     own scratch slot as [footprint row][8-column block][rotation][8 values]
-//     (512 bytes per row block).  In shared memory each row has 3 zero blocks
-//     in front, so row m = 32 j + r of a core-matrix group reads block
-//     (a + j): consecutive 8-row groups are 128 bytes apart (SBO) and the two
-//     K halves 512 bytes apart (LBO), i.e. the x-shift by 8 j columns costs
-//     nothing but the descriptor.  Rows are brought in with bulk async copies
-//     (cp.async.bulk, no multicast).
-//   * B operand (N = 256 = 32 y offsets by 8 x offsets, K = 16 image
-//     columns): the current frame in a Hankel layout - per image row and
-//     8-column block, 8 entries of 16 bytes, entry s holding the 8 pixels that
-//     start s columns into the block - so the 8 x offsets of a core matrix are
-//     16 bytes apart, K halves 128 bytes apart (LBO) and y offsets one image
-//     row apart (SBO).
+// CTAs, one per SM, 512 threads):
+//   * A operands (M = 128 = 4 x-shifts j by 32 rotation slots r, K = 16
+//     footprint columns): W_r and M_r, stored in the grain's scratch slot as
+//     [footprint row][8-column block][rotation][8 values] (512 bytes per row
+//     block).  In shared memory each row has 3 zero blocks in front, so row
+//     m = 32 j + r of a core-matrix group reads block (a + j): consecutive
+//     8-row groups are 128 bytes apart (SBO) and the two K halves 512 bytes
+//     apart (LBO), i.e. the x-shift by 8 j columns costs nothing but the
+//     descriptor.  Rows are brought in with bulk async copies (cp.async.bulk,
+//     no multicast).
+//   * B operands (N = 256 = 32 y offsets by 8 x offsets, K = 16 image
+//     columns): the current frame minus m, and its square, in a Hankel
+//     layout - per image row and 8-column block, 8 entries of 16 bytes, entry
+//     s holding the 8 pixels that start s columns into the block - so the 8 x
+//     offsets of a core matrix are 16 bytes apart, K halves 128 bytes apart
+//     (LBO) and y offsets one image row apart (SBO).
 //   * For footprint row y and chunk c, D[32 j + r][8 v + s] accumulates
-//     W_r(y, f) * I(y + v, f + 24 - 8 j + s): candidate x offset 24 - 8 j + s.
-//     One MMA (M=128, N=256, K=16) covers the whole 32 x 32 x 32 tile; a
-//     grain's tile takes (footprint rows) x (chunks) MMAs, issued by one thread
-//     per strip of rows and committed to an mbarrier.
-//   * The epilogue reads the 128 x 256 FP32 accumulator with tcgen05.ld
-//     (warp w: lanes 32 (w % 4).., columns 128 (w / 4)..), takes the maximum
-//     over rotation lanes per candidate with a warp max-reduction, divides by
-//     sqrt(C11) and keeps the best candidates.
+//     W_r(y, f) * I(y + v, f + 24 - 8 j + s): candidate x offset 24 - 8 j + s
+//     (S likewise with M_r and the squares).  Two MMAs (M=128, N=256, K=16)
+//     cover the whole 32 x 32 x 32 tile for one row and chunk; a grain's tile
+//     takes 2 x (footprint rows) x (chunks) MMAs, issued by one thread per
+//     strip of rows and committed to an mbarrier.  D occupies tensor-memory
+//     columns 0..255, S columns 256..511.
+//   * The epilogue reads both accumulators with tcgen05.ld (warp w: lanes
+//     32 (w % 4).., columns 64 (w / 4)..), divides per rotation lane, takes
+//     the maximum over rotation lanes per candidate with a warp max-reduction
+//     and keeps the best candidates.
 //
-// Pattern rotation (all three kernels) is rotate_pixel_pattern's
+// Pattern rotation (all kernels) is rotate_pixel_pattern's
 // (src/p-tracker.cpp:615-621) result bit for bit: an FP32 estimate decides the
 // rounding, and the FP64 expression is evaluated whenever the estimate lies
 // within 1e-3 of a half-integer (the estimate's error is below 2e-5 for the
@@ -58,6 +64,7 @@
 //
 // Limits (else the exact kernels run): pattern extent within +-47 px
 // (footprint side <= 95), at most 32 rotation steps.
+
 #include <cuda_bf16.h>
 
 #include <climits>
@@ -68,26 +75,21 @@ namespace ptk {
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kNRot = 32;         // rotation slots of the A operand
+constexpr int kThreads = 512;     // 16 warps
+constexpr int kWarps = kThreads / 32;
+constexpr int kNRot = 32;         // rotation slots of the A operands
 constexpr int kMaxFoot = 96;      // footprint side limit (2 * half + 1 < 96)
-constexpr int kTmemCols = 256;    // 128 lanes x 256 FP32 columns: the whole tile
-constexpr int kSmemBudget = 108 * 1024;  // two CTAs per SM
-// Kept candidates: the tile's best approximate score and those within 2 % of
-// it (up to `keep`).  On the 5616x3744 2000-grain workload the exact best lies
-// at most 0.05 % below the approximate best.
-constexpr float kKeepRel = 0.02f;
+constexpr int kTmemCols = 512;    // D in columns 0..255, S in 256..511 (128 lanes x FP32)
+constexpr int kSmemBudget = 224 * 1024;  // one CTA per SM
+// Kept candidates: the tile's best score and those within 3 % of it (up to
+// `keep`).  Over 959 grains of the 50-frame 5616x3744 sequence (small grains
+// with edge-dominated patterns, accumulated reference rotations) the exact
+// best lay at most 1.9 % below the tile's best score.
+constexpr float kKeepRel = 0.03f;
 constexpr long kWaitLimit = 1L << 22;
-// weights kernel: 512 threads, 64 KB of float maps (three blocks per SM)
+// weights kernel: 512 threads, 64 KB of float maps and byte counters
 constexpr int kWThreads = 512;
 constexpr int kWSmem = 64 * 1024;
-
-// window statistics: 512 threads, prefix rows of 128 entries, runs per row
-constexpr int kStatsThreads = 512;
-constexpr int kPrefRow = 128;
-constexpr int kRunCap = kMaxFoot;
-constexpr size_t kPrefBytes = (size_t)(kMaxFoot + kTileV - 1) * kPrefRow * 8;
-constexpr size_t kStatsSmem = kPrefBytes + 2 * (size_t)kMaxFoot * kRunCap * 4;
 
 // A and B operand formats: BF16 x BF16 -> FP32, both K-major, M = 128, N = 256.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
@@ -111,8 +113,9 @@ __host__ __device__ inline Geom geom_of(int half) {
   g.nch = (g.nbf + 3 + 1) / 2;
   g.wb = 2 * g.nch + 3;
   g.hb = 2 * g.nch;
-  const int per_row = g.wb * 512 + g.hb * 128;
-  int rs = (kSmemBudget - 31 * g.hb * 128) / per_row;
+  // W and M rows, and two Hankel buffers with 31 rows of halo
+  const int per_row = 2 * g.wb * 512 + 2 * g.hb * 128;
+  int rs = (kSmemBudget - 31 * 2 * g.hb * 128) / per_row;
   if (rs > g.fw) rs = g.fw;
   g.rs = rs < 1 ? 1 : rs;
   return g;
@@ -224,163 +227,13 @@ __device__ __forceinline__ bool better_b(double ncc, int idx, double bn, int bi)
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// 1. Window variance under pattern0_rotated for every candidate of a tile.
-//    The pattern's multiplicity map is split into row runs of equal
-//    multiplicity; the frame patch gets row prefix sums of I (uint32, exact)
-//    and I^2 (FP32).  Candidate (u, v) then costs two lookups per run:
-//    S1 = sum_runs m * (P1[y + v][x1 + u + 1] - P1[y + v][x0 + u]).
-//    lane = x offset u, warp w = y offsets 2w, 2w + 1.
-__global__ void __launch_bounds__(kStatsThreads) k_window_stats(Bf16Launch p) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int s_bb[4];
-  __shared__ int s_nrun[kMaxFoot];
-  const int item = blockIdx.x;
-  const int tiles = p.tiles_u * p.tiles_v;
-  const int li = item / tiles, t = item - li * tiles;
-  if (li >= *p.list_count) return;
-  const int tu = t / p.tiles_v, tv = t - tu * p.tiles_v;
-  const int gi = p.list[li];
-  const GrainsDev& g = p.g;
-  const int b = g.pstart[gi], P = g.pstart[gi + 1] - b;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  constexpr int kWarps = kStatsThreads / 32;
-  if (g.masked[gi] || (g.flags[gi] & 2) || P <= 0 || P > kMaxPatternPoints) return;
-  if (tid == 0) {
-    s_bb[0] = s_bb[2] = INT_MAX;
-    s_bb[1] = s_bb[3] = INT_MIN;
-  }
-  __syncthreads();
-  {
-    int xmn = INT_MAX, xmx = INT_MIN, ymn = INT_MAX, ymx = INT_MIN;
-    for (int i = tid; i < P; i += kStatsThreads) {
-      const short2 q = g.pat0[b + i];
-      xmn = min(xmn, (int)q.x);
-      xmx = max(xmx, (int)q.x);
-      ymn = min(ymn, (int)q.y);
-      ymx = max(ymx, (int)q.y);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      xmn = min(xmn, __shfl_xor_sync(0xffffffffu, xmn, o));
-      xmx = max(xmx, __shfl_xor_sync(0xffffffffu, xmx, o));
-      ymn = min(ymn, __shfl_xor_sync(0xffffffffu, ymn, o));
-      ymx = max(ymx, __shfl_xor_sync(0xffffffffu, ymx, o));
-    }
-    if (lane == 0) {
-      atomicMin(&s_bb[0], xmn);
-      atomicMax(&s_bb[1], xmx);
-      atomicMin(&s_bb[2], ymn);
-      atomicMax(&s_bb[3], ymx);
-    }
-  }
-  __syncthreads();
-  const int bx0 = s_bb[0], by0 = s_bb[2];
-  const int bw = s_bb[1] - bx0 + 1, bh = s_bb[3] - by0 + 1;
-  if (bw >= kMaxFoot || bh >= kMaxFoot) return;  // excluded by the host's geometry check
-  int* mmap = reinterpret_cast<int*>(smem);  // bh x bw multiplicities (aliased by the prefix rows later)
-  uint32_t* run_a = reinterpret_cast<uint32_t*>(smem + kPrefBytes);  // [y][k]: x0 | m << 16
-  uint32_t* run_b = run_a + kMaxFoot * kRunCap;                          // [y][k]: x1
-  for (int e = tid; e < bw * bh; e += kStatsThreads) mmap[e] = 0;
-  __syncthreads();
-  for (int i = tid; i < P; i += kStatsThreads) {
-    const short2 q = g.pat0[b + i];
-    atomicAdd(&mmap[(q.y - by0) * bw + (q.x - bx0)], 1);
-  }
-  __syncthreads();
-  // runs of equal multiplicity, one warp per row (starts and ends paired by rank)
-  for (int y = warp; y < bh; y += kWarps) {
-    const int* row = mmap + y * bw;
-    int ns = 0, ne = 0;
-    for (int x0 = 0; x0 < bw; x0 += 32) {
-      const int x = x0 + lane;
-      const int m = x < bw ? row[x] : 0;
-      const int ml = (x >= 1 && x <= bw) ? row[x - 1] : 0;
-      const int mr = (x + 1 < bw) ? row[x + 1] : 0;
-      const bool st = m != 0 && m != ml, en = m != 0 && m != mr;
-      const unsigned bs = __ballot_sync(0xffffffffu, st), be = __ballot_sync(0xffffffffu, en);
-      const unsigned below = (1u << lane) - 1u;
-      if (st) run_a[y * kRunCap + ns + __popc(bs & below)] = (uint32_t)x | ((uint32_t)m << 16);
-      if (en) run_b[y * kRunCap + ne + __popc(be & below)] = (uint32_t)x;
-      ns += __popc(bs);
-      ne += __popc(be);
-    }
-    if (lane == 0) s_nrun[y] = ns;
-  }
-  __syncthreads();
-  // prefix rows: pref[rho][x] = (sum of I, sum of I^2) over columns < x
-  const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
-  const int u0 = -p.left + tu * kTileU, v0 = -p.up + tv * kTileV;
-  const int X0 = g.refx[gi] + gdx + bx0 + u0, Y0 = g.refy[gi] + gdy + by0 + v0;
-  const int pc = bw + kTileU - 1;  // patch columns; prefix entries 0..pc
-  uint2* pref = reinterpret_cast<uint2*>(smem);
-  for (int rho = warp; rho < bh + kTileV - 1; rho += kWarps) {
-    const int Y = Y0 + rho;
-    const bool rowin = Y >= 0 && Y < p.cur.dimy;
-    uint32_t s[4];
-    float q[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int x = 4 * lane + j, X = X0 + x;
-      uint32_t v = 0;
-      if (rowin && x < pc && X >= 0 && X < p.cur.dimx) v = p.cur.pix[(size_t)Y * p.cur.pitch + X];
-      const float vf = small_i2f((int)v);
-      s[j] = v + (j ? s[j - 1] : 0u);
-      q[j] = vf * vf + (j ? q[j - 1] : 0.0f);
-    }
-    uint32_t ts = s[3];
-    float tq = q[3];
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t os = __shfl_up_sync(0xffffffffu, ts, o);
-      const float oq = __shfl_up_sync(0xffffffffu, tq, o);
-      if (lane >= o) {
-        ts += os;
-        tq += oq;
-      }
-    }
-    const uint32_t es = ts - s[3];
-    const float eq = tq - q[3];
-    uint2* prow = pref + rho * kPrefRow;
-    if (lane == 0) prow[0] = make_uint2(0u, 0u);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int x = 4 * lane + j;
-      if (x + 1 < kPrefRow) prow[x + 1] = make_uint2(es + s[j], __float_as_uint(eq + q[j]));
-    }
-  }
-  __syncthreads();
-  const int u = lane;
-  uint32_t S1[2] = {0u, 0u};
-  float S11[2] = {0.0f, 0.0f};
-  for (int y = 0; y < bh; ++y) {
-    const int nr = s_nrun[y];
-    for (int k = 0; k < nr; ++k) {
-      const uint32_t a = run_a[y * kRunCap + k];
-      const int x0 = (int)(a & 0xffffu), x1 = (int)run_b[y * kRunCap + k];
-      const uint32_t m = a >> 16;
-      const float mf = small_i2f((int)m);
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const uint2* prow = pref + (y + 2 * warp + j) * kPrefRow;
-        const uint2 hi = prow[x1 + u + 1], lo = prow[x0 + u];
-        S1[j] += m * (hi.x - lo.x);
-        S11[j] = fmaf(mf, __uint_as_float(hi.y) - __uint_as_float(lo.y), S11[j]);
-      }
-    }
-  }
-  float* out = p.c11 + (size_t)item * (kTileU * kTileV);
-#pragma unroll
-  for (int j = 0; j < 2; ++j) {
-    const double c11 = (double)S11[j] - (double)S1[j] * (double)S1[j] / (double)P;
-    out[(2 * warp + j) * kTileU + u] = (float)c11;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// 2a. BF16 weights of every rotation step of a grain (one block per list
-//     entry): the pattern rotated by each step, scattered with the centred
-//     reference values I0 - mean0 into float maps (coinciding points add up),
-//     written to the grain's weight slot as [footprint row][8-column block]
-//     [rotation][8 values].  As many rotations per pass as maps fit in shared
-//     memory.
+// 1. BF16 operands of every rotation step of a grain (one block per list
+//    entry): the pattern rotated by each step, scattered into float maps of
+//    the centred reference values I0 - mean0 (coinciding points add up) and
+//    byte counters of the multiplicity, written to the grain's slot as
+//    W [footprint row][8-column block][rotation][8 values], followed by M in
+//    the same layout.  As many rotations per pass as maps fit in shared
+//    memory.
 __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double2 s_cs[kNRot];
@@ -394,7 +247,9 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
   const Geom G = geom_of(p.half[gi]);
   if (G.fw >= kMaxFoot) return;  // excluded by the host's geometry check
   const int tid = threadIdx.x;
-  uint4* slot = reinterpret_cast<uint4*>(p.wslots) + p.wofs[gi];
+  const int rows = G.fw * G.nbf;
+  uint4* slotW = reinterpret_cast<uint4*>(p.wslots) + p.wofs[gi];
+  uint4* slotM = slotW + (size_t)rows * kNRot;
   const double base_rot = g.refrot[gi] + g.drot[gi];  // total_rot = base_rot + step, as the exact search
   if (tid < p.nrot) {
     double sr, cr;
@@ -403,13 +258,15 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
     s_csf[tid] = make_float2((float)cr, (float)sr);
   }
   const float mean0 = (float)g.mean0[gi];
-  float* fmap = reinterpret_cast<float*>(smem);
   const int fw2 = G.fw * G.fw;
-  const int nb_max = max(1, min(p.nrot, kWSmem / (fw2 * 4)));
-  const int rows = G.fw * G.nbf;
+  const int cw = (fw2 + 3) / 4;  // 32-bit words of a map's byte counters
+  const int nb_max = max(1, min(p.nrot, kWSmem / (4 * (fw2 + cw))));
+  float* fmap = reinterpret_cast<float*>(smem);
+  unsigned* cmap = reinterpret_cast<unsigned*>(fmap + (size_t)nb_max * fw2);
   for (int r0 = 0; r0 < p.nrot; r0 += nb_max) {
     const int nb = min(nb_max, p.nrot - r0);
     for (int e = tid; e < nb * fw2; e += kWThreads) fmap[e] = 0.0f;
+    for (int e = tid; e < nb * cw; e += kWThreads) cmap[e] = 0u;
     __syncthreads();
     for (int i = tid; i < P; i += kWThreads) {
       const short2 q0 = g.pat[b + i];
@@ -420,37 +277,51 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
         const short2 q = rotate_round_fast(q0, cf.x, cf.y, cd.x, cd.y);
         // |q| <= ceil(|p|) = half - 1: always inside the footprint
         const unsigned fx = (unsigned)(q.x + G.half), fy = (unsigned)(q.y + G.half);
-        if (fx < (unsigned)G.fw && fy < (unsigned)G.fw) atomicAdd(&fmap[k * fw2 + fy * G.fw + fx], w);
+        if (fx < (unsigned)G.fw && fy < (unsigned)G.fw) {
+          const int e = fy * G.fw + fx;
+          atomicAdd(&fmap[k * fw2 + e], w);
+          atomicAdd(&cmap[k * cw + (e >> 2)], 1u << (8 * (e & 3)));
+        }
       }
     }
     __syncthreads();
+    const unsigned char* cnt = reinterpret_cast<const unsigned char*>(cmap);
     for (int e = tid; e < nb * rows; e += kWThreads) {
       const int rem = e / nb, k = e - rem * nb;
       const int y = rem / G.nbf, af = rem - y * G.nbf;
-      const float* src = fmap + k * fw2 + y * G.fw + 8 * af;
-      float v[8];
+      const int o = y * G.fw + 8 * af;
+      const float* src = fmap + k * fw2 + o;
+      const unsigned char* csrc = cnt + (size_t)k * cw * 4 + o;
+      float v[8], m[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) v[j] = (8 * af + j < G.fw) ? src[j] : 0.0f;
-      slot[(size_t)rem * kNRot + r0 + k] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
-                                                      pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
+      for (int j = 0; j < 8; ++j) {
+        const bool in = 8 * af + j < G.fw;
+        v[j] = in ? src[j] : 0.0f;
+        m[j] = in ? (float)csrc[j] : 0.0f;
+      }
+      const size_t at = (size_t)rem * kNRot + r0 + k;
+      slotW[at] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                             pack_bf16x2(v[6], v[7]));
+      slotM[at] = make_uint4(pack_bf16x2(m[0], m[1]), pack_bf16x2(m[2], m[3]), pack_bf16x2(m[4], m[5]),
+                             pack_bf16x2(m[6], m[7]));
     }
     __syncthreads();
   }
 }
-
 // ---------------------------------------------------------------------------
-// 2. Tensor-core cross terms and the kept candidates of every tile.
-__global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
+// 2. Tensor-core cross terms and second moments, and the kept candidates of
+//    every tile.
+__global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   extern __shared__ __align__(128) unsigned char smem_bf[];
   unsigned char* smem = smem_bf;
   __shared__ __align__(8) unsigned long long s_mbar;   // MMA completion
-  __shared__ __align__(8) unsigned long long s_wbar;   // weight-row bulk copies
+  __shared__ __align__(8) unsigned long long s_wbar;   // operand-row bulk copies
   __shared__ uint32_t s_tmem;
   __shared__ int s_li, s_err, s_bb[4];
   __shared__ double2 s_cs[kNRot];
   __shared__ float2 s_csf[kNRot];
-  __shared__ float s_cv[8 * kBf16KeepMax];
-  __shared__ int s_ci[8 * kBf16KeepMax];
+  __shared__ float s_cv[kWarps * kBf16KeepMax];
+  __shared__ int s_ci[kWarps * kBf16KeepMax];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t mbar = smem_u32(&s_mbar), wbar = smem_u32(&s_wbar);
 
@@ -505,16 +376,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
     const Geom G = geom_of(p.half[gi]);
     const float mean0 = (float)g.mean0[gi];
     const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
-    const uint4* slot = reinterpret_cast<const uint4*>(p.wslots) + p.wofs[gi];
+    const size_t wrows = (size_t)G.fw * G.nbf * kNRot;
+    const uint4* slotW = reinterpret_cast<const uint4*>(p.wslots) + p.wofs[gi];
+    const uint4* slotM = slotW + wrows;
+    const size_t abytes = (size_t)G.rs * G.wb * 512, hbytes = (size_t)(G.rs + 31) * G.hb * 128;
     unsigned char* sW = smem;
-    unsigned char* sH = smem + (size_t)G.rs * G.wb * 512;
-    const uint32_t wbase = smem_u32(sW), hbase = smem_u32(sH);
-    // zero blocks of every weight row (3 in front, the rest after the footprint)
+    unsigned char* sM = sW + abytes;
+    unsigned char* sHa = sM + abytes;
+    unsigned char* sHs = sHa + hbytes;
+    const uint32_t wbase = smem_u32(sW), mbase = smem_u32(sM), habase = smem_u32(sHa), hsbase = smem_u32(sHs);
+    // zero blocks of every operand row (3 in front, the rest after the footprint)
     for (int e = tid; e < G.rs * (G.wb - G.nbf) * kNRot; e += kThreads) {
       const int yl = e / ((G.wb - G.nbf) * kNRot), rem = e - yl * ((G.wb - G.nbf) * kNRot);
       const int zb = rem >> 5, r = rem & 31;
       const int a = zb < 3 ? zb : zb + G.nbf;
-      reinterpret_cast<uint4*>(sW)[((size_t)yl * G.wb + a) * kNRot + r] = make_uint4(0, 0, 0, 0);
+      const size_t at = ((size_t)yl * G.wb + a) * kNRot + r;
+      reinterpret_cast<uint4*>(sW)[at] = make_uint4(0, 0, 0, 0);
+      reinterpret_cast<uint4*>(sM)[at] = make_uint4(0, 0, 0, 0);
     }
     __syncthreads();
     // Bounding box of the rotated patterns: +-(half - 1) bounds it; the exact
@@ -522,7 +400,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
     // the exact search) is computed only when that bound reaches the edge.
     int bbx0 = 1 - G.half, bbx1 = G.half - 1, bby0 = 1 - G.half, bby1 = G.half - 1;
     bool exact_bb = false;
-    const float sub = 8388608.0f + rintf(mean0);  // pixel v -> (2^23 + v) - sub = v - ishift, exactly
+    const float sub = 8388608.0f + rintf(mean0);  // pixel v -> (2^23 + v) - sub = v - m, exactly
 
     for (int t = 0; t < tiles; ++t) {
       const int tu = t / p.tiles_v, tv = t - tu * p.tiles_v;
@@ -575,27 +453,31 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
       const int Xi = g.refx[gi] + gdx - G.half + u0, Yi = g.refy[gi] + gdy - G.half + v0;
       for (int ys = 0; ys < G.fw; ys += G.rs) {
         const int nr = min(G.rs, G.fw - ys);
-        if (warp == 0) {  // weight rows ys .. ys + nr - 1: the live rotation rows of each block, bulk copies
-          if (lane == 0) mbar_expect_tx(wbar, (uint32_t)(nr * G.nbf * p.nrot * 16));
+        if (warp == 0) {  // operand rows ys .. ys + nr - 1: the live rotation rows of each block, bulk copies
+          if (lane == 0) mbar_expect_tx(wbar, (uint32_t)(2 * nr * G.nbf * p.nrot * 16));
           __syncwarp();
           for (int e = lane; e < nr * G.nbf; e += 32) {
             const int yl = e / G.nbf, af = e - yl * G.nbf;
-            bulk_g2s(wbase + (uint32_t)((yl * G.wb + 3 + af) * 512), slot + ((size_t)(ys + yl) * G.nbf + af) * kNRot,
-                     (uint32_t)p.nrot * 16, wbar);
+            const uint32_t dst = (uint32_t)((yl * G.wb + 3 + af) * 512);
+            const size_t src = ((size_t)(ys + yl) * G.nbf + af) * kNRot;
+            bulk_g2s(wbase + dst, slotW + src, (uint32_t)p.nrot * 16, wbar);
+            bulk_g2s(mbase + dst, slotM + src, (uint32_t)p.nrot * 16, wbar);
           }
         }
-        // Hankel image rows ys .. ys + nr + 30.  Entry (block a, shift s) of a
-        // row is the 8-pixel window starting at column x = 8 a + s, stored at
-        // byte 16 x: a warp fills one row, 25 windows per pass, lane x loading
-        // pixel x and taking pixels x + 1 .. x + 7 from the next lanes, so the
-        // 16-byte stores of a pass are contiguous.
+        // Hankel image rows ys .. ys + nr + 30 of I - m and of (I - m)^2.
+        // Entry (block a, shift s) of a row is the 8-pixel window starting at
+        // column x = 8 a + s, stored at byte 16 x: a warp fills one row, 25
+        // windows per pass, lane x loading pixel x and taking pixels
+        // x + 1 .. x + 7 from the next lanes, so the 16-byte stores of a pass
+        // are contiguous.
         const int Y0 = Yi + ys, nwin = 8 * G.hb;
         const bool inside = Y0 >= 0 && Y0 + nr + 30 < p.cur.dimy && Xi >= 0 && Xi + nwin + 6 < p.cur.dimx;
-        for (int rho = warp; rho < nr + 31; rho += kThreads / 32) {
+        for (int rho = warp; rho < nr + 31; rho += kWarps) {
           const int Y = Y0 + rho;
           const bool rowin = Y >= 0 && Y < p.cur.dimy;
           const uint16_t* src = p.cur.pix + (size_t)(rowin ? Y : 0) * p.cur.pitch;
-          unsigned char* drow = sH + (size_t)rho * G.hb * 128;
+          unsigned char* drow = sHa + (size_t)rho * G.hb * 128;
+          unsigned char* qrow = sHs + (size_t)rho * G.hb * 128;
           for (int x0 = 0; x0 < nwin; x0 += 25) {
             const int x = x0 + lane, X = Xi + x;
             float f = 0.0f;
@@ -603,10 +485,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
               f = __int_as_float(0x4B000000 | (int)__ldg(src + X)) - sub;
             const float f1 = __shfl_down_sync(0xffffffffu, f, 1);
             const uint32_t p0 = pack_bf16x2(f, f1);
+            const uint32_t q0 = pack_bf16x2(f * f, f1 * f1);
             const uint32_t p2 = __shfl_down_sync(0xffffffffu, p0, 2);
             const uint32_t p4 = __shfl_down_sync(0xffffffffu, p0, 4);
             const uint32_t p6 = __shfl_down_sync(0xffffffffu, p0, 6);
-            if (lane < 25 && x < nwin) *reinterpret_cast<uint4*>(drow + 16 * x) = make_uint4(p0, p2, p4, p6);
+            const uint32_t q2 = __shfl_down_sync(0xffffffffu, q0, 2);
+            const uint32_t q4 = __shfl_down_sync(0xffffffffu, q0, 4);
+            const uint32_t q6 = __shfl_down_sync(0xffffffffu, q0, 6);
+            if (lane < 25 && x < nwin) {
+              *reinterpret_cast<uint4*>(drow + 16 * x) = make_uint4(p0, p2, p4, p6);
+              *reinterpret_cast<uint4*>(qrow + 16 * x) = make_uint4(q0, q2, q4, q6);
+            }
           }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -619,10 +508,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             for (int yl = 0; yl < nr; ++yl)
               for (int c = 0; c < G.nch; ++c) {
-                const uint64_t ad = make_desc(wbase + (uint32_t)((yl * G.wb + 2 * c) * 512), 512, 128);
-                const uint64_t bd =
-                    make_desc(hbase + (uint32_t)((yl * G.hb + 2 * c) * 128), 128, (uint32_t)(G.hb * 128));
-                mma_bf16(tmem, ad, bd, (ys == 0 && yl == 0 && c == 0) ? 0u : 1u);
+                const uint32_t ao = (uint32_t)((yl * G.wb + 2 * c) * 512);
+                const uint32_t bo = (uint32_t)((yl * G.hb + 2 * c) * 128);
+                const uint32_t acc = (ys == 0 && yl == 0 && c == 0) ? 0u : 1u;
+                mma_bf16(tmem, make_desc(wbase + ao, 512, 128), make_desc(habase + bo, 128, (uint32_t)(G.hb * 128)),
+                         acc);
+                mma_bf16(tmem + 256u, make_desc(mbase + ao, 512, 128),
+                         make_desc(hsbase + bo, 128, (uint32_t)(G.hb * 128)), acc);
               }
             mma_commit(mbar);
           }
@@ -643,51 +535,41 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
       }
       if (s_err) break;
 
-      // ---- epilogue: max over rotations, normalise, keep the best candidates
-      const int q = warp & 3, h = warp >> 2;  // TMEM lane quadrant (x shift j) and column half
-      const float* c11 = p.c11 + ((size_t)li * tiles + t) * (kTileU * kTileV);
-      float sc[4];
+      // ---- epilogue: per rotation lane D / sqrt(S), max over rotations, keep the best candidates
+      const int q = warp & 3, h = warp >> 2;  // TMEM lane quadrant (x shift j) and column quarter
+      float sc[2];
 #pragma unroll
-      for (int ch = 0; ch < 4; ++ch) {
-        uint32_t rv[32];
-        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(128 * h + 32 * ch), rv);
+      for (int ch = 0; ch < 2; ++ch) {
+        uint32_t dv[32], sv[32];
+        const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(64 * h + 32 * ch);
+        tmem_ld32(ta, dv);
+        tmem_ld32(ta + 256u, sv);
         int mine = INT_MIN;
 #pragma unroll
         for (int k = 0; k < 32; ++k) {
-          const int key = lane < p.nrot ? f2key(__uint_as_float(rv[k])) : INT_MIN;
+          const float d = __uint_as_float(dv[k]), s2 = __uint_as_float(sv[k]);
+          const int key = (lane < p.nrot && s2 > 0.0f) ? f2key(d * rsqrtf(s2)) : INT_MIN;
           const int m = __reduce_max_sync(0xffffffffu, key);
           if (lane == k) mine = m;
         }
-        // this lane's candidate: accumulator column 128 h + 32 ch + lane
-        const int ul = 24 - 8 * q + (lane & 7), vl = 16 * h + 4 * ch + (lane >> 3);
-        float s = -INFINITY;
-        if (u0 + ul <= u1 && v0 + vl <= v1) {
-          const float var = c11[vl * kTileU + ul];
-          if (var > 0.0f) s = key2f(mine) * rsqrtf(var);
-        }
-        sc[ch] = s;
+        // this lane's candidate: accumulator column 64 h + 32 ch + lane
+        const int ul = 24 - 8 * q + (lane & 7), vl = 8 * h + 4 * ch + (lane >> 3);
+        sc[ch] = (u0 + ul <= u1 && v0 + vl <= v1 && mine != INT_MIN) ? key2f(mine) : -INFINITY;
       }
       // per-warp best `keep`, then the block's best `keep` among them
       for (int k = 0; k < keep; ++k) {
-        float bv = -INFINITY;
-        int bc = -1;
-#pragma unroll
-        for (int ch = 0; ch < 4; ++ch)
-          if (sc[ch] > bv) {
-            bv = sc[ch];
-            bc = ch;
-          }
+        const int bc = sc[1] > sc[0] ? 1 : (sc[0] > -INFINITY ? 0 : -1);
+        const float bv = bc == 1 ? sc[1] : sc[0];
         const int key = (bc >= 0) ? f2key(bv) : INT_MIN;
         const int mkey = __reduce_max_sync(0xffffffffu, key);
         const unsigned who = __ballot_sync(0xffffffffu, key == mkey && bc >= 0);
         const int wl = who ? __ffs(who) - 1 : -1;
         int packed = -1;
         if (lane == wl) {
-          const int ul = 24 - 8 * q + (lane & 7), vl = 16 * h + 4 * bc + (lane >> 3);
+          const int ul = 24 - 8 * q + (lane & 7), vl = 8 * h + 4 * bc + (lane >> 3);
           packed = (ul << 8) | vl;
-#pragma unroll
-          for (int ch = 0; ch < 4; ++ch)
-            if (ch == bc) sc[ch] = -INFINITY;
+          if (bc == 0) sc[0] = -INFINITY;
+          else sc[1] = -INFINITY;
         }
         packed = __shfl_sync(0xffffffffu, packed, wl >= 0 ? wl : 0);
         if (lane == 0) {
@@ -697,15 +579,26 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
       }
       __syncthreads();
       if (warp == 0) {
-        // 8 warps x 8 entries: this lane holds entries lane and lane + 32
-        const bool used0 = (lane & (kBf16KeepMax - 1)) < keep;
-        float cv0 = used0 ? s_cv[lane] : -INFINITY, cv1 = used0 ? s_cv[lane + 32] : -INFINITY;
-        int ci0 = used0 ? s_ci[lane] : -1, ci1 = used0 ? s_ci[lane + 32] : -1;
+        // 16 warps x 8 entries: this lane holds entries lane + 32 i
+        const bool used = (lane & (kBf16KeepMax - 1)) < keep;
+        float cv[4];
+        int ci[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          cv[i] = used ? s_cv[lane + 32 * i] : -INFINITY;
+          ci[i] = used ? s_ci[lane + 32 * i] : -1;
+        }
         float top = -INFINITY;
         for (int k = 0; k < kBf16KeepMax; ++k) {
-          const bool sel = cv1 > cv0;
-          const float bv = sel ? cv1 : cv0;
-          const int bi = sel ? ci1 : ci0;
+          float bv = cv[0];
+          int bi = ci[0], bsel = 0;
+#pragma unroll
+          for (int i = 1; i < 4; ++i)
+            if (cv[i] > bv) {
+              bv = cv[i];
+              bi = ci[i];
+              bsel = i;
+            }
           const int key = bi >= 0 ? f2key(bv) : INT_MIN;
           const int mkey = __reduce_max_sync(0xffffffffu, key);
           if (k == 0) top = key2f(mkey);
@@ -716,13 +609,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
           int packed = -1;
           if (lane == wl) {
             packed = bi;
-            if (sel) {
-              cv1 = -INFINITY;
-              ci1 = -1;
-            } else {
-              cv0 = -INFINITY;
-              ci0 = -1;
-            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              if (i == bsel) {
+                cv[i] = -INFINITY;
+                ci[i] = -1;
+              }
           }
           packed = __shfl_sync(0xffffffffu, packed, wl >= 0 ? wl : 0);
           if (lane == 0)
@@ -744,7 +636,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_search_bf16(Bf16Launch p) {
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
-
 // ---------------------------------------------------------------------------
 // 3. Exact rescoring: every rotation step at each kept candidate of a tile,
 //    with the exact search's integer sums and NCC expression.  One block per
@@ -865,7 +756,7 @@ __global__ void __launch_bounds__(256) k_rescore_bf16(Bf16Launch p) {
 // ---------------------------------------------------------------------------
 size_t bf16_weight_entries(int half) {
   const Geom G = geom_of(half);
-  return (size_t)G.fw * G.nbf * kNRot;
+  return 2 * (size_t)G.fw * G.nbf * kNRot;  // W, then M
 }
 
 bool bf16_supported(int max_r, int nrot) { return 2 * max_r + 1 < kMaxFoot && nrot >= 1 && nrot <= kNRot; }
@@ -874,7 +765,6 @@ void prepare_search_bf16() {
   static bool done = false;
   if (done) return;
   cudaFuncSetAttribute(k_search_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget);
-  cudaFuncSetAttribute(k_window_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStatsSmem);
   cudaFuncSetAttribute(k_weights_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, kWSmem);
   done = true;
 }
@@ -882,14 +772,12 @@ void prepare_search_bf16() {
 void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent_t* ev) {
   const int items = p.max_items;
   if (ev) cudaEventRecord(ev[0], s);
-  k_window_stats<<<items, kStatsThreads, kStatsSmem, s>>>(p);
-  if (ev) cudaEventRecord(ev[1], s);
   k_weights_bf16<<<p.max_items / (p.tiles_u * p.tiles_v), kWThreads, kWSmem, s>>>(p);
-  if (ev) cudaEventRecord(ev[2], s);
+  if (ev) cudaEventRecord(ev[1], s);
   k_search_bf16<<<grid, kThreads, kSmemBudget, s>>>(p);
-  if (ev) cudaEventRecord(ev[3], s);
+  if (ev) cudaEventRecord(ev[2], s);
   k_rescore_bf16<<<items, 256, 0, s>>>(p);
-  if (ev) cudaEventRecord(ev[4], s);
+  if (ev) cudaEventRecord(ev[3], s);
 }
 
 }  // namespace ptk

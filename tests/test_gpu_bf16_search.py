@@ -6,7 +6,7 @@ Bar: the exact search's own - the same integer offset and rotation step as the
 CPU oracle on every grain whose two best NCC values differ by more than 1e-6,
 NCC within 1e-5 - on 8- and 16-bit frames, noisy frames, multi-tile zones,
 rescue levels and irregular patterns.  The launch count shows that the
-tensor-core kernels ran (5 launches per level instead of 2)."""
+tensor-core kernels ran (6 launches per level instead of 2)."""
 from __future__ import annotations
 
 import os
@@ -51,7 +51,8 @@ def _pixel_case(ptk, oracle, pair, zones, pattern=("grain_diameter", 1.0, 1.0), 
     g.precompute()
     before = g.launches()
     g.search(0)
-    assert g.launches() - before == 6, "stage begin, window stats, weights, tensor-core search, rescore, finalize"
+    assert g.launches() - before == 7, ("stage begin, weights, tensor-core search, rescore, finalize, "
+                                        "exact re-search of rejected grains, finalize")
     c = _cpu(oracle, pair, zones, {"rescue_level": 0, "NCC_min": 0.7}, pattern)
     c.precompute()
     c.pixel_all()
