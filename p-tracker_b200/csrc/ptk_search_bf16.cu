@@ -21,7 +21,7 @@
 //     D_r / sqrt(S_r) is a lower bound of NCC_r * sqrt(C0C0) that no footprint
 //     difference between rotation steps can inflate, and it is tight when the
 //     window's mean is close to the reference pattern's.  The best candidates
-//     of each tile (within kKeepRel of its best score) are written out.
+//     of each tile (within a few percent of its best score) are written out.
 //  3. k_rescore_bf16 (CUDA cores, exact integers): every rotation step at each
 //     kept candidate, with the exact search's sums and NCC expression, giving
 //     per-candidate best records in the reference's order; the level's usual
@@ -81,11 +81,16 @@ constexpr int kNRot = 32;         // rotation slots of the A operands
 constexpr int kMaxFoot = 96;      // footprint side limit (2 * half + 1 < 96)
 constexpr int kTmemCols = 512;    // D in columns 0..255, S in 256..511 (128 lanes x FP32)
 constexpr int kSmemBudget = 224 * 1024;  // one CTA per SM
-// Kept candidates: the tile's best score and those within 3 % of it (up to
-// `keep`).  Over 959 grains of the 50-frame 5616x3744 sequence (small grains
-// with edge-dominated patterns, accumulated reference rotations) the exact
-// best lay at most 1.9 % below the tile's best score.
+// Kept candidates: the tile's best score and those within kKeepRel of it (up
+// to `keep`).  Over 959 grains of the 50-frame 5616x3744 sequence (small
+// grains with edge-dominated patterns, accumulated reference rotations) the
+// exact best lay at most 1.9 % below the tile's best score.  The bound is
+// looser for mediocre matches (the window's mean further from the pattern's),
+// so tiles whose best score, as an NCC lower bound, is below kGoodMatch keep
+// candidates within kKeepRelWeak.
 constexpr float kKeepRel = 0.03f;
+constexpr float kKeepRelWeak = 0.10f;
+constexpr float kGoodMatch = 0.9f;
 constexpr long kWaitLimit = 1L << 22;
 // weights kernel: 512 threads, 64 KB of float maps and byte counters
 constexpr int kWThreads = 512;
@@ -375,6 +380,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     }
     const Geom G = geom_of(p.half[gi]);
     const float mean0 = (float)g.mean0[gi];
+    const float c00_rsqrt = g.c0c0[gi] > 0.0 ? (float)(1.0 / sqrt(g.c0c0[gi])) : 0.0f;
     const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
     const size_t wrows = (size_t)G.fw * G.nbf * kNRot;
     const uint4* slotW = reinterpret_cast<const uint4*>(p.wslots) + p.wofs[gi];
@@ -588,7 +594,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
           cv[i] = used ? s_cv[lane + 32 * i] : -INFINITY;
           ci[i] = used ? s_ci[lane + 32 * i] : -1;
         }
-        float top = -INFINITY;
+        float top = -INFINITY, rel = kKeepRel;
         for (int k = 0; k < kBf16KeepMax; ++k) {
           float bv = cv[0];
           int bi = ci[0], bsel = 0;
@@ -601,9 +607,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
             }
           const int key = bi >= 0 ? f2key(bv) : INT_MIN;
           const int mkey = __reduce_max_sync(0xffffffffu, key);
-          if (k == 0) top = key2f(mkey);
-          // candidates scoring more than kKeepRel below the tile's best are not rescored
-          const bool near = !(top > 0.0f) || key2f(mkey) >= top * (1.0f - kKeepRel);
+          if (k == 0) {
+            top = key2f(mkey);
+            // D / sqrt(S) <= NCC sqrt(C0C0)
+            if (!(top * c00_rsqrt >= kGoodMatch)) rel = kKeepRelWeak;
+          }
+          // candidates scoring more than `rel` below the tile's best are not rescored
+          const bool near = !(top > 0.0f) || key2f(mkey) >= top * (1.0f - rel);
           const unsigned who = near ? __ballot_sync(0xffffffffu, key == mkey && bi >= 0) : 0u;
           const int wl = who ? __ffs(who) - 1 : -1;
           int packed = -1;
