@@ -348,7 +348,7 @@ int search_geometry(ptk_ctx* c, int level, SearchGeom* sg, bool allow_bf16 = tru
   if (sg->items > (size_t)INT32_MAX) return fail(c, PTK_ERR_LIMIT, "too many search work items");
   // The BF16 form covers footprints up to 95 px and 32 rotation steps; other
   // geometries take the exact kernels (same results, exact ranking).
-  sg->bf16 = allow_bf16 && c->cfg.search_method == PTK_SEARCH_BF16 && bf16_supported(c->max_R, sg->nrot);
+  sg->bf16 = allow_bf16 && c->cfg.search_method == PTK_SEARCH_BF16 && bf16_supported(c->max_R, sg->nrot, c->max_dup);
   if (sg->bf16) {
     prepare_search_bf16();
     sg->tiled = false;
@@ -418,6 +418,8 @@ int ensure_bf16(ptk_ctx* c, size_t items) {
       c->bf_wslots_bytes = 0;
       CK(cudaMalloc(&c->d_bf_wslots, bytes));
       c->bf_wslots_bytes = bytes;
+      // rotation slots beyond a level's steps are copied with their block: defined contents
+      CK(cudaMemset(c->d_bf_wslots, 0, bytes));
     }
     c->bf_geom_dirty = false;
     invalidate(c);

@@ -146,7 +146,7 @@ size_t search_tiled_smem(int max_r);
 int search_tiled_occupancy(size_t smem, int max_r);
 void launch_search_tiled(const SearchLaunch& p, int max_r, int grid, size_t smem, cudaStream_t s);
 void launch_finalize(const FinalizeLaunch& p, int n_grains, cudaStream_t s);
-bool bf16_supported(int max_r, int nrot);
+bool bf16_supported(int max_r, int nrot, int max_dup);
 size_t bf16_weight_entries(int half);
 void prepare_search_bf16();
 // ev (optional, 5 events): recorded before the first kernel and after each of the four

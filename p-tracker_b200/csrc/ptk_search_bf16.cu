@@ -37,7 +37,9 @@
 //     8-row groups are 128 bytes apart (SBO) and the two K halves 512 bytes
 //     apart (LBO), i.e. the x-shift by 8 j columns costs nothing but the
 //     descriptor.  Rows are brought in with bulk async copies (cp.async.bulk,
-//     no multicast).
+//     no multicast), one per footprint row and operand: the rotation slots
+//     beyond the level's steps come along and feed accumulator lanes that
+//     are never read.
 //   * B operands (N = 256 = 32 y offsets by 8 x offsets, K = 16 image
 //     columns): the current frame minus m, and its square, in a Hankel
 //     layout - per image row and 8-column block, 8 entries of 16 bytes, entry
@@ -63,7 +65,8 @@
 // offsets allowed here).
 //
 // Limits (else the exact kernels run): pattern extent within +-47 px
-// (footprint side <= 95), at most 32 rotation steps.
+// (footprint side <= 95), at most 32 rotation steps, no offset repeated more
+// than 63 times within a pattern.
 
 #include <cuda_bf16.h>
 
@@ -92,7 +95,7 @@ constexpr float kKeepRel = 0.03f;
 constexpr float kKeepRelWeak = 0.10f;
 constexpr float kGoodMatch = 0.9f;
 constexpr long kWaitLimit = 1L << 22;
-// weights kernel: 512 threads, 64 KB of float maps and byte counters
+// weights kernel: 512 threads, 64 KB of 32-bit maps
 constexpr int kWThreads = 512;
 constexpr int kWSmem = 64 * 1024;
 
@@ -107,6 +110,7 @@ struct Geom {
   int nch;   // 16-column MMA chunks (footprint + 24 columns of shift)
   int wb;    // weight blocks per row in shared memory (3 leading zero blocks)
   int hb;    // Hankel blocks per image row
+  int rp;    // bytes per staged image row (the Hankel's 8 hb + 7 pixels from a 16-byte boundary)
   int rs;    // footprint rows per strip
 };
 
@@ -118,9 +122,12 @@ __host__ __device__ inline Geom geom_of(int half) {
   g.nch = (g.nbf + 3 + 1) / 2;
   g.wb = 2 * g.nch + 3;
   g.hb = 2 * g.nch;
-  // W and M rows, and two Hankel buffers with 31 rows of halo
-  const int per_row = 2 * g.wb * 512 + 2 * g.hb * 128;
-  int rs = (kSmemBudget - 31 * 2 * g.hb * 128) / per_row;
+  g.rp = 16 * g.hb + 32;
+  // W and M rows, two Hankel buffers and the staged image rows, the last
+  // three with 31 rows of halo
+  const int halo_row = 2 * g.hb * 128 + g.rp;
+  const int per_row = 2 * g.wb * 512 + halo_row;
+  int rs = (kSmemBudget - 31 * halo_row) / per_row;
   if (rs > g.fw) rs = g.fw;
   g.rs = rs < 1 ? 1 : rs;
   return g;
@@ -174,6 +181,12 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
       "l"(src), "r"(bytes), "r"(mbar)
       : "memory");
 }
+
+// 16-byte asynchronous copy global -> shared through L2 (per thread).
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
@@ -233,12 +246,13 @@ __device__ __forceinline__ bool better_b(double ncc, int idx, double bn, int bi)
 
 // ---------------------------------------------------------------------------
 // 1. BF16 operands of every rotation step of a grain (one block per list
-//    entry): the pattern rotated by each step, scattered into float maps of
-//    the centred reference values I0 - mean0 (coinciding points add up) and
-//    byte counters of the multiplicity, written to the grain's slot as
-//    W [footprint row][8-column block][rotation][8 values], followed by M in
-//    the same layout.  As many rotations per pass as maps fit in shared
-//    memory.
+//    entry): the pattern rotated by each step, scattered into one 32-bit map
+//    per step holding, per footprint pixel, the sum of the reference values
+//    I0 of the points landing there (low 24 bits, exact) and their number
+//    (high 8 bits), with integer shared-memory atomics.  Written to the
+//    grain's slot as W_r = sum I0 - count * mean0 and M_r = count, each
+//    [footprint row][8-column block][rotation][8 values], M after W.  As many
+//    rotations per pass as maps fit in shared memory.
 __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double2 s_cs[kNRot];
@@ -264,45 +278,37 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
   }
   const float mean0 = (float)g.mean0[gi];
   const int fw2 = G.fw * G.fw;
-  const int cw = (fw2 + 3) / 4;  // 32-bit words of a map's byte counters
-  const int nb_max = max(1, min(p.nrot, kWSmem / (4 * (fw2 + cw))));
-  float* fmap = reinterpret_cast<float*>(smem);
-  unsigned* cmap = reinterpret_cast<unsigned*>(fmap + (size_t)nb_max * fw2);
+  const int nb_max = max(1, min(p.nrot, kWSmem / (4 * fw2)));
+  unsigned* map = reinterpret_cast<unsigned*>(smem);
   for (int r0 = 0; r0 < p.nrot; r0 += nb_max) {
     const int nb = min(nb_max, p.nrot - r0);
-    for (int e = tid; e < nb * fw2; e += kWThreads) fmap[e] = 0.0f;
-    for (int e = tid; e < nb * cw; e += kWThreads) cmap[e] = 0u;
+    for (int e = tid; e < nb * fw2; e += kWThreads) map[e] = 0u;
     __syncthreads();
     for (int i = tid; i < P; i += kWThreads) {
       const short2 q0 = g.pat[b + i];
-      const float w = small_i2f((int)g.w0[b + i]) - mean0;
+      // at most 255 points share a pixel (bf16_supported): the sum stays below 2^24
+      const unsigned add = (unsigned)g.w0[b + i] + (1u << 24);
       for (int k = 0; k < nb; ++k) {
         const float2 cf = s_csf[r0 + k];
         const double2 cd = s_cs[r0 + k];
         const short2 q = rotate_round_fast(q0, cf.x, cf.y, cd.x, cd.y);
         // |q| <= ceil(|p|) = half - 1: always inside the footprint
         const unsigned fx = (unsigned)(q.x + G.half), fy = (unsigned)(q.y + G.half);
-        if (fx < (unsigned)G.fw && fy < (unsigned)G.fw) {
-          const int e = fy * G.fw + fx;
-          atomicAdd(&fmap[k * fw2 + e], w);
-          atomicAdd(&cmap[k * cw + (e >> 2)], 1u << (8 * (e & 3)));
-        }
+        if (fx < (unsigned)G.fw && fy < (unsigned)G.fw) atomicAdd(&map[k * fw2 + fy * G.fw + fx], add);
       }
     }
     __syncthreads();
-    const unsigned char* cnt = reinterpret_cast<const unsigned char*>(cmap);
     for (int e = tid; e < nb * rows; e += kWThreads) {
       const int rem = e / nb, k = e - rem * nb;
       const int y = rem / G.nbf, af = rem - y * G.nbf;
-      const int o = y * G.fw + 8 * af;
-      const float* src = fmap + k * fw2 + o;
-      const unsigned char* csrc = cnt + (size_t)k * cw * 4 + o;
+      const unsigned* src = map + k * fw2 + y * G.fw + 8 * af;
       float v[8], m[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const bool in = 8 * af + j < G.fw;
-        v[j] = in ? src[j] : 0.0f;
-        m[j] = in ? (float)csrc[j] : 0.0f;
+        const unsigned c = (8 * af + j < G.fw) ? src[j] : 0u;
+        const float n = (float)(c >> 24);
+        m[j] = n;
+        v[j] = (float)(c & 0xFFFFFFu) - n * mean0;
       }
       const size_t at = (size_t)rem * kNRot + r0 + k;
       slotW[at] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
@@ -313,6 +319,7 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
     __syncthreads();
   }
 }
+
 // ---------------------------------------------------------------------------
 // 2. Tensor-core cross terms and second moments, and the kept candidates of
 //    every tile.
@@ -346,6 +353,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = s_tmem;
   uint32_t parity = 0, wparity = 0;
+  int zhalf = -1;  // footprint geometry whose zero blocks the operand rows hold
 
   const GrainsDev& g = p.g;
   const int count = *p.list_count;
@@ -390,15 +398,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     unsigned char* sM = sW + abytes;
     unsigned char* sHa = sM + abytes;
     unsigned char* sHs = sHa + hbytes;
+    unsigned char* sR = sHs + hbytes;
     const uint32_t wbase = smem_u32(sW), mbase = smem_u32(sM), habase = smem_u32(sHa), hsbase = smem_u32(sHs);
-    // zero blocks of every operand row (3 in front, the rest after the footprint)
-    for (int e = tid; e < G.rs * (G.wb - G.nbf) * kNRot; e += kThreads) {
-      const int yl = e / ((G.wb - G.nbf) * kNRot), rem = e - yl * ((G.wb - G.nbf) * kNRot);
-      const int zb = rem >> 5, r = rem & 31;
-      const int a = zb < 3 ? zb : zb + G.nbf;
-      const size_t at = ((size_t)yl * G.wb + a) * kNRot + r;
-      reinterpret_cast<uint4*>(sW)[at] = make_uint4(0, 0, 0, 0);
-      reinterpret_cast<uint4*>(sM)[at] = make_uint4(0, 0, 0, 0);
+    const uint32_t rbase = smem_u32(sR);
+    // zero blocks of every operand row (3 in front, the rest after the footprint);
+    // the copies never write them, so they stay valid while the geometry does
+    // (grains come in decreasing pattern size)
+    if (G.half != zhalf) {
+      for (int e = tid; e < G.rs * (G.wb - G.nbf) * kNRot; e += kThreads) {
+        const int yl = e / ((G.wb - G.nbf) * kNRot), rem = e - yl * ((G.wb - G.nbf) * kNRot);
+        const int zb = rem >> 5, r = rem & 31;
+        const int a = zb < 3 ? zb : zb + G.nbf;
+        const size_t at = ((size_t)yl * G.wb + a) * kNRot + r;
+        reinterpret_cast<uint4*>(sW)[at] = make_uint4(0, 0, 0, 0);
+        reinterpret_cast<uint4*>(sM)[at] = make_uint4(0, 0, 0, 0);
+      }
+      zhalf = G.half;
     }
     __syncthreads();
     // Bounding box of the rotated patterns: +-(half - 1) bounds it; the exact
@@ -457,38 +472,68 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
       }
       // image origin of footprint column 0 at candidate (u0, v0)
       const int Xi = g.refx[gi] + gdx - G.half + u0, Yi = g.refy[gi] + gdy - G.half + v0;
+      // A strip whose image rows lie inside the frame stages them in shared
+      // memory with 16-byte asynchronous copies (columns Xa .. Xa + ncols - 1),
+      // issued by every thread during the previous strip's MMAs where there
+      // is one.
+      const int nwin = 8 * G.hb;
+      const int Xa = Xi & ~7, xoff = Xi - Xa;
+      const int ncols = (xoff + nwin + 7 + 7) & ~7;
+      auto staged = [&](int ys_) {
+        const int y0 = Yi + ys_, n_ = min(G.rs, G.fw - ys_);
+        return y0 >= 0 && y0 + n_ + 30 < p.cur.dimy && Xi >= 0 && Xi + nwin + 6 < p.cur.dimx &&
+               Xa + ncols <= p.cur.pitch;
+      };
+      auto stage_rows = [&](int ys_) {
+        const int n_ = min(G.rs, G.fw - ys_) + 31, cpr = ncols >> 3;
+        for (int e = tid; e < n_ * cpr; e += kThreads) {
+          const int rho = e / cpr, c = e - rho * cpr;
+          cp_async16(rbase + (uint32_t)(rho * G.rp + 16 * c),
+                     p.cur.pix + (size_t)(Yi + ys_ + rho) * p.cur.pitch + Xa + 8 * c);
+        }
+      };
+      bool prefetched = false;
       for (int ys = 0; ys < G.fw; ys += G.rs) {
         const int nr = min(G.rs, G.fw - ys);
-        if (warp == 0) {  // operand rows ys .. ys + nr - 1: the live rotation rows of each block, bulk copies
-          if (lane == 0) mbar_expect_tx(wbar, (uint32_t)(2 * nr * G.nbf * p.nrot * 16));
+        const bool inside = staged(ys);
+        if (inside && !prefetched) stage_rows(ys);
+        if (warp == 0) {  // operand rows ys .. ys + nr - 1: one bulk copy per row and operand (whole blocks)
+          if (lane == 0) mbar_expect_tx(wbar, (uint32_t)(2 * nr * G.nbf * 512));
           __syncwarp();
-          for (int e = lane; e < nr * G.nbf; e += 32) {
-            const int yl = e / G.nbf, af = e - yl * G.nbf;
-            const uint32_t dst = (uint32_t)((yl * G.wb + 3 + af) * 512);
-            const size_t src = ((size_t)(ys + yl) * G.nbf + af) * kNRot;
-            bulk_g2s(wbase + dst, slotW + src, (uint32_t)p.nrot * 16, wbar);
-            bulk_g2s(mbase + dst, slotM + src, (uint32_t)p.nrot * 16, wbar);
+          for (int e = lane; e < 2 * nr; e += 32) {
+            const int yl = e >> 1;
+            const uint32_t dst = (uint32_t)((yl * G.wb + 3) * 512);
+            const size_t src = (size_t)(ys + yl) * G.nbf * kNRot;
+            if (e & 1) bulk_g2s(mbase + dst, slotM + src, (uint32_t)(G.nbf * 512), wbar);
+            else bulk_g2s(wbase + dst, slotW + src, (uint32_t)(G.nbf * 512), wbar);
           }
+        }
+        if (inside && !prefetched) {  // (a prefetch completed before the previous strip's last barrier)
+          cp_async_wait_all();
+          __syncthreads();
         }
         // Hankel image rows ys .. ys + nr + 30 of I - m and of (I - m)^2.
         // Entry (block a, shift s) of a row is the 8-pixel window starting at
         // column x = 8 a + s, stored at byte 16 x: a warp fills one row, 25
-        // windows per pass, lane x loading pixel x and taking pixels
+        // windows per pass, lane x reading pixel x and taking pixels
         // x + 1 .. x + 7 from the next lanes, so the 16-byte stores of a pass
-        // are contiguous.
-        const int Y0 = Yi + ys, nwin = 8 * G.hb;
-        const bool inside = Y0 >= 0 && Y0 + nr + 30 < p.cur.dimy && Xi >= 0 && Xi + nwin + 6 < p.cur.dimx;
+        // are contiguous.  Staged strips read the pixels from shared memory,
+        // strips at the frame's edges from global memory with bounds checks.
+        const int Y0 = Yi + ys;
         for (int rho = warp; rho < nr + 31; rho += kWarps) {
           const int Y = Y0 + rho;
           const bool rowin = Y >= 0 && Y < p.cur.dimy;
           const uint16_t* src = p.cur.pix + (size_t)(rowin ? Y : 0) * p.cur.pitch;
+          const uint16_t* srow = reinterpret_cast<const uint16_t*>(sR + (size_t)rho * G.rp) + xoff;
           unsigned char* drow = sHa + (size_t)rho * G.hb * 128;
           unsigned char* qrow = sHs + (size_t)rho * G.hb * 128;
           for (int x0 = 0; x0 < nwin; x0 += 25) {
             const int x = x0 + lane, X = Xi + x;
             float f = 0.0f;
-            if (x < nwin + 7 && (inside || (rowin && X >= 0 && X < p.cur.dimx)))
-              f = __int_as_float(0x4B000000 | (int)__ldg(src + X)) - sub;
+            if (x < nwin + 7) {
+              if (inside) f = __int_as_float(0x4B000000 | (int)srow[x]) - sub;
+              else if (rowin && X >= 0 && X < p.cur.dimx) f = __int_as_float(0x4B000000 | (int)__ldg(src + X)) - sub;
+            }
             const float f1 = __shfl_down_sync(0xffffffffu, f, 1);
             const uint32_t p0 = pack_bf16x2(f, f1);
             const uint32_t q0 = pack_bf16x2(f * f, f1 * f1);
@@ -506,6 +551,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
+        // the staged rows are consumed: bring in the next strip's during these MMAs
+        prefetched = ys + G.rs < G.fw && staged(ys + G.rs);
+        if (prefetched) stage_rows(ys + G.rs);
         if (tid == 0) {
           if (!mbar_wait(wbar, wparity)) {
             s_err = 1;
@@ -535,6 +583,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
           asm volatile("tcgen05.fence::before_thread_sync;");
         }
         parity ^= 1u;
+        if (prefetched) cp_async_wait_all();
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;");
         if (s_err) break;
@@ -637,6 +686,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     }
     if (s_err) break;
   }
+  cp_async_wait_all();
   __syncthreads();
   if (s_err && tid == 0) {  // one more bounded wait on the last armed copy and MMA phases
     mbar_wait(wbar, wparity ^ 1u);
@@ -649,11 +699,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
 // ---------------------------------------------------------------------------
 // 3. Exact rescoring: every rotation step at each kept candidate of a tile,
 //    with the exact search's integer sums and NCC expression.  One block per
-//    (grain, tile); warp w takes rotation steps w, w + 8, ..., its lanes the
-//    pattern points, all kept candidates at once.
-__global__ void __launch_bounds__(256) k_rescore_bf16(Bf16Launch p) {
-  __shared__ double s_bn[8][kBf16KeepMax];
-  __shared__ int s_bi[8][kBf16KeepMax];
+//    (grain, tile); a work unit is one rotation step for two kept candidates,
+//    taken by one warp whose lanes share the pattern points; per candidate the
+//    best record over the rotation steps in the reference's order.
+__global__ void __launch_bounds__(256, 4) k_rescore_bf16(Bf16Launch p) {
+  constexpr int kW = 8;
+  __shared__ double s_bn[kBf16KeepMax][kW];
+  __shared__ int s_bi[kBf16KeepMax][kW];
+  __shared__ int s_base[kBf16KeepMax], s_uv[kBf16KeepMax];
+  __shared__ int s_nk;
   const int item = blockIdx.x;
   const int tiles = p.tiles_u * p.tiles_v;
   const int li = item / tiles;
@@ -664,21 +718,29 @@ __global__ void __launch_bounds__(256) k_rescore_bf16(Bf16Launch p) {
   SearchBest* rec = p.rescored + (size_t)item * kBf16KeepMax;
   const int b = g.pstart[gi], P = g.pstart[gi + 1] - b;
   const bool skip = g.masked[gi] || (g.flags[gi] & 7) || P <= 0 || P > kMaxPatternPoints;
-  const int2* cand = p.topk + (size_t)item * kBf16KeepMax;
   const int NU = p.left + p.right + 1, NV = p.up + p.down + 1;
-  int nk = 0;
-  int base[kBf16KeepMax];  // pixel index of each kept candidate's anchor, -1 when none
-  int uv[kBf16KeepMax];    // (u + left) * NV + (v + up): the candidate's order index without the rotation
-  const int gdx = skip ? 0 : (int)round(g.dx[gi]), gdy = skip ? 0 : (int)round(g.dy[gi]);
-#pragma unroll
-  for (int k = 0; k < kBf16KeepMax; ++k) {
-    const int2 c = skip ? make_int2(INT_MIN, INT_MIN) : cand[k];
-    const bool ok = k < p.keep && c.x != INT_MIN;
-    base[k] = ok ? (g.refy[gi] + gdy + c.y) * p.cur.pitch + (g.refx[gi] + gdx + c.x) : -1;
-    uv[k] = ok ? (c.x + p.left) * NV + (c.y + p.up) : 0;
-    nk += ok ? 1 : 0;
+  if (tid == 0) {  // the kept candidates, compacted: anchor pixel index and order index without the rotation
+    int nk = 0;
+    if (!skip) {
+      const int2* cand = p.topk + (size_t)item * kBf16KeepMax;
+      const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
+      for (int k = 0; k < p.keep && k < kBf16KeepMax; ++k) {
+        const int2 c = cand[k];
+        if (c.x == INT_MIN) continue;
+        s_base[nk] = (g.refy[gi] + gdy + c.y) * p.cur.pitch + (g.refx[gi] + gdx + c.x);
+        s_uv[nk] = (c.x + p.left) * NV + (c.y + p.up);
+        ++nk;
+      }
+    }
+    s_nk = nk;
   }
-  if (skip || nk == 0) {
+  if (tid < kBf16KeepMax * kW) {
+    s_bn[tid / kW][tid % kW] = 0.0;
+    s_bi[tid / kW][tid % kW] = INT_MAX;
+  }
+  __syncthreads();
+  const int nk = s_nk;
+  if (nk == 0) {
     if (tid < kBf16KeepMax) rec[tid] = SearchBest{0.0, INT_MAX, 0};
     return;
   }
@@ -686,78 +748,64 @@ __global__ void __launch_bounds__(256) k_rescore_bf16(Bf16Launch p) {
   const double den1 = (double)(Pl * g.s00[gi] - S0 * S0);
   const int pitch = p.cur.pitch;
   const double base_rot = g.refrot[gi] + g.drot[gi];
-  double bn[kBf16KeepMax];
-  int bi[kBf16KeepMax];
-#pragma unroll
-  for (int k = 0; k < kBf16KeepMax; ++k) {
-    bn[k] = 0.0;
-    bi[k] = INT_MAX;
-  }
-  for (int r = warp; r < p.nrot; r += 8) {
+  const int npair = (nk + 1) >> 1;
+  for (int u = warp; u < p.nrot * npair; u += kW) {
+    const int r = u % p.nrot, k0 = 2 * (u / p.nrot), k1 = k0 + 1;
     double sr, cr;
     sincos(base_rot + p.steps[r], &sr, &cr);
     const float cf = (float)cr, sf = (float)sr;
-    unsigned s1[kBf16KeepMax];
-    unsigned long long s11[kBf16KeepMax], s01[kBf16KeepMax];
-#pragma unroll
-    for (int k = 0; k < kBf16KeepMax; ++k) {
-      s1[k] = 0;
-      s11[k] = 0;
-      s01[k] = 0;
-    }
-    // two points per lane per pass: both points' loads are in flight together
-    for (int i = lane; i < P; i += 64) {
-      const bool two = i + 32 < P;
-      const short2 qa = rotate_round_fast(g.pat[b + i], cf, sf, cr, sr);
-      const short2 qb = two ? rotate_round_fast(g.pat[b + i + 32], cf, sf, cr, sr) : qa;
-      const int oa = (int)qa.y * pitch + (int)qa.x, ob = (int)qb.y * pitch + (int)qb.x;
-      const unsigned wa = g.w0[b + i], wb = two ? (unsigned)g.w0[b + i + 32] : 0u;
-#pragma unroll
-      for (int k = 0; k < kBf16KeepMax; ++k) {
-        if (base[k] < 0) continue;
-        const uint16_t* px = p.cur.pix + base[k];
-        const unsigned va = __ldg(px + oa);
-        const unsigned vb = two ? (unsigned)__ldg(px + ob) : 0u;
-        s1[k] += va + vb;
-        s11[k] += (unsigned long long)(va * va) + (unsigned long long)(vb * vb);
-        s01[k] += (unsigned long long)(wa * va) + (unsigned long long)(wb * vb);
+    const bool two = k1 < nk;
+    const uint16_t* pa = p.cur.pix + s_base[k0];
+    const uint16_t* pb = p.cur.pix + s_base[two ? k1 : k0];
+    unsigned s1a = 0, s1b = 0;
+    unsigned long long s11a = 0, s11b = 0, s01a = 0, s01b = 0;
+#pragma unroll 4
+    for (int i = lane; i < P; i += 32) {
+      const short2 q = rotate_round_fast(g.pat[b + i], cf, sf, cr, sr);
+      const int o = (int)q.y * pitch + (int)q.x;
+      const unsigned w = g.w0[b + i];
+      const unsigned va = __ldg(pa + o);
+      s1a += va;
+      s11a += (unsigned long long)(va * va);
+      s01a += (unsigned long long)(w * va);
+      if (two) {
+        const unsigned vb = __ldg(pb + o);
+        s1b += vb;
+        s11b += (unsigned long long)(vb * vb);
+        s01b += (unsigned long long)(w * vb);
       }
     }
-#pragma unroll
-    for (int k = 0; k < kBf16KeepMax; ++k) {
-      if (base[k] < 0) continue;
-      unsigned long long a = s1[k], c = s11[k], d = s01[k];
-      for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_xor_sync(0xffffffffu, a, o);
-        c += __shfl_xor_sync(0xffffffffu, c, o);
-        d += __shfl_xor_sync(0xffffffffu, d, o);
-      }
-      const long long S1 = (long long)a, S11 = (long long)c, S01 = (long long)d;
+    unsigned long long a0 = s1a, c0 = s11a, d0 = s01a, a1 = s1b, c1 = s11b, d1 = s01b;
+    for (int o = 16; o > 0; o >>= 1) {
+      a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+      c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+      d0 += __shfl_xor_sync(0xffffffffu, d0, o);
+      a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+      c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+      d1 += __shfl_xor_sync(0xffffffffu, d1, o);
+    }
+    if (lane < 2 && (lane == 0 || two)) {
+      const int k = lane == 0 ? k0 : k1;
+      const long long S1 = (long long)(lane == 0 ? a0 : a1), S11 = (long long)(lane == 0 ? c0 : c1);
+      const long long S01 = (long long)(lane == 0 ? d0 : d1);
       const long long num = Pl * S01 - S0 * S1;
       const long long d2 = Pl * S11 - S1 * S1;
       const double ncc = (double)num / sqrt(den1 * (double)d2);
-      const int idx = r * NU * NV + uv[k];
-      if (better_b(ncc, idx, bn[k], bi[k])) {
-        bn[k] = ncc;
-        bi[k] = idx;
+      const int idx = r * NU * NV + s_uv[k];
+      if (better_b(ncc, idx, s_bn[k][warp], s_bi[k][warp])) {
+        s_bn[k][warp] = ncc;
+        s_bi[k][warp] = idx;
       }
-    }
-  }
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < kBf16KeepMax; ++k) {
-      s_bn[warp][k] = bn[k];
-      s_bi[warp][k] = bi[k];
     }
   }
   __syncthreads();
   if (tid < kBf16KeepMax) {
     double fn = 0.0;
     int fi = INT_MAX;
-    for (int w = 0; w < 8; ++w)
-      if (better_b(s_bn[w][tid], s_bi[w][tid], fn, fi)) {
-        fn = s_bn[w][tid];
-        fi = s_bi[w][tid];
+    for (int w = 0; w < kW; ++w)
+      if (better_b(s_bn[tid][w], s_bi[tid][w], fn, fi)) {
+        fn = s_bn[tid][w];
+        fi = s_bi[tid][w];
       }
     rec[tid] = SearchBest{fn, fi, 0};
   }
@@ -769,7 +817,12 @@ size_t bf16_weight_entries(int half) {
   return 2 * (size_t)G.fw * G.nbf * kNRot;  // W, then M
 }
 
-bool bf16_supported(int max_r, int nrot) { return 2 * max_r + 1 < kMaxFoot && nrot >= 1 && nrot <= kNRot; }
+// The weights kernel counts the points landing on a pixel in 8 bits: a
+// rotated pattern puts at most 4 distinct offsets on one pixel, each repeated
+// at most max_dup times.
+bool bf16_supported(int max_r, int nrot, int max_dup) {
+  return 2 * max_r + 1 < kMaxFoot && nrot >= 1 && nrot <= kNRot && 4 * max_dup <= 255;
+}
 
 void prepare_search_bf16() {
   static bool done = false;
