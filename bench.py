@@ -422,19 +422,46 @@ def run_sequence(args, rank: int, world: int, local: int) -> int:
     return 0
 
 
-def gemm_flops(rec: np.ndarray, nrot_slots: int = 32) -> float:
+def gemm_flops(rec: np.ndarray, inc_rot: float = 0.005, num_rot: int = 10) -> float:
     """Tensor-core flops of one BF16 search launch over the 32x32 candidate
-    tile of each grain: footprint rows x 16-column chunks x 2 MMAs (cross
-    terms and second moments) of M=128 (4 x-shifts x 32 rotation slots) x
-    N=256 x K=16, footprint and rotation-slot padding included
-    (grain_diameter 1.0 patterns: half-extent = radius + 1)."""
+    tile of each grain: per footprint row, the 16-column chunks that touch a
+    block holding a point of some rotation step, 2 MMAs each (cross terms and
+    second moments) of M=128 (4 x-shifts x 32 rotation slots) x N=256 x K=16,
+    rotation-slot and chunk padding included (grain_diameter 1.0 discs at
+    reference rotation 0, rotated as rotate_pixel_pattern rotates them)."""
+    rotmax = abs(inc_rot * num_rot)
+    steps, a = [], -rotmax
+    while a <= rotmax:
+        steps.append(a)
+        a += inc_rot
+    per_radius = {}
     total = 0.0
     for r in rec[:, 3]:
-        half = max(int(r), 1) + 1
-        fw = 2 * half + 1
-        nbf = (fw + 7) // 8
-        nch = (nbf + 4) // 2
-        total += 2 * fw * nch * 2.0 * 128 * 256 * 16
+        R = max(int(r), 1)
+        if R not in per_radius:
+            half = R + 1
+            fw = 2 * half + 1
+            nbf = (fw + 7) // 8
+            nch = (nbf + 4) // 2
+            yy, xx = np.mgrid[-R:R + 1, -R:R + 1]
+            inside = xx * xx + yy * yy <= R * R
+            px, py = xx[inside].astype(float), yy[inside].astype(float)
+            lo = np.full(fw, 10 ** 6)
+            hi = np.full(fw, -1)
+            for t in steps:
+                c, sn = np.cos(t), np.sin(t)
+                qx = np.sign(c * px + sn * py) * np.floor(np.abs(c * px + sn * py) + 0.5)
+                qy = np.sign(-sn * px + c * py) * np.floor(np.abs(-sn * px + c * py) + 0.5)
+                row = (qy + half).astype(int)
+                blk = ((qx + half).astype(int)) // 8
+                np.minimum.at(lo, row, blk)
+                np.maximum.at(hi, row, blk)
+            n = 0
+            for y in range(fw):
+                if hi[y] >= 0:
+                    n += max(0, min(nch - 1, (hi[y] + 3) // 2) - lo[y] // 2 + 1)
+            per_radius[R] = n
+        total += per_radius[R] * 2 * 2.0 * 128 * 256 * 16
     return total
 
 

@@ -50,8 +50,10 @@
 //     W_r(y, f) * I(y + v, f + 24 - 8 j + s): candidate x offset 24 - 8 j + s
 //     (S likewise with M_r and the squares).  Two MMAs (M=128, N=256, K=16)
 //     cover the whole 32 x 32 x 32 tile for one row and chunk; a grain's tile
-//     takes 2 x (footprint rows) x (chunks) MMAs, issued by one thread per
-//     strip of rows and committed to an mbarrier.  D occupies tensor-memory
+//     takes 2 MMAs per footprint row and chunk touching a block that holds a
+//     point of some rotation step (the weights kernel records each row's
+//     first and last such block), issued by one thread per strip of rows and
+//     committed to an mbarrier.  D occupies tensor-memory
 //     columns 0..255, S columns 256..511.
 //   * The epilogue reads both accumulators with tcgen05.ld (warp w: lanes
 //     32 (w % 4).., columns 64 (w / 4)..), divides per rotation lane, takes
@@ -269,6 +271,11 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
   const int rows = G.fw * G.nbf;
   uint4* slotW = reinterpret_cast<uint4*>(p.wslots) + p.wofs[gi];
   uint4* slotM = slotW + (size_t)rows * kNRot;
+  __shared__ int s_rlo[kMaxFoot], s_rhi[kMaxFoot];
+  if (tid < G.fw) {
+    s_rlo[tid] = INT_MAX;
+    s_rhi[tid] = -1;
+  }
   const double base_rot = g.refrot[gi] + g.drot[gi];  // total_rot = base_rot + step, as the exact search
   if (tid < p.nrot) {
     double sr, cr;
@@ -310,6 +317,16 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
         m[j] = n;
         v[j] = (float)(c & 0xFFFFFFu) - n * mean0;
       }
+      {  // occupied blocks of the row, one atomic pair per row and warp
+        const bool occ = m[0] + m[1] + m[2] + m[3] + m[4] + m[5] + m[6] + m[7] > 0.0f;
+        const unsigned same = __match_any_sync(__activemask(), y);
+        const int lo = __reduce_min_sync(same, occ ? af : INT_MAX);
+        const int hi = __reduce_max_sync(same, occ ? af : -1);
+        if ((threadIdx.x & 31) == __ffs(same) - 1 && hi >= 0) {
+          atomicMin(&s_rlo[y], lo);
+          atomicMax(&s_rhi[y], hi);
+        }
+      }
       const size_t at = (size_t)rem * kNRot + r0 + k;
       slotW[at] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
                              pack_bf16x2(v[6], v[7]));
@@ -317,6 +334,13 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
                              pack_bf16x2(m[6], m[7]));
     }
     __syncthreads();
+  }
+  // per footprint row: the first and last 8-column block holding a point of
+  // any rotation step (an empty row: first > last)
+  unsigned char* rng = reinterpret_cast<unsigned char*>(slotM + (size_t)rows * kNRot);
+  if (tid < G.fw) {
+    rng[2 * tid] = (unsigned char)min(s_rlo[tid], 255);
+    rng[2 * tid + 1] = (unsigned char)max(s_rhi[tid], 0);
   }
 }
 
@@ -334,6 +358,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   __shared__ float2 s_csf[kNRot];
   __shared__ float s_cv[kWarps * kBf16KeepMax];
   __shared__ int s_ci[kWarps * kBf16KeepMax];
+  __shared__ unsigned char s_rng[2 * kMaxFoot];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t mbar = smem_u32(&s_mbar), wbar = smem_u32(&s_wbar);
 
@@ -393,6 +418,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     const size_t wrows = (size_t)G.fw * G.nbf * kNRot;
     const uint4* slotW = reinterpret_cast<const uint4*>(p.wslots) + p.wofs[gi];
     const uint4* slotM = slotW + wrows;
+    if (tid < 2 * G.fw) s_rng[tid] = reinterpret_cast<const unsigned char*>(slotM + wrows)[tid];
     const size_t abytes = (size_t)G.rs * G.wb * 512, hbytes = (size_t)(G.rs + 31) * G.hb * 128;
     unsigned char* sW = smem;
     unsigned char* sM = sW + abytes;
@@ -493,6 +519,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
         }
       };
       bool prefetched = false;
+      uint32_t acc = 0u;  // the tile's first MMA into each accumulator overwrites it
       for (int ys = 0; ys < G.fw; ys += G.rs) {
         const int nr = min(G.rs, G.fw - ys);
         const bool inside = staged(ys);
@@ -560,16 +587,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
             atomicOr(p.error, 1);
           } else {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            for (int yl = 0; yl < nr; ++yl)
-              for (int c = 0; c < G.nch; ++c) {
+            for (int yl = 0; yl < nr; ++yl) {
+              // chunk c reads footprint blocks 2c - 3 .. 2c + 1 (over the 4 x-shifts):
+              // the chunks touching the row's occupied blocks [lo, hi]
+              const int lo = s_rng[2 * (ys + yl)], hi = s_rng[2 * (ys + yl) + 1];
+              const int c1 = min(G.nch - 1, (hi + 3) >> 1);
+              for (int c = lo >> 1; c <= c1; ++c) {
                 const uint32_t ao = (uint32_t)((yl * G.wb + 2 * c) * 512);
                 const uint32_t bo = (uint32_t)((yl * G.hb + 2 * c) * 128);
-                const uint32_t acc = (ys == 0 && yl == 0 && c == 0) ? 0u : 1u;
                 mma_bf16(tmem, make_desc(wbase + ao, 512, 128), make_desc(habase + bo, 128, (uint32_t)(G.hb * 128)),
                          acc);
                 mma_bf16(tmem + 256u, make_desc(mbase + ao, 512, 128),
                          make_desc(hsbase + bo, 128, (uint32_t)(G.hb * 128)), acc);
+                acc = 1u;
               }
+            }
             mma_commit(mbar);
           }
         }
@@ -814,7 +846,8 @@ __global__ void __launch_bounds__(256, 4) k_rescore_bf16(Bf16Launch p) {
 // ---------------------------------------------------------------------------
 size_t bf16_weight_entries(int half) {
   const Geom G = geom_of(half);
-  return 2 * (size_t)G.fw * G.nbf * kNRot;  // W, then M
+  // W, M, per-row block ranges (2 fw <= 190 bytes, padded to keep slots 512-byte aligned)
+  return 2 * (size_t)G.fw * G.nbf * kNRot + kNRot;
 }
 
 // The weights kernel counts the points landing on a pixel in 8 bits: a
