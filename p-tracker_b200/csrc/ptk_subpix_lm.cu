@@ -11,8 +11,9 @@
 // gbar = mean g, n = |b|, c = sum b_i g_i / n:
 //     J^T J = (sum g g^T - P gbar gbar^T - c c^T) / n^2
 //     J^T r = -(sum a_i g_i / |a| - c NCC) / n
-// so one pass over the points accumulates 21 sums.  Samples, derivatives and
-// sums are FP32 (values centred on mean0 to avoid cancellation); the 3x3
+// so one pass over the points accumulates 18 sums.  Samples and derivatives
+// are FP32 (values centred on mean0 to avoid cancellation), the sums of the
+// objective FP64 and the derivative sums FP32; the 3x3
 // damped normal equations are solved in FP64 and X and the cumulative grain
 // state accumulate in FP64.
 //
@@ -65,6 +66,7 @@ struct LmEval {
 
 // Sums over the grain's points at X, reduced over the block in a fixed order
 // (every thread returns the same values).
+template <int NT>
 __device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain& o, const double X[3],
                           double (*part)[kNSums]) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -72,11 +74,14 @@ __device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain
   sincos(o.drot + X[2], &sr, &cr);
   const float c = (float)cr, s = (float)sr;
   const float bx = o.fx + (float)X[0], by = o.fy + (float)X[1];
+  // the objective's three sums accumulate in FP64 (they set the noise floor of
+  // the acceptance test), the derivative sums in FP32
+  double S0 = 0.0, S1 = 0.0, S2 = 0.0;
   float S[kNSums];
 #pragma unroll
-  for (int k = 0; k < kNSums; ++k) S[k] = 0.0f;
+  for (int k = 3; k < kNSums; ++k) S[k] = 0.0f;
   bool clamped = false;
-  for (int i = tid; i < o.P; i += kLmThreads) {
+  for (int i = tid; i < o.P; i += NT) {
     const short2 q = g.pat0[o.b + i];
     const float x = (float)q.x, y = (float)q.y;
     const float px = bx + c * x + s * y;
@@ -107,9 +112,9 @@ __device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain
     const float gr = gx * (-s * x + c * y) + gy * (-c * x - s * y);
     const float vc = v - o.mean0;
     const float a = u16f(g.w0[o.b + i]) - o.mean0;
-    S[0] += vc;
-    S[1] += vc * vc;
-    S[2] += a * vc;
+    S0 += (double)vc;
+    S1 = fma((double)vc, (double)vc, S1);
+    S2 = fma((double)a, (double)vc, S2);
     S[3] += gx;
     S[4] += gy;
     S[5] += gr;
@@ -129,7 +134,7 @@ __device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain
   // warp sums in FP64, then the warps' partial sums in index order
 #pragma unroll
   for (int k = 0; k < kNSums; ++k) {
-    double t = (double)S[k];
+    double t = k == 0 ? S0 : (k == 1 ? S1 : (k == 2 ? S2 : (double)S[k]));
     for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
     if (lane == 0) part[warp][k] = t;
   }
@@ -138,7 +143,7 @@ __device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain
 #pragma unroll
   for (int k = 0; k < kNSums; ++k) {
     double t = part[0][k];
-    for (int w = 1; w < kLmThreads / 32; ++w) t += part[w][k];
+    for (int w = 1; w < NT / 32; ++w) t += part[w][k];
     T[k] = t;
   }
   __syncthreads();  // part[] is rewritten by the next evaluation
@@ -202,7 +207,7 @@ __global__ void __launch_bounds__(kLmThreads) k_subpix_lm(GrainsDev g, FrameDev 
   const double rscale = g.radius[gi] > 1.0 ? g.radius[gi] : 1.0;  // rotation step in pixels at the rim
 
   double X[3] = {0.0, 0.0, 0.0};
-  LmEval cur_e = lm_eval(g, cur, o, X, part);
+  LmEval cur_e = lm_eval<kLmThreads>(g, cur, o, X, part);
   bool clamped = cur_e.clamped;
   double lambda = 1e-3;
   int it = 0, accepted = 0, rejected_run = 0;
@@ -217,7 +222,7 @@ __global__ void __launch_bounds__(kLmThreads) k_subpix_lm(GrainsDev g, FrameDev 
       const double step = fmax(fmax(fabs(d[0]), fabs(d[1])), fabs(d[2]) * rscale);
       if (step < lp.tol) break;
       const double Xn[3] = {X[0] + d[0], X[1] + d[1], X[2] + d[2]};
-      const LmEval ne = lm_eval(g, cur, o, Xn, part);
+      const LmEval ne = lm_eval<kLmThreads>(g, cur, o, Xn, part);
       if (isfinite(ne.F) && ne.F < cur_e.F) {
         X[0] = Xn[0];
         X[1] = Xn[1];
@@ -267,7 +272,7 @@ __global__ void __launch_bounds__(kLmThreads) k_grad_f32(GrainsDev g, FrameDev c
   o.mean0 = (float)g.mean0[gi];
   o.norm_a = sqrt(g.c0c0[gi]);
   const double X[3] = {Xall[3 * gi], Xall[3 * gi + 1], Xall[3 * gi + 2]};
-  const LmEval e = lm_eval(g, cur, o, X, part);
+  const LmEval e = lm_eval<kLmThreads>(g, cur, o, X, part);
   if (threadIdx.x == 0) {
     f[gi] = 1.0 - e.ncc;
     // d(1 - NCC)/dX = (1/2) dF/dX = J^T r
