@@ -643,12 +643,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
         const int ul = 24 - 8 * q + (lane & 7), vl = 8 * h + 4 * ch + (lane >> 3);
         sc[ch] = (u0 + ul <= u1 && v0 + vl <= v1 && mine != INT_MIN) ? key2f(mine) : -INFINITY;
       }
-      // per-warp best `keep`, then the block's best `keep` among them
+      // per-warp best `keep` (down to kKeepRelWeak below the warp's best: the
+      // tile's best is at least as high), then the block's best `keep` among them
+      float wtop = -INFINITY;
       for (int k = 0; k < keep; ++k) {
         const int bc = sc[1] > sc[0] ? 1 : (sc[0] > -INFINITY ? 0 : -1);
         const float bv = bc == 1 ? sc[1] : sc[0];
         const int key = (bc >= 0) ? f2key(bv) : INT_MIN;
         const int mkey = __reduce_max_sync(0xffffffffu, key);
+        if (k == 0) wtop = key2f(mkey);
+        if (mkey == INT_MIN || (k > 0 && wtop > 0.0f && key2f(mkey) < wtop * (1.0f - kKeepRelWeak))) {
+          if (lane == 0)
+            for (int r = k; r < keep; ++r) {
+              s_cv[warp * kBf16KeepMax + r] = -INFINITY;
+              s_ci[warp * kBf16KeepMax + r] = -1;
+            }
+          break;
+        }
         const unsigned who = __ballot_sync(0xffffffffu, key == mkey && bc >= 0);
         const int wl = who ? __ffs(who) - 1 : -1;
         int packed = -1;
@@ -695,7 +706,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
           }
           // candidates scoring more than `rel` below the tile's best are not rescored
           const bool near = !(top > 0.0f) || key2f(mkey) >= top * (1.0f - rel);
-          const unsigned who = near ? __ballot_sync(0xffffffffu, key == mkey && bi >= 0) : 0u;
+          if (k >= keep || !near || mkey == INT_MIN) {
+            if (lane == 0)
+              for (int r = k; r < kBf16KeepMax; ++r) topk[r] = make_int2(INT_MIN, INT_MIN);
+            break;
+          }
+          const unsigned who = __ballot_sync(0xffffffffu, key == mkey && bi >= 0);
           const int wl = who ? __ffs(who) - 1 : -1;
           int packed = -1;
           if (lane == wl) {
@@ -709,8 +725,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
           }
           packed = __shfl_sync(0xffffffffu, packed, wl >= 0 ? wl : 0);
           if (lane == 0)
-            topk[k] = (k < keep && wl >= 0 && packed >= 0) ? make_int2(u0 + (packed >> 8), v0 + (packed & 0xff))
-                                                            : make_int2(INT_MIN, INT_MIN);
+            topk[k] = (wl >= 0 && packed >= 0) ? make_int2(u0 + (packed >> 8), v0 + (packed & 0xff))
+                                               : make_int2(INT_MIN, INT_MIN);
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;");
