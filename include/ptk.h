@@ -98,7 +98,7 @@ typedef struct ptk_config {
   int32_t search_method;         /* PTK_SEARCH_*, default EXACT               */
   int32_t topk;                  /* BF16 search: candidates per 32x32 tile rescored exactly, those within 3 % of its best score (1..8, default 8) */
   int32_t lm_max_iter;           /* adjoint LM: iteration cap                 */
-  double lm_tol;                 /* adjoint LM: step tolerance (pixels)       */
+  double lm_tol;                 /* adjoint LM: step tolerance (pixels, default 1e-4) */
 } ptk_config;
 
 typedef struct ptk_ctx ptk_ctx;

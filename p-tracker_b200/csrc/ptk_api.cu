@@ -558,7 +558,7 @@ int enqueue_subpixel(ptk_ctx* c, int method, cudaStream_t s) {
       return fail(c, PTK_ERR_ARG, "the adjoint LM refinement is implemented for the cubic interpolator");
     LmParams lp;
     lp.max_iter = c->cfg.lm_max_iter > 0 ? c->cfg.lm_max_iter : 30;
-    lp.tol = c->cfg.lm_tol > 0.0 ? c->cfg.lm_tol : 1e-6;
+    lp.tol = c->cfg.lm_tol > 0.0 ? c->cfg.lm_tol : 1e-4;
     lp.iters = nullptr;
     lp.order = c->d_order;
     launch_subpix_lm(c->g, frame(c, c->cur_slot), lp, s);
@@ -635,7 +635,7 @@ int ptk_config_default(ptk_config* cfg) {
   cfg->search_method = PTK_SEARCH_EXACT;
   cfg->topk = 8;
   cfg->lm_max_iter = 30;
-  cfg->lm_tol = 1e-6;
+  cfg->lm_tol = 1e-4;
   return PTK_OK;
 }
 
