@@ -97,6 +97,8 @@ constexpr float kKeepRel = 0.03f;
 constexpr float kKeepRelWeak = 0.10f;
 constexpr float kGoodMatch = 0.9f;
 constexpr long kWaitLimit = 1L << 22;
+// operand rows in flight: W_r and M_r of one footprint row per ring buffer
+constexpr int kRing = 4;
 // weights kernel: 512 threads, 64 KB of 32-bit maps
 constexpr int kWThreads = 512;
 constexpr int kWSmem = 64 * 1024;
@@ -113,7 +115,7 @@ struct Geom {
   int wb;    // weight blocks per row in shared memory (3 leading zero blocks)
   int hb;    // Hankel blocks per image row
   int rp;    // bytes per staged image row (the Hankel's 8 hb + 7 pixels from a 16-byte boundary)
-  int rs;    // footprint rows per strip
+  int rs;    // footprint rows per strip (Hankel rows filled at once, plus 31)
 };
 
 __host__ __device__ inline Geom geom_of(int half) {
@@ -125,11 +127,10 @@ __host__ __device__ inline Geom geom_of(int half) {
   g.wb = 2 * g.nch + 3;
   g.hb = 2 * g.nch;
   g.rp = 16 * g.hb + 32;
-  // W and M rows, two Hankel buffers and the staged image rows, the last
-  // three with 31 rows of halo
+  // the operand-row ring, then two Hankel buffers and the staged image rows
+  // with 31 rows of halo
   const int halo_row = 2 * g.hb * 128 + g.rp;
-  const int per_row = 2 * g.wb * 512 + halo_row;
-  int rs = (kSmemBudget - 31 * halo_row) / per_row;
+  int rs = (kSmemBudget - kRing * 2 * g.wb * 512) / halo_row - 31;
   if (rs > g.fw) rs = g.fw;
   g.rs = rs < 1 ? 1 : rs;
   return g;
@@ -351,7 +352,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   extern __shared__ __align__(128) unsigned char smem_bf[];
   unsigned char* smem = smem_bf;
   __shared__ __align__(8) unsigned long long s_mbar;   // MMA completion
-  __shared__ __align__(8) unsigned long long s_wbar;   // operand-row bulk copies
+  __shared__ __align__(8) unsigned long long s_full[kRing];  // operand row copied into a ring buffer
+  __shared__ __align__(8) unsigned long long s_free[kRing];  // the MMAs reading a ring buffer completed
   __shared__ uint32_t s_tmem;
   __shared__ int s_li, s_err, s_bb[4];
   __shared__ double2 s_cs[kNRot];
@@ -360,7 +362,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   __shared__ int s_ci[kWarps * kBf16KeepMax];
   __shared__ unsigned char s_rng[2 * kMaxFoot];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t mbar = smem_u32(&s_mbar), wbar = smem_u32(&s_wbar);
+  const uint32_t mbar = smem_u32(&s_mbar);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -369,7 +371,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(wbar));
+    for (int k = 0; k < kRing; ++k) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_full[k])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_free[k])));
+    }
     asm volatile("fence.mbarrier_init.release.cluster;");
     s_err = 0;
   }
@@ -377,8 +382,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = s_tmem;
-  uint32_t parity = 0, wparity = 0;
+  uint32_t parity = 0;
   int zhalf = -1;  // footprint geometry whose zero blocks the operand rows hold
+  // operand rows through the ring (thread 0): sequence numbers of the next row
+  // to copy and of the next row to consume; row n uses buffer n % kRing
+  unsigned iseq = 0, cseq = 0;
 
   const GrainsDev& g = p.g;
   const int count = *p.list_count;
@@ -419,25 +427,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     const uint4* slotW = reinterpret_cast<const uint4*>(p.wslots) + p.wofs[gi];
     const uint4* slotM = slotW + wrows;
     if (tid < 2 * G.fw) s_rng[tid] = reinterpret_cast<const unsigned char*>(slotM + wrows)[tid];
-    const size_t abytes = (size_t)G.rs * G.wb * 512, hbytes = (size_t)(G.rs + 31) * G.hb * 128;
-    unsigned char* sW = smem;
-    unsigned char* sM = sW + abytes;
-    unsigned char* sHa = sM + abytes;
+    // ring buffer k: W row at k * 2 wb * 512, M row wb * 512 after it
+    const size_t hbytes = (size_t)(G.rs + 31) * G.hb * 128;
+    unsigned char* sA = smem;
+    unsigned char* sHa = sA + (size_t)kRing * 2 * G.wb * 512;
     unsigned char* sHs = sHa + hbytes;
     unsigned char* sR = sHs + hbytes;
-    const uint32_t wbase = smem_u32(sW), mbase = smem_u32(sM), habase = smem_u32(sHa), hsbase = smem_u32(sHs);
+    const uint32_t abase = smem_u32(sA), habase = smem_u32(sHa), hsbase = smem_u32(sHs);
     const uint32_t rbase = smem_u32(sR);
     // zero blocks of every operand row (3 in front, the rest after the footprint);
     // the copies never write them, so they stay valid while the geometry does
     // (grains come in decreasing pattern size)
     if (G.half != zhalf) {
-      for (int e = tid; e < G.rs * (G.wb - G.nbf) * kNRot; e += kThreads) {
-        const int yl = e / ((G.wb - G.nbf) * kNRot), rem = e - yl * ((G.wb - G.nbf) * kNRot);
+      for (int e = tid; e < 2 * kRing * (G.wb - G.nbf) * kNRot; e += kThreads) {
+        const int row = e / ((G.wb - G.nbf) * kNRot), rem = e - row * ((G.wb - G.nbf) * kNRot);
         const int zb = rem >> 5, r = rem & 31;
         const int a = zb < 3 ? zb : zb + G.nbf;
-        const size_t at = ((size_t)yl * G.wb + a) * kNRot + r;
-        reinterpret_cast<uint4*>(sW)[at] = make_uint4(0, 0, 0, 0);
-        reinterpret_cast<uint4*>(sM)[at] = make_uint4(0, 0, 0, 0);
+        reinterpret_cast<uint4*>(sA)[((size_t)row * G.wb + a) * kNRot + r] = make_uint4(0, 0, 0, 0);
       }
       zhalf = G.half;
     }
@@ -518,23 +524,36 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
                      p.cur.pix + (size_t)(Yi + ys_ + rho) * p.cur.pitch + Xa + 8 * c);
         }
       };
+      // Operand rows stream through the ring (thread 0): row y of the tile is
+      // sequence number tile0 + y; its copy waits for the MMAs of the row that
+      // used the buffer before (kRing rows earlier), and is issued kRing - 1
+      // rows ahead of its MMAs, so the copies overlap the fills and MMAs.
+      const unsigned tile0 = iseq;
+      auto issue_row = [&](int y) -> bool {  // thread 0
+        const unsigned n = tile0 + (unsigned)y, k = n % kRing;
+        if (n >= (unsigned)kRing && !mbar_wait(smem_u32(&s_free[k]), ((n / kRing) - 1) & 1u)) return false;
+        const uint32_t full = smem_u32(&s_full[k]);
+        mbar_expect_tx(full, (uint32_t)(2 * G.nbf * 512));
+        const uint32_t dst = abase + (uint32_t)(k * 2 * G.wb * 512 + 3 * 512);
+        const size_t src = (size_t)y * G.nbf * kNRot;
+        bulk_g2s(dst, slotW + src, (uint32_t)(G.nbf * 512), full);
+        bulk_g2s(dst + (uint32_t)(G.wb * 512), slotM + src, (uint32_t)(G.nbf * 512), full);
+        ++iseq;
+        return true;
+      };
+      if (tid == 0)
+        for (int y = 0; y < min(kRing - 1, G.fw); ++y)
+          if (!issue_row(y)) {
+            s_err = 1;
+            atomicOr(p.error, 1);
+            break;
+          }
       bool prefetched = false;
       uint32_t acc = 0u;  // the tile's first MMA into each accumulator overwrites it
       for (int ys = 0; ys < G.fw; ys += G.rs) {
         const int nr = min(G.rs, G.fw - ys);
         const bool inside = staged(ys);
         if (inside && !prefetched) stage_rows(ys);
-        if (warp == 0) {  // operand rows ys .. ys + nr - 1: one bulk copy per row and operand (whole blocks)
-          if (lane == 0) mbar_expect_tx(wbar, (uint32_t)(2 * nr * G.nbf * 512));
-          __syncwarp();
-          for (int e = lane; e < 2 * nr; e += 32) {
-            const int yl = e >> 1;
-            const uint32_t dst = (uint32_t)((yl * G.wb + 3) * 512);
-            const size_t src = (size_t)(ys + yl) * G.nbf * kNRot;
-            if (e & 1) bulk_g2s(mbase + dst, slotM + src, (uint32_t)(G.nbf * 512), wbar);
-            else bulk_g2s(wbase + dst, slotW + src, (uint32_t)(G.nbf * 512), wbar);
-          }
-        }
         if (inside && !prefetched) {  // (a prefetch completed before the previous strip's last barrier)
           cp_async_wait_all();
           __syncthreads();
@@ -581,31 +600,40 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
         // the staged rows are consumed: bring in the next strip's during these MMAs
         prefetched = ys + G.rs < G.fw && staged(ys + G.rs);
         if (prefetched) stage_rows(ys + G.rs);
-        if (tid == 0) {
-          if (!mbar_wait(wbar, wparity)) {
-            s_err = 1;
-            atomicOr(p.error, 1);
-          } else {
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            for (int yl = 0; yl < nr; ++yl) {
-              // chunk c reads footprint blocks 2c - 3 .. 2c + 1 (over the 4 x-shifts):
-              // the chunks touching the row's occupied blocks [lo, hi]
-              const int lo = s_rng[2 * (ys + yl)], hi = s_rng[2 * (ys + yl) + 1];
-              const int c1 = min(G.nch - 1, (hi + 3) >> 1);
-              for (int c = lo >> 1; c <= c1; ++c) {
-                const uint32_t ao = (uint32_t)((yl * G.wb + 2 * c) * 512);
-                const uint32_t bo = (uint32_t)((yl * G.hb + 2 * c) * 128);
-                mma_bf16(tmem, make_desc(wbase + ao, 512, 128), make_desc(habase + bo, 128, (uint32_t)(G.hb * 128)),
-                         acc);
-                mma_bf16(tmem + 256u, make_desc(mbase + ao, 512, 128),
-                         make_desc(hsbase + bo, 128, (uint32_t)(G.hb * 128)), acc);
-                acc = 1u;
-              }
+        if (tid == 0 && !s_err) {
+          for (int yl = 0; yl < nr; ++yl) {
+            const int y = ys + yl;
+            const unsigned n = tile0 + (unsigned)y, k = n % kRing;
+            if (!mbar_wait(smem_u32(&s_full[k]), (n / kRing) & 1u)) {
+              s_err = 1;
+              atomicOr(p.error, 1);
+              break;
             }
-            mma_commit(mbar);
+            ++cseq;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            // chunk c reads footprint blocks 2c - 3 .. 2c + 1 (over the 4 x-shifts):
+            // the chunks touching the row's occupied blocks [lo, hi]
+            const int lo = s_rng[2 * y], hi = s_rng[2 * y + 1];
+            const int c1 = min(G.nch - 1, (hi + 3) >> 1);
+            const uint32_t wrow = abase + (uint32_t)(k * 2 * G.wb * 512), mrow = wrow + (uint32_t)(G.wb * 512);
+            for (int c = lo >> 1; c <= c1; ++c) {
+              const uint32_t ao = (uint32_t)(2 * c * 512);
+              const uint32_t bo = (uint32_t)((yl * G.hb + 2 * c) * 128);
+              mma_bf16(tmem, make_desc(wrow + ao, 512, 128), make_desc(habase + bo, 128, (uint32_t)(G.hb * 128)),
+                       acc);
+              mma_bf16(tmem + 256u, make_desc(mrow + ao, 512, 128),
+                       make_desc(hsbase + bo, 128, (uint32_t)(G.hb * 128)), acc);
+              acc = 1u;
+            }
+            mma_commit(smem_u32(&s_free[k]));
+            if (y + kRing - 1 < G.fw && !issue_row(y + kRing - 1)) {
+              s_err = 1;
+              atomicOr(p.error, 1);
+              break;
+            }
           }
+          if (!s_err) mma_commit(mbar);
         }
-        wparity ^= 1u;
         // one thread waits for the MMAs; the others rest at the barrier
         if (tid == 0 && !s_err) {
           if (!mbar_wait(mbar, parity)) {
@@ -736,8 +764,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   }
   cp_async_wait_all();
   __syncthreads();
-  if (s_err && tid == 0) {  // one more bounded wait on the last armed copy and MMA phases
-    mbar_wait(wbar, wparity ^ 1u);
+  if (s_err && tid == 0) {  // bounded waits on the copies still in flight and the last MMA phase
+    for (unsigned n = cseq; n < iseq; ++n) mbar_wait(smem_u32(&s_full[n % kRing]), (n / kRing) & 1u);
     mbar_wait(mbar, parity ^ 1u);
   }
   asm volatile("tcgen05.fence::after_thread_sync;");
