@@ -98,7 +98,8 @@ constexpr float kKeepRelWeak = 0.10f;
 constexpr float kGoodMatch = 0.9f;
 constexpr long kWaitLimit = 1L << 22;
 // operand rows in flight: W_r and M_r of one footprint row per ring buffer
-constexpr int kRing = 4;
+constexpr int kRing = 8;       // barrier slots
+constexpr int kRingUsed = 4;   // buffers
 // weights kernel: 512 threads, 64 KB of 32-bit maps
 constexpr int kWThreads = 512;
 constexpr int kWSmem = 64 * 1024;
@@ -116,6 +117,7 @@ struct Geom {
   int hb;    // Hankel blocks per image row
   int rp;    // bytes per staged image row (the Hankel's 8 hb + 7 pixels from a 16-byte boundary)
   int rs;    // footprint rows per strip (Hankel rows filled at once, plus 31)
+  int nb;    // operand-row ring buffers
 };
 
 __host__ __device__ inline Geom geom_of(int half) {
@@ -130,9 +132,11 @@ __host__ __device__ inline Geom geom_of(int half) {
   // the operand-row ring, then two Hankel buffers and the staged image rows
   // with 31 rows of halo
   const int halo_row = 2 * g.hb * 128 + g.rp;
-  int rs = (kSmemBudget - kRing * 2 * g.wb * 512) / halo_row - 31;
+  const int nb = kRingUsed;
+  int rs = (kSmemBudget - nb * 2 * g.wb * 512) / halo_row - 31;
   if (rs > g.fw) rs = g.fw;
   g.rs = rs < 1 ? 1 : rs;
+  g.nb = nb;
   return g;
 }
 
@@ -354,6 +358,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   __shared__ __align__(8) unsigned long long s_mbar;   // MMA completion
   __shared__ __align__(8) unsigned long long s_full[kRing];  // operand row copied into a ring buffer
   __shared__ __align__(8) unsigned long long s_free[kRing];  // the MMAs reading a ring buffer completed
+  // operand rows through the ring (thread 0): uses of each buffer copied and
+  // consumed so far (a buffer's barriers complete one phase per use)
+  __shared__ unsigned s_iss[kRing], s_con[kRing];
   __shared__ uint32_t s_tmem;
   __shared__ int s_li, s_err, s_bb[4];
   __shared__ double2 s_cs[kNRot];
@@ -377,6 +384,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     }
     asm volatile("fence.mbarrier_init.release.cluster;");
     s_err = 0;
+    for (int k = 0; k < kRing; ++k) s_iss[k] = s_con[k] = 0u;
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
@@ -384,9 +392,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   const uint32_t tmem = s_tmem;
   uint32_t parity = 0;
   int zhalf = -1;  // footprint geometry whose zero blocks the operand rows hold
-  // operand rows through the ring (thread 0): sequence numbers of the next row
-  // to copy and of the next row to consume; row n uses buffer n % kRing
-  unsigned iseq = 0, cseq = 0;
 
   const GrainsDev& g = p.g;
   const int count = *p.list_count;
@@ -430,7 +435,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     // ring buffer k: W row at k * 2 wb * 512, M row wb * 512 after it
     const size_t hbytes = (size_t)(G.rs + 31) * G.hb * 128;
     unsigned char* sA = smem;
-    unsigned char* sHa = sA + (size_t)kRing * 2 * G.wb * 512;
+    unsigned char* sHa = sA + (size_t)G.nb * 2 * G.wb * 512;
     unsigned char* sHs = sHa + hbytes;
     unsigned char* sR = sHs + hbytes;
     const uint32_t abase = smem_u32(sA), habase = smem_u32(sHa), hsbase = smem_u32(sHs);
@@ -439,7 +444,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     // the copies never write them, so they stay valid while the geometry does
     // (grains come in decreasing pattern size)
     if (G.half != zhalf) {
-      for (int e = tid; e < 2 * kRing * (G.wb - G.nbf) * kNRot; e += kThreads) {
+      for (int e = tid; e < 2 * G.nb * (G.wb - G.nbf) * kNRot; e += kThreads) {
         const int row = e / ((G.wb - G.nbf) * kNRot), rem = e - row * ((G.wb - G.nbf) * kNRot);
         const int zb = rem >> 5, r = rem & 31;
         const int a = zb < 3 ? zb : zb + G.nbf;
@@ -524,25 +529,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
                      p.cur.pix + (size_t)(Yi + ys_ + rho) * p.cur.pitch + Xa + 8 * c);
         }
       };
-      // Operand rows stream through the ring (thread 0): row y of the tile is
-      // sequence number tile0 + y; its copy waits for the MMAs of the row that
-      // used the buffer before (kRing rows earlier), and is issued kRing - 1
-      // rows ahead of its MMAs, so the copies overlap the fills and MMAs.
-      const unsigned tile0 = iseq;
+      // Operand rows stream through the ring (thread 0): row y of the tile goes
+      // to buffer y % nb; its copy waits for the MMAs of the row that used the
+      // buffer before (nb rows earlier), and is issued nb - 1 rows ahead of its
+      // MMAs, so the copies overlap the fills and MMAs.
+      const int NB = G.nb;
       auto issue_row = [&](int y) -> bool {  // thread 0
-        const unsigned n = tile0 + (unsigned)y, k = n % kRing;
-        if (n >= (unsigned)kRing && !mbar_wait(smem_u32(&s_free[k]), ((n / kRing) - 1) & 1u)) return false;
+        const int k = y % NB;
+        const unsigned use = s_iss[k];
+        if (use > 0 && !mbar_wait(smem_u32(&s_free[k]), (use - 1) & 1u)) return false;
         const uint32_t full = smem_u32(&s_full[k]);
         mbar_expect_tx(full, (uint32_t)(2 * G.nbf * 512));
         const uint32_t dst = abase + (uint32_t)(k * 2 * G.wb * 512 + 3 * 512);
         const size_t src = (size_t)y * G.nbf * kNRot;
         bulk_g2s(dst, slotW + src, (uint32_t)(G.nbf * 512), full);
         bulk_g2s(dst + (uint32_t)(G.wb * 512), slotM + src, (uint32_t)(G.nbf * 512), full);
-        ++iseq;
+        s_iss[k] = use + 1;
         return true;
       };
       if (tid == 0)
-        for (int y = 0; y < min(kRing - 1, G.fw); ++y)
+        for (int y = 0; y < min(NB - 1, G.fw); ++y)
           if (!issue_row(y)) {
             s_err = 1;
             atomicOr(p.error, 1);
@@ -603,13 +609,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
         if (tid == 0 && !s_err) {
           for (int yl = 0; yl < nr; ++yl) {
             const int y = ys + yl;
-            const unsigned n = tile0 + (unsigned)y, k = n % kRing;
-            if (!mbar_wait(smem_u32(&s_full[k]), (n / kRing) & 1u)) {
+            const int k = y % NB;
+            const unsigned use = s_con[k];
+            if (!mbar_wait(smem_u32(&s_full[k]), use & 1u)) {
               s_err = 1;
               atomicOr(p.error, 1);
               break;
             }
-            ++cseq;
+            s_con[k] = use + 1;
             asm volatile("tcgen05.fence::after_thread_sync;");
             // chunk c reads footprint blocks 2c - 3 .. 2c + 1 (over the 4 x-shifts):
             // the chunks touching the row's occupied blocks [lo, hi]
@@ -626,7 +633,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
               acc = 1u;
             }
             mma_commit(smem_u32(&s_free[k]));
-            if (y + kRing - 1 < G.fw && !issue_row(y + kRing - 1)) {
+            if (y + NB - 1 < G.fw && !issue_row(y + NB - 1)) {
               s_err = 1;
               atomicOr(p.error, 1);
               break;
@@ -765,7 +772,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   cp_async_wait_all();
   __syncthreads();
   if (s_err && tid == 0) {  // bounded waits on the copies still in flight and the last MMA phase
-    for (unsigned n = cseq; n < iseq; ++n) mbar_wait(smem_u32(&s_full[n % kRing]), (n / kRing) & 1u);
+    for (int k = 0; k < kRing; ++k)
+      for (unsigned u = s_con[k]; u < s_iss[k]; ++u) mbar_wait(smem_u32(&s_full[k]), u & 1u);
     mbar_wait(mbar, parity ^ 1u);
   }
   asm volatile("tcgen05.fence::after_thread_sync;");
