@@ -296,17 +296,28 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
     const int nb = min(nb_max, p.nrot - r0);
     for (int e = tid; e < nb * fw2; e += kWThreads) map[e] = 0u;
     __syncthreads();
-    for (int i = tid; i < P; i += kWThreads) {
-      const short2 q0 = g.pat[b + i];
-      // at most 255 points share a pixel (bf16_supported): the sum stays below 2^24
-      const unsigned add = (unsigned)g.w0[b + i] + (1u << 24);
-      for (int k = 0; k < nb; ++k) {
-        const float2 cf = s_csf[r0 + k];
-        const double2 cd = s_cs[r0 + k];
-        const short2 q = rotate_round_fast(q0, cf.x, cf.y, cd.x, cd.y);
-        // |q| <= ceil(|p|) = half - 1: always inside the footprint
-        const unsigned fx = (unsigned)(q.x + G.half), fy = (unsigned)(q.y + G.half);
-        if (fx < (unsigned)G.fw && fy < (unsigned)G.fw) atomicAdd(&map[k * fw2 + fy * G.fw + fx], add);
+    // four points per thread at a time: their loads are in flight together
+    for (int i0 = tid; i0 < P; i0 += 4 * kWThreads) {
+      short2 q0[4];
+      unsigned add[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u * kWThreads;
+        q0[u] = i < P ? g.pat[b + i] : make_short2(0, 0);
+        // at most 255 points share a pixel (bf16_supported): the sum stays below 2^24
+        add[u] = i < P ? (unsigned)g.w0[b + i] + (1u << 24) : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (i0 + u * kWThreads >= P) break;
+        for (int k = 0; k < nb; ++k) {
+          const float2 cf = s_csf[r0 + k];
+          const double2 cd = s_cs[r0 + k];
+          const short2 q = rotate_round_fast(q0[u], cf.x, cf.y, cd.x, cd.y);
+          // |q| <= ceil(|p|) = half - 1: always inside the footprint
+          const unsigned fx = (unsigned)(q.x + G.half), fy = (unsigned)(q.y + G.half);
+          if (fx < (unsigned)G.fw && fy < (unsigned)G.fw) atomicAdd(&map[k * fw2 + fy * G.fw + fx], add[u]);
+        }
       }
     }
     __syncthreads();
