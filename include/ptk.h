@@ -263,6 +263,44 @@ int ptk_read_image_file(const char* path, uint16_t* out, size_t capacity, int* d
                         int datetime_len);
 const char* ptk_image_error(void);
 
+/* Distortion-parameter fit: the minimisation of the correction_distortion
+ * procedure (src/distortion_correction.cpp:135-479) over grains tracked from
+ * a reference image into n_tracked images.
+ * ptk_disto_pairs: precompute_paires (src/distortion_correction.cpp:63-81),
+ *   the pairs (i < j, i-major) whose reference positions lie dmin .. dmax
+ *   apart; host only.  Writes at most `capacity` pairs (2 ints each) and the
+ *   count to *npairs (PTK_ERR_LIMIT when it exceeds capacity).
+ * ptk_disto_create: uploads the grains' reference positions, their tracked
+ *   displacements and subpixel NCC per image ([image][grain], images after the
+ *   reference) and the pairs.
+ * ptk_disto_objective: the equiprojectivity criterion (the POWELL functor,
+ *   :249-290) for the 14 undistor parameters, evaluated on the GPU in FP64;
+ *   ptk_disto_residuals also returns the residual of every (image, pair),
+ *   image-major, 0 where a pair is skipped (NCC below NCC_min).
+ * ptk_disto_fit: default centres (negative xc/yc entries -> the frame centre),
+ *   then POWELL (one minimisation, ftol 1e-12, initial directions the
+ *   perturbations) or POWELL_ITER (num_iter minimisations, each followed by
+ *   re-anchoring on the undistorted reference positions, :300-386); params14
+ *   in/out, index_ini / index_end = criterion / n_tracked before and after,
+ *   history (may be NULL) = num_iter x 15 (index, 14 parameters) for
+ *   POWELL_ITER.  The reference's LEVMAR uses lmdif1 from the absent toofus
+ *   library and is rejected (PTK_ERR_ARG).
+ * ptk_disto_tracked: the displacements after POWELL_ITER's re-anchoring. */
+typedef struct ptk_disto ptk_disto;
+enum { PTK_DISTO_POWELL = 0, PTK_DISTO_POWELL_ITER = 1, PTK_DISTO_LEVMAR = 2 };
+int ptk_disto_pairs(const int32_t* refx, const int32_t* refy, int n, double dmin, double dmax, int32_t* pairs_ij,
+                    int64_t capacity, int64_t* npairs);
+int ptk_disto_create(ptk_disto** out, int dimx, int dimy, const int32_t* refx, const int32_t* refy, int n,
+                     int n_tracked, const double* dx, const double* dy, const double* ncc_subpix, double NCC_min,
+                     const int32_t* pairs_ij, int64_t npairs);
+int ptk_disto_destroy(ptk_disto* d);
+const char* ptk_disto_last_error(ptk_disto* d);
+int ptk_disto_objective(ptk_disto* d, const double* params14, double* value);
+int ptk_disto_residuals(ptk_disto* d, const double* params14, double* value, double* fvec);
+int ptk_disto_fit(ptk_disto* d, double* params14, const double* perturb14, int algo, int num_iter,
+                  double* index_ini, double* index_end, double* history);
+int ptk_disto_tracked(ptk_disto* d, double* dx, double* dy);
+
 #ifdef __cplusplus
 }
 #endif

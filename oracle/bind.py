@@ -233,6 +233,86 @@ def undistor(params14, xd: float, yd: float):
     return xu.value, yu.value
 
 
+def _disto_lib(reference: bool):
+    return C.CDLL(str(REF_SO if reference else PORT_SO))
+
+
+def disto_pairs(refx, refy, dmin: float, dmax: float, reference: bool = False) -> np.ndarray:
+    """precompute_paires: the port's restatement, or the reference's member
+    function run on grains placed at refx, refy."""
+    L = _disto_lib(reference)
+    rx = np.ascontiguousarray(refx, dtype=np.int32)
+    ry = np.ascontiguousarray(refy, dtype=np.int32)
+    n = rx.shape[0]
+    cap = n * (n - 1) // 2 + 1
+    out = np.zeros((cap, 2), dtype=np.int32)
+    if reference:
+        L.ref_create.restype = _P
+        L.ref_disto_pairs.restype = C.c_int64
+        h = C.c_void_p(L.ref_create(8, 8))
+        np_ = L.ref_disto_pairs(h, _p(rx), _p(ry), _I(n), _D(dmin), _D(dmax), _p(out), C.c_int64(cap))
+        L.ref_destroy(h)
+    else:
+        L.orc_disto_pairs.restype = C.c_int64
+        np_ = L.orc_disto_pairs(_p(rx), _p(ry), _I(n), _D(dmin), _D(dmax), _p(out), C.c_int64(cap))
+    return out[:np_].copy()
+
+
+def disto_objective(params14, refx, refy, dx, dy, ncc, NCC_min: float, pairs, origx=None, origy=None,
+                    reference: bool = False, with_residuals: bool = False):
+    """The equiprojectivity criterion (POWELL functor; with origx/origy the
+    POWELL_ITER functor): the port's restatement, or the loop around the
+    reference's own undistor."""
+    L = _disto_lib(reference)
+    X = np.ascontiguousarray(params14, dtype=np.float64)
+    rx = np.ascontiguousarray(refx, dtype=np.int32)
+    ry = np.ascontiguousarray(refy, dtype=np.int32)
+    ddx = np.ascontiguousarray(dx, dtype=np.float64)
+    ddy = np.ascontiguousarray(dy, dtype=np.float64)
+    nc = np.ascontiguousarray(ncc, dtype=np.float64)
+    pr = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+    n, nimg1 = rx.shape[0], ddx.shape[0]
+    use_orig = origx is not None
+    ox = np.ascontiguousarray(origx if use_orig else rx, dtype=np.float64)
+    oy = np.ascontiguousarray(origy if use_orig else ry, dtype=np.float64)
+    if reference:
+        L.ref_create.restype = _P
+        L.ref_disto_objective.restype = _D
+        h = C.c_void_p(L.ref_create(8, 8))
+        v = L.ref_disto_objective(h, _p(X), _p(rx), _p(ry), _p(ox), _p(oy), _I(n), _I(nimg1), _p(ddx), _p(ddy), _p(nc),
+                                  _D(NCC_min), _p(pr), C.c_int64(pr.shape[0]), _I(int(use_orig)))
+        L.ref_destroy(h)
+        return v
+    L.orc_disto_objective.restype = _D
+    f = np.zeros(nimg1 * pr.shape[0])
+    v = L.orc_disto_objective(_p(X), _p(rx), _p(ry), _p(ox), _p(oy), _I(n), _I(nimg1), _p(ddx), _p(ddy), _p(nc),
+                              _D(NCC_min), _p(pr), C.c_int64(pr.shape[0]), _I(int(use_orig)),
+                              _p(f) if with_residuals else None)
+    return (v, f) if with_residuals else v
+
+
+def disto_fit(params14, perturb14, algo: int, num_iter: int, dimx: int, dimy: int, refx, refy, dx, dy, ncc,
+              NCC_min: float, pairs):
+    """The port's minimisation of correction_distortion (POWELL = 0,
+    POWELL_ITER = 1) with the oracle Powell; returns (params, index_ini,
+    index_end, history, dx, dy)."""
+    L = _disto_lib(False)
+    X = np.array(params14, dtype=np.float64)
+    DX = np.ascontiguousarray(perturb14, dtype=np.float64)
+    rx = np.ascontiguousarray(refx, dtype=np.int32)
+    ry = np.ascontiguousarray(refy, dtype=np.int32)
+    ddx = np.array(dx, dtype=np.float64)
+    ddy = np.array(dy, dtype=np.float64)
+    nc = np.ascontiguousarray(ncc, dtype=np.float64)
+    pr = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+    ini, end = C.c_double(), C.c_double()
+    hist = np.zeros((max(num_iter, 1), 15))
+    L.orc_disto_fit(_p(X), _p(DX), _I(algo), _I(num_iter), _I(dimx), _I(dimy), _p(rx), _p(ry), _I(rx.shape[0]),
+                    _I(ddx.shape[0]), _p(ddx), _p(ddy), _p(nc), _D(NCC_min), _p(pr), C.c_int64(pr.shape[0]),
+                    C.byref(ini), C.byref(end), _p(hist))
+    return X, ini.value, end.value, (hist[:num_iter] if algo == 1 else hist[:0]), ddx, ddy
+
+
 def remap(params14, src: np.ndarray, threads: int = 1) -> np.ndarray:
     L = C.CDLL(str(PORT_SO))
     p = np.ascontiguousarray(params14, dtype=np.float64)

@@ -722,6 +722,140 @@ void orc_undistor(const double* params14, double xd, double yd, double* xu, doub
   undistor(params14, xd, yd, xu, yu);
 }
 
+// precompute_paires, src/distortion_correction.cpp:63-81: the pairs (i < j) of
+// grains whose reference positions lie dmin .. dmax apart, i-major.  Writes at
+// most cap pairs (i, j) and returns the count.
+int64_t orc_disto_pairs(const int32_t* refx, const int32_t* refy, int n, double dmin, double dmax, int32_t* out,
+                        int64_t cap) {
+  int64_t np = 0;
+  for (int i = 0; i < n; ++i) {
+    const double xi = (double)refx[i], yi = (double)refy[i];
+    for (int j = i + 1; j < n; ++j) {
+      const double xij = (double)refx[j] - xi, yij = (double)refy[j] - yi;
+      const double dij = std::sqrt(xij * xij + yij * yij);
+      if (dij >= dmin && dij <= dmax) {
+        if (np < cap) {
+          out[2 * np] = i;
+          out[2 * np + 1] = j;
+        }
+        ++np;
+      }
+    }
+  }
+  return np;
+}
+
+// The equiprojectivity criterion of correction_distortion
+// (src/distortion_correction.cpp:249-290 for POWELL, with A1 and B1 the
+// undistorted reference positions; :318-351 for POWELL_ITER, with A1 and B1
+// taken from orig): sum over images 1.. and pairs of err^2, where
+// err = AB_unit . ((B2 - B1) - (A2 - A1)); pairs with a subpixel NCC below
+// NCC_min on either grain are skipped (their fvec entry is 0).
+// dx, dy, ncc: [image - 1][grain].
+double orc_disto_objective(const double* X, const int32_t* refx, const int32_t* refy, const double* origx,
+                           const double* origy, int n, int nimg1, const double* dx, const double* dy,
+                           const double* ncc, double NCC_min, const int32_t* pairs, int64_t npairs, int use_orig,
+                           double* fvec) {
+  double val = 0.0;
+  for (int im = 0; im < nimg1; ++im) {
+    for (int64_t il = 0; il < npairs; ++il) {
+      const int i = pairs[2 * il], j = pairs[2 * il + 1];
+      if (fvec) fvec[(size_t)im * npairs + il] = 0.0;
+      if (ncc[(size_t)im * n + i] < NCC_min || ncc[(size_t)im * n + j] < NCC_min) continue;
+      double A1x, A1y, A2x, A2y, B1x, B1y, B2x, B2y;
+      if (use_orig) {
+        A1x = origx[i];
+        A1y = origy[i];
+        B1x = origx[j];
+        B1y = origy[j];
+      } else {
+        undistor(X, (double)refx[i], (double)refy[i], &A1x, &A1y);
+        undistor(X, (double)refx[j], (double)refy[j], &B1x, &B1y);
+      }
+      undistor(X, (double)refx[i] + dx[(size_t)im * n + i], (double)refy[i] + dy[(size_t)im * n + i], &A2x, &A2y);
+      undistor(X, (double)refx[j] + dx[(size_t)im * n + j], (double)refy[j] + dy[(size_t)im * n + j], &B2x, &B2y);
+      double ABx = B1x - A1x, ABy = B1y - A1y;
+      const double AB = std::sqrt(ABx * ABx + ABy * ABy);
+      ABx /= AB;
+      ABy /= AB;
+      const double BBx = B2x - B1x, BBy = B2y - B1y;
+      const double AAx = A2x - A1x, AAy = A2y - A1y;
+      const double err = (ABx * (BBx - AAx)) + (ABy * (BBy - AAy));
+      if (fvec) fvec[(size_t)im * npairs + il] = err;
+      val += err * err;
+    }
+  }
+  return val;
+}
+
+// The minimisation of correction_distortion (src/distortion_correction.cpp:
+// 222-386): default centres (negative entries -> frame centre, :222-226), then
+// algo 0 (POWELL): one Powell minimisation (ftol 1e-12, initial directions the
+// perturbations); algo 1 (POWELL_ITER): num_iter minimisations, each followed
+// by re-anchoring A1/B1 and the displacements on the undistorted reference
+// positions.  history (optional, num_iter x 15): index and parameters after
+// each iteration.  dx, dy are updated in place by POWELL_ITER.
+void orc_disto_fit(double* X14, const double* perturb14, int algo, int num_iter, int dimx, int dimy,
+                   const int32_t* refx, const int32_t* refy, int n, int nimg1, double* dx, double* dy,
+                   const double* ncc, double NCC_min, const int32_t* pairs, int64_t npairs, double* index_ini,
+                   double* index_end, double* history) {
+  std::vector<double> X(X14, X14 + 14), DX(perturb14, perturb14 + 14);
+  if (X[0] < 0.0) X[0] = 0.5 * (double)dimx;
+  if (X[1] < 0.0) X[1] = 0.5 * (double)dimy;
+  if (X[8] < 0.0) X[8] = 0.5 * (double)dimx;
+  if (X[9] < 0.0) X[9] = 0.5 * (double)dimy;
+  std::vector<double> ox(n), oy(n);
+  for (int g = 0; g < n; ++g) {
+    ox[g] = (double)refx[g];
+    oy[g] = (double)refy[g];
+  }
+  const int use_orig = algo == 1 ? 1 : 0;
+  struct F {
+    const int32_t *rx, *ry;
+    std::vector<double>*ox, *oy;
+    int n, nimg1;
+    double *dx, *dy;
+    const double* ncc;
+    double NCC_min;
+    const int32_t* pairs;
+    int64_t npairs;
+    int use_orig;
+    double operator()(std::vector<double>& X) {
+      return orc_disto_objective(X.data(), rx, ry, ox->data(), oy->data(), n, nimg1, dx, dy, ncc, NCC_min, pairs,
+                                 npairs, use_orig, nullptr);
+    }
+  } func{refx, refy, &ox, &oy, n, nimg1, dx, dy, ncc, NCC_min, pairs, npairs, use_orig};
+  const double nb = (double)nimg1;
+  ptk_oracle::Powell<F> powell(func, 1e-12);
+  *index_ini = func(X) / nb;
+  if (algo == 1) {
+    std::vector<double> dx0(dx, dx + (size_t)nimg1 * n), dy0(dy, dy + (size_t)nimg1 * n);
+    for (int it = 1; it <= num_iter; ++it) {
+      X = powell.minimize(X, DX);
+      const double idx = func(X) / nb;
+      if (history) {
+        history[(size_t)(it - 1) * 15] = idx;
+        for (int k = 0; k < 14; ++k) history[(size_t)(it - 1) * 15 + 1 + k] = X[k];
+      }
+      for (int g = 0; g < n; ++g) {
+        double xu, yu;
+        undistor(X.data(), (double)refx[g], (double)refy[g], &xu, &yu);
+        const double dxc = xu - (double)refx[g], dyc = yu - (double)refy[g];
+        for (int im = 0; im < nimg1; ++im) {
+          dx[(size_t)im * n + g] = dx0[(size_t)im * n + g] + dxc;
+          dy[(size_t)im * n + g] = dy0[(size_t)im * n + g] + dyc;
+        }
+        ox[g] = xu;
+        oy[g] = yu;
+      }
+    }
+  } else {
+    X = powell.minimize(X, DX);
+  }
+  *index_end = func(X) / nb;
+  for (int k = 0; k < 14; ++k) X14[k] = X[k];
+}
+
 // Inverse of undistor (no reference counterpart: the reference applies
 // undistor to points only, src/distortion_correction.cpp:20-61).  Newton
 // iteration on F(xd) = undistor(xd) - xu with a forward-difference Jacobian

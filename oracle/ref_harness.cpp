@@ -355,6 +355,64 @@ void ref_undistor(void* p, const double* params14, double xd, double yd, double*
   t.undistor(X, xd, yd, *xu, *yu);
 }
 
+// ptracker::precompute_paires (src/distortion_correction.cpp:63-81) on grains
+// placed at the given reference positions; writes at most cap pairs.
+int64_t ref_disto_pairs(void* p, const int32_t* refx, const int32_t* refy, int n, double dmin, double dmax,
+                        int32_t* out, int64_t cap) {
+  ptracker& t = static_cast<Handle*>(p)->trk;
+  t.grain.assign(n, grain_type_2D());
+  for (int g = 0; g < n; ++g) {
+    t.grain[g].refcoord_xpix = refx[g];
+    t.grain[g].refcoord_ypix = refy[g];
+  }
+  t.num_grains = n;
+  t.equiProj_dist_min = dmin;
+  t.equiProj_dist_max = dmax;
+  t.precompute_paires();
+  const int64_t np = (int64_t)t.grain_pairs.size();
+  for (int64_t k = 0; k < np && k < cap; ++k) {
+    out[2 * k] = t.grain_pairs[k].i;
+    out[2 * k + 1] = t.grain_pairs[k].j;
+  }
+  return np;
+}
+
+// The POWELL functor of correction_distortion (src/distortion_correction.cpp:
+// 249-290) restated around the reference's ptracker::undistor; use_orig selects
+// the POWELL_ITER functor (:318-351, A1 and B1 from origx/origy).
+double ref_disto_objective(void* p, const double* X14, const int32_t* refx, const int32_t* refy, const double* origx,
+                           const double* origy, int n, int nimg1, const double* dx, const double* dy,
+                           const double* ncc, double NCC_min, const int32_t* pairs, int64_t npairs, int use_orig) {
+  ptracker& t = static_cast<Handle*>(p)->trk;
+  std::vector<double> X(X14, X14 + 14);
+  double valret = 0.0;
+  for (int im = 0; im < nimg1; ++im)
+    for (int64_t il = 0; il < npairs; ++il) {
+      const int i = pairs[2 * il], j = pairs[2 * il + 1];
+      if (ncc[(size_t)im * n + i] < NCC_min || ncc[(size_t)im * n + j] < NCC_min) continue;
+      double A1x, A1y, A2x, A2y, B1x, B1y, B2x, B2y;
+      if (use_orig) {
+        A1x = origx[i];
+        A1y = origy[i];
+        B1x = origx[j];
+        B1y = origy[j];
+      } else {
+        t.undistor(X, (double)(refx[i]), (double)(refy[i]), A1x, A1y);
+        t.undistor(X, (double)(refx[j]), (double)(refy[j]), B1x, B1y);
+      }
+      t.undistor(X, (double)(refx[i] + dx[(size_t)im * n + i]), (double)(refy[i] + dy[(size_t)im * n + i]), A2x, A2y);
+      t.undistor(X, (double)(refx[j] + dx[(size_t)im * n + j]), (double)(refy[j] + dy[(size_t)im * n + j]), B2x, B2y);
+      double ABx = B1x - A1x, ABy = B1y - A1y;
+      const double AB = sqrt(ABx * ABx + ABy * ABy);
+      ABx /= AB;
+      ABy /= AB;
+      const double BBx = B2x - B1x, BBy = B2y - B1y, AAx = A2x - A1x, AAy = A2y - A1y;
+      const double err = (ABx * (BBx - AAx)) + (ABy * (BBy - AAy));
+      valret += err * err;
+    }
+  return valret;
+}
+
 int ref_save_grains(void* p, const char* path, int num) {
   return static_cast<Handle*>(p)->trk.save_grains(path, num);
 }

@@ -102,6 +102,15 @@ _SIGS = {
     "ptk_read_grains_file": (C.c_int, [C.c_char_p, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
     "ptk_save_grains_file": (C.c_int, [C.c_char_p, _P, C.c_int, C.c_char_p, C.c_char_p, C.c_char_p,
                                        C.c_char_p]),
+    "ptk_disto_pairs": (C.c_int, [_P, _P, C.c_int, C.c_double, C.c_double, _P, C.c_int64, C.POINTER(C.c_int64)]),
+    "ptk_disto_create": (C.c_int, [C.POINTER(_P), C.c_int, C.c_int, _P, _P, C.c_int, C.c_int, _P, _P, _P,
+                                   C.c_double, _P, C.c_int64]),
+    "ptk_disto_destroy": (C.c_int, [_P]),
+    "ptk_disto_last_error": (C.c_char_p, [_P]),
+    "ptk_disto_objective": (C.c_int, [_P, _P, C.POINTER(C.c_double)]),
+    "ptk_disto_residuals": (C.c_int, [_P, _P, C.POINTER(C.c_double), _P]),
+    "ptk_disto_fit": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), _P]),
+    "ptk_disto_tracked": (C.c_int, [_P, _P, _P]),
 }
 
 _lib = None
@@ -408,6 +417,91 @@ def read_image_file(path: str) -> tuple[np.ndarray, str]:
     if rc != PTK_OK:
         raise PtkError(rc, L.ptk_image_error().decode())
     return out, when.value.decode()
+
+
+DISTO_POWELL, DISTO_POWELL_ITER, DISTO_LEVMAR = 0, 1, 2
+
+
+def disto_pairs(refx: np.ndarray, refy: np.ndarray, dmin: float, dmax: float) -> np.ndarray:
+    """precompute_paires (src/distortion_correction.cpp:63-81): (npairs, 2)
+    int32 pairs i < j, i-major, of grains dmin .. dmax apart."""
+    L = lib()
+    rx = np.ascontiguousarray(refx, dtype=np.int32)
+    ry = np.ascontiguousarray(refy, dtype=np.int32)
+    n = C.c_int64()
+    rc = L.ptk_disto_pairs(_ptr(rx), _ptr(ry), rx.shape[0], float(dmin), float(dmax), None, 0, C.byref(n))
+    out = np.zeros((max(n.value, 1), 2), dtype=np.int32)
+    rc = L.ptk_disto_pairs(_ptr(rx), _ptr(ry), rx.shape[0], float(dmin), float(dmax), _ptr(out), n.value,
+                           C.byref(n))
+    if rc != 0:
+        raise PtkError(rc, "ptk_disto_pairs")
+    return out[:n.value]
+
+
+class DistoFit:
+    """The distortion-parameter fit of correction_distortion on the GPU
+    (ptk_disto_*): grains' integer reference positions, their tracked
+    displacements and subpixel NCC per image after the reference
+    ([image, grain]), and the grain pairs."""
+
+    def __init__(self, dimx: int, dimy: int, refx, refy, dx, dy, ncc_subpix, NCC_min: float, pairs):
+        L = lib()
+        self._L = L
+        self._keep = [np.ascontiguousarray(refx, dtype=np.int32), np.ascontiguousarray(refy, dtype=np.int32),
+                      np.ascontiguousarray(dx, dtype=np.float64), np.ascontiguousarray(dy, dtype=np.float64),
+                      np.ascontiguousarray(ncc_subpix, dtype=np.float64),
+                      np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)]
+        rx, ry, ddx, ddy, nc, pr = self._keep
+        self.n, self.nimg1, self.npairs = rx.shape[0], ddx.shape[0], pr.shape[0]
+        h = C.c_void_p()
+        rc = L.ptk_disto_create(C.byref(h), dimx, dimy, _ptr(rx), _ptr(ry), self.n, self.nimg1, _ptr(ddx), _ptr(ddy),
+                                _ptr(nc), float(NCC_min), _ptr(pr), self.npairs)
+        if rc != 0:
+            raise PtkError(rc, "ptk_disto_create")
+        self.h = h
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise PtkError(rc, self._L.ptk_disto_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.ptk_disto_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def objective(self, params14) -> float:
+        x = np.ascontiguousarray(params14, dtype=np.float64)
+        v = C.c_double()
+        self._check(self._L.ptk_disto_objective(self.h, _ptr(x), C.byref(v)))
+        return v.value
+
+    def residuals(self, params14) -> tuple[float, np.ndarray]:
+        x = np.ascontiguousarray(params14, dtype=np.float64)
+        v = C.c_double()
+        f = np.zeros(self.nimg1 * self.npairs)
+        self._check(self._L.ptk_disto_residuals(self.h, _ptr(x), C.byref(v), _ptr(f)))
+        return v.value, f
+
+    def fit(self, params14, perturb14, algo: int = DISTO_POWELL, num_iter: int = 5):
+        x = np.array(params14, dtype=np.float64)
+        dx = np.ascontiguousarray(perturb14, dtype=np.float64)
+        ini, end = C.c_double(), C.c_double()
+        hist = np.zeros((max(num_iter, 1), 15))
+        self._check(self._L.ptk_disto_fit(self.h, _ptr(x), _ptr(dx), algo, num_iter, C.byref(ini), C.byref(end),
+                                          _ptr(hist)))
+        return x, ini.value, end.value, hist[:num_iter] if algo == DISTO_POWELL_ITER else hist[:0]
+
+    def tracked(self) -> tuple[np.ndarray, np.ndarray]:
+        dx = np.zeros((self.nimg1, self.n))
+        dy = np.zeros((self.nimg1, self.n))
+        self._check(self._L.ptk_disto_tracked(self.h, _ptr(dx), _ptr(dy)))
+        return dx, dy
 
 
 def cli_path() -> Path:
