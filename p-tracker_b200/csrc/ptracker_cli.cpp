@@ -1,15 +1,15 @@
-// ptracker_b200: the particle_tracking procedure of `ptracker <command_file>`
-// (src/p-tracker.cpp:422-612, run.cpp) driven through the C ABI of this
-// library, for one GPU.
+// ptracker_b200: the particle_tracking and correction_distortion procedures
+// of `ptracker <command_file>` (src/p-tracker.cpp:422-612,
+// src/distortion_correction.cpp:135-607, run.cpp) driven through the C ABI of
+// this library, for one GPU.
 //
 // Command file: the reference's token stream (read_data,
 // src/p-tracker.cpp:1487-1784): whitespace-separated tokens, '#' or '!' starts
 // a comment to the end of the line, unknown tokens are reported and skipped.
 // Grain files, `pattern`, `targetRadiusPattern` and `mask_rect` act on the
 // grains loaded so far, in file order, as they do in the reference.  Tokens of
-// procedures other than particle tracking (distortion fitting, RAW decoding,
-// neighbour lists, thread counts) are accepted and have no effect.  Added
-// tokens select the forms of this library:
+// other features (RAW decoding, neighbour lists, thread counts) are accepted
+// and have no effect.  Added tokens select the forms of this library:
 //     search_method  exact | bf16          integer search (default exact)
 //     subpix_method  powell | adjoint_lm   subpixel refinement (default powell)
 //     topk K, lm_max_iter N, lm_tol T      their parameters
@@ -24,6 +24,14 @@
 // grains go to dic_out_<num>.txt in the working directory, byte for byte as
 // save_grains (src/p-tracker.cpp:1313-1367).
 //
+// `procedure correction_distortion` tracks image_numbers_corrDisto[1..]
+// against image_numbers_corrDisto[0] (pixel search from the imposed
+// approximate displacements, no rescue, then subpixel; dic_out_<num>.txt per
+// image), then fits the 14 undistor parameters with ptk_disto_fit (POWELL or
+// POWELL_ITER; LEVMAR needs toofus's lmdif1 and is refused) and writes
+// corrDisto_log.txt, errors.txt, distobox.txt and, for POWELL_ITER,
+// convergence.txt as the reference does.
+//
 //   ptracker_b200 [command_file]     (default: commands.txt)
 //   ptracker_b200 --check file       parse only; print the settings as JSON
 #include <chrono>
@@ -33,6 +41,8 @@
 #include <cstring>
 #include <fstream>
 #include <future>
+#include <iomanip>
+#include <iostream>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -53,7 +63,15 @@ struct Settings {
   int raw_images = 0, undistort = 0;
   ptk_config cfg;
   double target_radius = -1.0;
-  double disto[14] = {};
+  // undistor parameters (defaults of ptracker::ptracker, src/p-tracker.cpp:
+  // 22-52: negative centres stand for the frame centre) and the fit's
+  // perturbations
+  double disto[14] = {-1.0, -1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, -1.0, -1.0, 0.0, 0.0, 0.0, 0.0};
+  double disto_perturb[14] = {1e-6, 1e-6, 1e-6, 1e-6, 1e-6, 1e-6, 1e-6, 1e-6, 1e-6, 1e-6, 1e-6, 1e-6, 1e-6, 1e-6};
+  std::vector<int> corr_images;
+  std::vector<double> imposed_x, imposed_y;
+  double equiproj_min = 0.0, equiproj_max = 1000.0;
+  int optim_algo = PTK_DISTO_POWELL, powell_num_iter = 5;
   std::vector<ptk_grain> grains;
   std::vector<PatternOp> patterns;  // acting on the grains loaded last
   std::vector<std::string> warnings;
@@ -124,10 +142,18 @@ Settings read_commands(const char* path) {
     } else if (tok == "RawImages") {
       in >> s.raw_images;
     } else if (tok == "DemosaicModel" || tok == "rescaleGrayLevels" || tok == "idelta" ||
-               tok == "wanted_num_threads" || tok == "verbose_level" || tok == "powell_num_iter" ||
-               tok == "num_neighbour_max" || tok == "neighbour_dist_pix" || tok == "period_rebuild_neighbour_list" ||
-               tok == "use_neighbour_list" || tok == "optim_algo") {
+               tok == "wanted_num_threads" || tok == "verbose_level" || tok == "num_neighbour_max" ||
+               tok == "neighbour_dist_pix" || tok == "period_rebuild_neighbour_list" || tok == "use_neighbour_list") {
       skip(1);
+    } else if (tok == "powell_num_iter") {
+      in >> s.powell_num_iter;
+    } else if (tok == "optim_algo") {  // src/p-tracker.cpp:1553-1564
+      std::string k;
+      in >> k;
+      if (k == "POWELL") s.optim_algo = PTK_DISTO_POWELL;
+      else if (k == "POWELL_ITER") s.optim_algo = PTK_DISTO_POWELL_ITER;
+      else if (k == "LEVMAR") s.optim_algo = PTK_DISTO_LEVMAR;
+      else std::printf("WARNING, keyword %s is unknown for optim_algo\n", k.c_str());
     } else if (tok == "grains_to_follow" || tok == "start_file") {
       std::string f;
       in >> f;
@@ -233,26 +259,36 @@ Settings read_commands(const char* path) {
       for (ptk_grain& g : s.grains)
         if (g.refcoord_xpix >= x0 && g.refcoord_xpix <= x1 && g.refcoord_ypix >= y0 && g.refcoord_ypix <= y1)
           g.masked = 1;
-    } else if (tok == "image_numbers_corrDisto") {
-      size_t nb;
+    } else if (tok == "image_numbers_corrDisto") {  // src/p-tracker.cpp:1696-1702
+      size_t nb = 0;
       in >> nb;
-      skip((int)nb);
-    } else if (tok == "imposedDisplApprox_corrDisto") {
-      s.warnings.push_back("imposedDisplApprox_corrDisto belongs to the distortion fit: ignored");
+      s.corr_images.assign(nb, 0);
+      for (size_t i = 0; i < nb; ++i) in >> s.corr_images[i];
+    } else if (tok == "imposedDisplApprox_corrDisto") {  // :1703-1710, one pair per image after the first
+      s.imposed_x.assign(s.corr_images.size(), 0.0);
+      s.imposed_y.assign(s.corr_images.size(), 0.0);
+      for (size_t i = 1; i < s.corr_images.size(); ++i) in >> s.imposed_x[i] >> s.imposed_y[i];
     } else if (tok == "equiProj_dist_range") {
-      skip(2);
+      in >> s.equiproj_min >> s.equiproj_max;
     } else if (tok.size() > 11 && (tok.find("_corrDistor") != std::string::npos ||
                                    tok.find("_corrParallax") != std::string::npos)) {
       static const char* names[14] = {"xc_corrDistor", "yc_corrDistor", "K1_corrDistor", "K2_corrDistor",
                                       "K3_corrDistor", "P1_corrDistor", "P2_corrDistor", "P3_corrDistor",
                                       "xc_corrParallax", "yc_corrParallax", "angle1_corrParallax",
                                       "A1_corrParallax", "angle2_corrParallax", "A2_corrParallax"};
-      int k = -1;
-      for (int i = 0; i < 14; ++i)
+      int k = -1, kd = -1;
+      for (int i = 0; i < 14; ++i) {
         if (tok == names[i]) k = i;
+        if (tok == std::string("d") + names[i]) kd = i;
+      }
       double v;
       in >> v;
-      if (k >= 0) s.disto[k] = v;  // the d*_ perturbations belong to the fit
+      if (k >= 0) s.disto[k] = v;
+      else if (kd >= 0) s.disto_perturb[kd] = v;
+      else {
+        std::printf("Unknown token: %s\n", tok.c_str());
+        ++s.unknown_tokens;
+      }
     } else if (tok == "search_method") {
       std::string k;
       in >> k;
@@ -331,12 +367,108 @@ void print_json(const Settings& s) {
   o << "], \"search_method\": " << c.search_method << ", \"subpix_method\": " << c.subpix_method
     << ", \"undistort_images\": " << s.undistort << ", \"disto\": [";
   for (int k = 0; k < 14; ++k) o << (k ? ", " : "") << s.disto[k];
-  o << "], \"unknown_tokens\": " << s.unknown_tokens << ", \"warnings\": " << s.warnings.size() << "}";
+  o << "], \"disto_perturb\": [";
+  for (int k = 0; k < 14; ++k) o << (k ? ", " : "") << s.disto_perturb[k];
+  o << "], \"corr_images\": [";
+  for (size_t i = 0; i < s.corr_images.size(); ++i) o << (i ? ", " : "") << s.corr_images[i];
+  o << "], \"imposed\": [";
+  for (size_t i = 0; i < s.imposed_x.size(); ++i)
+    o << (i ? ", " : "") << "[" << s.imposed_x[i] << ", " << s.imposed_y[i] << "]";
+  o << "], \"equiproj_range\": [" << s.equiproj_min << ", " << s.equiproj_max << "], \"optim_algo\": "
+    << s.optim_algo << ", \"powell_num_iter\": " << s.powell_num_iter;
+  o << ", \"unknown_tokens\": " << s.unknown_tokens << ", \"warnings\": " << s.warnings.size() << "}";
   std::printf("%s\n", o.str().c_str());
 }
 
 double now() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// undistor (src/distortion_correction.cpp:20-61) on the host, for the
+// procedure's output files.
+void undistor_host(const double* X, double xd, double yd, double* xo, double* yo) {
+  const double dx = xd - X[0], dy = yd - X[1];
+  const double r2 = dx * dx + dy * dy, r4 = r2 * r2, r6 = r4 * r2;
+  const double xu = xd + dx * (X[2] * r2 + X[3] * r4 + X[4] * r6) +
+                    (X[5] * (r2 + 2.0 * dx * dx) + 2.0 * X[6] * dx * dy) * (1.0 + X[7] * r2);
+  const double yu = yd + dy * (X[2] * r2 + X[3] * r4 + X[4] * r6) +
+                    (2.0 * X[5] * dx * dy + X[6] * (r2 + 2.0 * dy * dy)) * (1.0 + X[7] * r2);
+  const double nx1 = std::cos(X[10]), ny1 = -std::sin(X[10]), nx2 = -std::sin(X[12]), ny2 = std::cos(X[12]);
+  const double dX = xu - X[8], dY = yu - X[9];
+  const double S1 = (1.0 + X[11]) * (dX * nx1 + dY * ny1);
+  const double S2 = (1.0 + X[13]) * (dX * nx2 + dY * ny2);
+  *xo = X[8] + S1 * nx1 + S2 * nx2;
+  *yo = X[9] + S1 * ny1 + S2 * ny2;
+}
+
+// Negative centres stand for the frame centre (src/distortion_correction.cpp:222-226).
+void default_centres(double* X, int dimx, int dimy) {
+  if (X[0] < 0.0) X[0] = 0.5 * (double)dimx;
+  if (X[1] < 0.0) X[1] = 0.5 * (double)dimy;
+  if (X[8] < 0.0) X[8] = 0.5 * (double)dimx;
+  if (X[9] < 0.0) X[9] = 0.5 * (double)dimy;
+}
+
+// The output files and console lines after the minimisation
+// (src/distortion_correction.cpp:480-607).
+void write_disto_outputs(const double* X, double index_ini, double index_end, int dimx, int dimy) {
+  static const char* labels[14] = {"xc_corrDistor ",       "yc_corrDistor ",       "K1_corrDistor ",
+                                   "K2_corrDistor ",       "K3_corrDistor ",       "P1_corrDistor ",
+                                   "P2_corrDistor ",       "P3_corrDistor ",       "xc_corrParallax     ",
+                                   "yc_corrParallax     ", "angle1_corrParallax ", "A1_corrParallax     ",
+                                   "angle2_corrParallax ", "A2_corrParallax     "};
+  const double gain = index_ini / index_end;
+  std::ofstream log("corrDisto_log.txt");
+  log << std::scientific << std::setprecision(15);
+  log << "Initial distorsion index " << index_ini << '\n';
+  log << "Final distorsion index " << index_end << '\n';
+  log << "Index gain (>1 is good) " << gain << '\n';
+  for (int k = 0; k < 14; ++k) log << labels[k] << X[k] << (k == 13 ? "" : "\n");
+  log << std::endl;
+  std::cout << std::scientific << std::setprecision(15);
+  std::cout << "    Initial distorsion index " << index_ini << '\n';
+  std::cout << "      Final distorsion index " << index_end << '\n';
+  std::cout << "gain (index_ini / index_end) " << gain << " (>1 is good)" << '\n';
+  for (int k = 0; k < 14; ++k) std::cout << labels[k] << X[k] << (k == 13 ? "" : "\n");
+  std::cout << std::endl;
+
+  std::ofstream ef("errors.txt");
+  double xerrmax = -1e20, yerrmax = -1e20, errmax = -1e20, xd, yd, xu, yu;
+  double dxd = (double)dimx / 50.0, dyd = (double)dimy / 50.0;
+  if (dxd < 1.0) dxd = 1.0;
+  if (dyd < 1.0) dyd = 1.0;
+  for (xd = 0.0; xd < dimx; xd += dxd) {
+    for (yd = 0.0; yd < dimy; yd += dyd) {
+      undistor_host(X, xd, yd, &xu, &yu);
+      const double xerr = xu - xd, yerr = yu - yd, err = std::sqrt(xerr * xerr + yerr * yerr);
+      if (std::fabs(xerr) > xerrmax) xerrmax = std::fabs(xerr);
+      if (std::fabs(yerr) > yerrmax) yerrmax = std::fabs(yerr);
+      if (err > errmax) errmax = err;
+      ef << xd << ' ' << yd << ' ' << xerr << ' ' << yerr << std::endl;
+    }
+    ef << std::endl;
+  }
+  log << "max |xu - xd| " << xerrmax << '\n';
+  log << "max |yu - yd| " << yerrmax << '\n';
+  log << "errormax " << errmax << std::endl;
+  std::cout << "max |xu - xd| " << xerrmax << '\n';
+  std::cout << "max |yu - yd| " << yerrmax << '\n';
+  std::cout << "errormax      " << errmax << std::endl;
+
+  std::ofstream bf("distobox.txt");
+  auto box = [&](double x, double y) {
+    undistor_host(X, x, y, &xu, &yu);
+    bf << x << " " << y << " " << xu - x << " " << yu - y << std::endl;
+  };
+  yd = 0;
+  for (xd = 0; xd < dimx; xd += dxd) box(xd, yd);
+  xd = dimx - 1;
+  for (yd = 0; yd < dimy; yd += dyd) box(xd, yd);
+  yd = dimy - 1;
+  for (xd = dimx - 1; xd >= 0; xd -= dxd) box(xd, yd);
+  xd = 0;
+  for (yd = dimy - 1; yd >= 0; yd -= dyd) box(xd, yd);
+  box(0.0, 0.0);
 }
 
 }  // namespace
@@ -360,12 +492,26 @@ int main(int argc, char** argv) {
     print_json(s);
     return 0;
   }
-  if (s.procedure != "particle_tracking") die("procedure " + s.procedure + " is not part of this build");
+  const bool corr = s.procedure == "correction_distortion";
+  if (!corr && s.procedure != "particle_tracking") die("procedure " + s.procedure + " is not part of this build");
   if (s.raw_images) die("RAW images (libraw) are not supported: convert the frames to TIFF or PGM");
   if (s.grains.empty()) die("no grains (grains_to_follow / start_file / restart_file)");
-  if (s.iinc <= 0 && s.ibeg <= s.iend) die("iinc must be > 0 (the reference loops forever otherwise)");
+  if (corr) {
+    if (s.corr_images.size() < 2) die("image_numbers_corrDisto needs the reference image and at least one more");
+    if (s.optim_algo == PTK_DISTO_LEVMAR)
+      die("optim_algo LEVMAR calls lmdif1 from the toofus library, which is not part of this build: use POWELL or "
+          "POWELL_ITER");
+    if (s.imposed_x.size() != s.corr_images.size()) {
+      s.imposed_x.assign(s.corr_images.size(), 0.0);
+      s.imposed_y.assign(s.corr_images.size(), 0.0);
+    }
+    s.iref = s.corr_images[0];
+  } else if (s.iinc <= 0 && s.ibeg <= s.iend) {
+    die("iinc must be > 0 (the reference loops forever otherwise)");
+  }
 
-  std::printf("*** PROCEDURE PARTICLE IMAGE TRACKING (B200) ***\n");
+  std::printf(corr ? "\n*** PROCEDURE CORRECTION OF DISTORTION (B200) ***\n\n"
+                   : "*** PROCEDURE PARTICLE IMAGE TRACKING (B200) ***\n");
   Frame ref = read_frame(s.image_name, s.iref);
   if (ref.rc) die(ref.error);
   s.cfg.dimx = ref.dimx;
@@ -387,9 +533,15 @@ int main(int argc, char** argv) {
       ck(ptk_make_patterns(ctx, op.kind, op.a, op.b, op.target), "ptk_make_patterns");
     }
   }
-  bool disto = false;
-  for (double v : s.disto) disto = disto || v != 0.0;
-  if (s.undistort && disto) ck(ptk_set_distortion(ctx, s.disto), "ptk_set_distortion");
+  bool disto = false;  // a non-identity undistor
+  for (int k : {2, 3, 4, 5, 6, 7, 10, 11, 12, 13}) disto = disto || s.disto[k] != 0.0;
+  if (corr) disto = false;  // the fit works on the frames as recorded
+  if (s.undistort && disto) {
+    double X[14];
+    std::memcpy(X, s.disto, sizeof(X));
+    default_centres(X, ref.dimx, ref.dimy);
+    ck(ptk_set_distortion(ctx, X), "ptk_set_distortion");
+  }
   auto load = [&](int slot, const Frame& f) {
     if (f.dimx != s.cfg.dimx || f.dimy != s.cfg.dimy) die(f.name + ": frame size differs from the reference frame");
     ck(ptk_load_frame(ctx, slot, f.pix.data(), f.dimx, f.dimy, 2, (size_t)f.dimx * 2), "ptk_load_frame");
@@ -400,6 +552,89 @@ int main(int argc, char** argv) {
   ck(ptk_set_iref(ctx, s.iref), "ptk_set_iref");
   int iref = s.iref;
   std::string ref_name = ref.name, ref_time = ref.datetime;
+
+  if (corr) {
+    // ---- correction_distortion: tracking from the reference image into
+    // each other image (src/distortion_correction.cpp:157-220)
+    std::vector<int32_t> refx((size_t)n), refy((size_t)n);
+    for (int g = 0; g < n; ++g) {
+      refx[g] = s.grains[g].refcoord_xpix;
+      refy[g] = s.grains[g].refcoord_ypix;
+    }
+    int64_t np = 0;
+    ptk_disto_pairs(refx.data(), refy.data(), n, s.equiproj_min, s.equiproj_max, nullptr, 0, &np);
+    std::vector<int32_t> pairs((size_t)(2 * np + 2));
+    if (ptk_disto_pairs(refx.data(), refy.data(), n, s.equiproj_min, s.equiproj_max, pairs.data(), np, &np))
+      die("ptk_disto_pairs");
+    std::printf("Number of points for equiprojectivity computations: %lld\n", (long long)np);
+    std::printf("Tracking displacements... \n");
+    const int nimg1 = (int)s.corr_images.size() - 1;
+    std::vector<double> dx((size_t)nimg1 * n), dy((size_t)nimg1 * n), ncc((size_t)nimg1 * n);
+    std::vector<ptk_grain> cur_g((size_t)n);
+    for (int im = 1; im <= nimg1; ++im) {
+      const int num = s.corr_images[im];
+      Frame cur = read_frame(s.image_name, num);
+      if (cur.rc) die(cur.error);
+      load(1, cur);
+      // the estimated displacement starts every grain's search (:173-178)
+      ck(ptk_get_grains(ctx, cur_g.data(), n), "ptk_get_grains");
+      for (ptk_grain& g : cur_g) {
+        g.dx = s.imposed_x[im];
+        g.dy = s.imposed_y[im];
+      }
+      ck(ptk_set_grains(ctx, cur_g.data(), n), "ptk_set_grains");
+      std::printf("> Follow %d grains... (from image number %d to number %d)\n", n, iref, num);
+      const double t0 = now();
+      ck(ptk_search(ctx, 0), "ptk_search");  // no rescue is attempted
+      ck(ptk_subpixel(ctx, s.cfg.subpix_method), "ptk_subpixel");
+      ck(ptk_get_grains(ctx, cur_g.data(), n), "ptk_get_grains");
+      int failed = 0;
+      for (int g = 0; g < n; ++g) {
+        dx[(size_t)(im - 1) * n + g] = cur_g[g].dx;
+        dy[(size_t)(im - 1) * n + g] = cur_g[g].dy;
+        ncc[(size_t)(im - 1) * n + g] = cur_g[g].NCC_subpix;
+        if (cur_g[g].NCC_subpix < s.cfg.NCC_min) ++failed;
+      }
+      std::printf("< [DONE in %f seconds]\nFailure rate = %g%%\n", now() - t0, 100.0 * (double)failed / (double)n);
+      char fname[64];
+      std::snprintf(fname, sizeof(fname), "dic_out_%d.txt", num);
+      if (ptk_save_grains_file(fname, cur_g.data(), n, ref_name.c_str(), ref_time.c_str(), cur.name.c_str(),
+                               cur.datetime.c_str()))
+        die(std::string("cannot write ") + fname);
+    }
+    std::printf("Tracking of points done\n");
+    ptk_destroy(ctx);
+
+    // ---- minimisation (:222-478)
+    double X[14];
+    std::memcpy(X, s.disto, sizeof(X));
+    std::printf("Numbers of position pairs used to undistor: %lld\nNumbers of image pairs: %d\n", (long long)np,
+                nimg1);
+    ptk_disto* dfit = nullptr;
+    if (ptk_disto_create(&dfit, s.cfg.dimx, s.cfg.dimy, refx.data(), refy.data(), n, nimg1, dx.data(), dy.data(),
+                         ncc.data(), s.cfg.NCC_min, pairs.data(), np))
+      die("ptk_disto_create failed");
+    const int iters = s.optim_algo == PTK_DISTO_POWELL_ITER ? s.powell_num_iter : 0;
+    std::vector<double> hist((size_t)(iters > 0 ? iters : 1) * 15);
+    double ini = 0.0, end = 0.0;
+    std::printf("START minimizing equiprojectivity criterion (with %s)\n",
+                s.optim_algo == PTK_DISTO_POWELL ? "POWELL" : "POWELL_ITER");
+    if (ptk_disto_fit(dfit, X, s.disto_perturb, s.optim_algo, iters, &ini, &end, hist.data()))
+      die(std::string("ptk_disto_fit: ") + ptk_disto_last_error(dfit));
+    std::printf("END minimizing equiprojectivity criterion\n\n");
+    ptk_disto_destroy(dfit);
+    if (s.optim_algo == PTK_DISTO_POWELL_ITER) {
+      std::ofstream cf("convergence.txt");
+      cf << std::scientific << std::setprecision(15);
+      for (int it = 0; it < iters; ++it) {
+        cf << it + 1;
+        for (int k = 0; k < 15; ++k) cf << ' ' << hist[(size_t)it * 15 + k];
+        cf << ' ' << std::endl;
+      }
+    }
+    write_disto_outputs(X, ini, end, s.cfg.dimx, s.cfg.dimy);
+    return 0;
+  }
 
   std::future<Frame> next;
   if (s.ibeg <= s.iend) next = std::async(std::launch::async, read_frame, s.image_name, s.ibeg);

@@ -152,3 +152,39 @@ def test_missing_command_file_fails(ptk, tmp_path):
     r = subprocess.run([str(ptk.cli_path()), "--check", str(tmp_path / "none.txt")], capture_output=True,
                        text=True, timeout=60)
     assert r.returncode != 0 and "cannot open command file" in r.stderr
+
+
+def test_correction_distortion_tokens(ptk, tmp_path):
+    """The tokens of the correction_distortion procedure (src/p-tracker.cpp:
+    1553-1566, 1696-1772): images, imposed displacements, pair range, the 14
+    initial parameters and their perturbations, the minimiser."""
+    (tmp_path / "start.txt").write_text("2\n10 20 0 12\n400 300 0 15\n")
+    (tmp_path / "commands.txt").write_text("""procedure correction_distortion
+image_name img_%d.pgm
+start_file start.txt
+image_numbers_corrDisto 3 10 11 12
+imposedDisplApprox_corrDisto 1.5 -2 3 4
+equiProj_dist_range 100 900
+optim_algo POWELL_ITER powell_num_iter 3
+K1_corrDistor -1e-9 dK1_corrDistor 1e-11 dxc_corrParallax 0.5 angle2_corrParallax 0.01
+optim_algo NEWTON
+""")
+    cfg, out, _ = _check(ptk, tmp_path / "commands.txt", tmp_path)
+    assert cfg["procedure"] == "correction_distortion"
+    assert cfg["corr_images"] == [10, 11, 12]
+    assert cfg["imposed"] == [[0, 0], [1.5, -2], [3, 4]]
+    assert cfg["equiproj_range"] == [100, 900]
+    assert cfg["optim_algo"] == 1 and cfg["powell_num_iter"] == 3
+    # defaults of ptracker::ptracker: negative centres, perturbations 1e-6
+    assert cfg["disto"] == [-1, -1, -1e-9, 0, 0, 0, 0, 0, -1, -1, 0, 0, 0.01, 0]
+    assert cfg["disto_perturb"][2] == 1e-11 and cfg["disto_perturb"][8] == 0.5
+    assert cfg["disto_perturb"][0] == 1e-6 and cfg["disto_perturb"][13] == 1e-6
+    assert any("unknown for optim_algo" in line for line in out)
+
+
+def test_levmar_is_refused(ptk, tmp_path):
+    (tmp_path / "start.txt").write_text("1\n10 20 0 12\n")
+    (tmp_path / "commands.txt").write_text("procedure correction_distortion\nstart_file start.txt\n"
+                                           "image_numbers_corrDisto 2 0 1\noptim_algo LEVMAR\n")
+    r = subprocess.run([str(ptk.cli_path()), "commands.txt"], capture_output=True, text=True, cwd=tmp_path, timeout=60)
+    assert r.returncode != 0 and "LEVMAR" in r.stderr

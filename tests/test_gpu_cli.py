@@ -134,3 +134,98 @@ subpix_method adjoint_lm
         assert np.abs(gr[:, 6] - cr[:, 6]).max() <= 1e-4
         # masked grains do not move (the file keeps 15 significant digits)
         assert np.abs(gr[masked][:, 4:7] - rec[masked][:, 4:7]).max() <= 1e-12
+
+
+def test_cli_correction_distortion(ptk, wl, oracle, cuda_device, tmp_path):
+    """procedure correction_distortion end to end: frames of translated grains
+    seen through radial distortion, tracked from image 0 into images 1 and 2
+    (compared with the oracle's pixel search + Powell from the same imposed
+    displacements), then the POWELL fit of K1 (compared with the oracle's fit
+    on the oracle's tracked displacements) and the output files."""
+    from disto_cases import params
+    p = dict(wl.PRESETS["small16"], dimx=1024, dimy=768, n=60, disp=0.0, rot=0.0, zone=6, disto=(-3e-8, 0.0))
+    X = params(p["dimx"], p["dimy"], -3e-8, 0.0)
+    grains = wl.place(p, 71)
+    ng = grains["cx"].shape[0]
+    shifts = [(0.0, 0.0), (6.3, -4.1), (-7.4, 5.2)]
+    imposed = [(0.0, 0.0), (6.0, -4.0), (-7.0, 5.0)]
+    frames = []
+    for k, (tx, ty) in enumerate(shifts):
+        f = wl.render(p, grains, np.full(ng, tx), np.full(ng, ty), np.zeros(ng), noise_seed=710 + k, disto=X)
+        frames.append(f)
+        write_pgm(tmp_path / f"f{k}.pgm", f.astype(np.uint16))
+    L = oracle.C.CDLL(str(oracle.PORT_SO))
+    with open(tmp_path / "start.txt", "w") as fh:
+        fh.write(f"{ng}\n")
+        for x, y, r in zip(grains["cx"], grains["cy"], grains["r"]):
+            xd, yd = oracle.C.c_double(), oracle.C.c_double()
+            L.orc_distort_point(oracle._p(X), oracle._D(float(x)), oracle._D(float(y)), oracle.C.byref(xd),
+                                oracle.C.byref(yd))
+            fh.write(f"{xd.value!r} {yd.value!r} 0.0 {float(r)!r}\n")
+    perturb = " ".join(f"d{nm} 0" for nm in ("xc_corrDistor", "yc_corrDistor", "K2_corrDistor", "K3_corrDistor",
+                                            "P1_corrDistor", "P2_corrDistor", "P3_corrDistor", "xc_corrParallax",
+                                            "yc_corrParallax", "angle1_corrParallax", "A1_corrParallax",
+                                            "angle2_corrParallax", "A2_corrParallax"))
+    z = (6, 6, 6, 6, 2, 0.005)
+    out = _run(ptk, tmp_path, f"""procedure correction_distortion
+image_name f%d.pgm
+start_file start.txt
+image_numbers_corrDisto 3 0 1 2
+imposedDisplApprox_corrDisto 6 -4 -7 5
+equiProj_dist_range 100 700
+NCC_min 0.7
+{_zone_tokens([z])}
+pattern grain_diameter 1.0 1.0
+optim_algo POWELL
+dK1_corrDistor 1e-9 {perturb}
+""")
+    assert "Number of points for equiprojectivity computations" in out
+    rec = ptk.read_grains_file(str(tmp_path / "start.txt"), format13=False)
+    pair = dict(params=p, ref=frames[0].astype(np.uint16), cur=frames[1].astype(np.uint16), rec=rec)
+    c = oracle.setup(oracle.Port, pair, threads=THREADS, zones=[z], params={"rescue_level": 0, "NCC_min": 0.7})
+    state = rec.copy()
+    dx, dy, ncc = np.zeros((2, ng)), np.zeros((2, ng)), np.zeros((2, ng))
+    for k in (1, 2):
+        if k > 1:
+            c.load_current(frames[k].astype(np.uint16))
+        state[:, 4], state[:, 5] = imposed[k]  # every search starts from the imposed displacement
+        c.set_grains(state)
+        c.grain_diameter_patterns(state, 1.0, 1.0)
+        c.precompute()
+        c.pixel_all()
+        c.subpixel_all()
+        cr = c.get_grains()
+        gr = ptk.read_grains_file(str(tmp_path / f"dic_out_{k}.txt"), format13=True)
+        np.testing.assert_array_equal(gr[:, 0:2], cr[:, 0:2])
+        assert np.abs(gr[:, 4:6] - cr[:, 4:6]).max() <= 1e-3
+        assert np.abs(gr[:, 6] - cr[:, 6]).max() <= 1e-4
+        dx[k - 1], dy[k - 1], ncc[k - 1] = cr[:, 4], cr[:, 5], cr[:, 12]
+        state = cr.copy()
+    log = dict()
+    for line in (tmp_path / "corrDisto_log.txt").read_text().splitlines():
+        key, _, val = line.rpartition(" ")
+        log[key.strip()] = float(val)
+    refx, refy = rec[:, 0].astype(np.int32), rec[:, 1].astype(np.int32)
+    pairs = oracle.disto_pairs(refx, refy, 100.0, 700.0)
+    X0 = np.zeros(14)
+    X0[0] = X0[1] = X0[8] = X0[9] = -1.0
+    DX = np.zeros(14)
+    DX[2] = 1e-9
+    # the fit stage: the oracle's Powell on the displacements the driver wrote
+    cols = [ptk.read_grains_file(str(tmp_path / f"dic_out_{k}.txt"), format13=True) for k in (1, 2)]
+    gdx = np.stack([r[:, 4] for r in cols])
+    gdy = np.stack([r[:, 5] for r in cols])
+    gncc = np.stack([r[:, 12] for r in cols])
+    fx, fini, fend, _, _, _ = oracle.disto_fit(X0, DX, 0, 0, p["dimx"], p["dimy"], refx, refy, gdx, gdy, gncc, 0.7,
+                                               pairs)
+    np.testing.assert_allclose(log["Initial distorsion index"], fini, rtol=1e-9)
+    np.testing.assert_allclose(log["Final distorsion index"], fend, rtol=1e-6)
+    np.testing.assert_allclose(log["K1_corrDistor"], fx[2], rtol=1e-6)
+    # tracking + fit: the oracle end to end, and the distortion the frames were rendered with
+    ox = oracle.disto_fit(X0, DX, 0, 0, p["dimx"], p["dimy"], refx, refy, dx, dy, ncc, 0.7, pairs)[0]
+    np.testing.assert_allclose(log["K1_corrDistor"], ox[2], rtol=0.02)
+    np.testing.assert_allclose(log["K1_corrDistor"], -3e-8, rtol=0.25)
+    assert log["Final distorsion index"] < 0.1 * log["Initial distorsion index"]
+    assert log["xc_corrDistor"] == 512.0 and log["yc_corrParallax"] == 384.0
+    assert len((tmp_path / "errors.txt").read_text().split("\n\n")) >= 50
+    assert (tmp_path / "distobox.txt").read_text().count("\n") > 4 * 50
