@@ -215,6 +215,140 @@ def run_reference_arm(args, rank: int, world: int):
     return 0
 
 
+DISTO_METRIC = "equiprojectivity residuals/s (distortion-fit objective)"
+DISTO_UNIT = "residuals/s"
+
+
+def _disto_setup(ptk, wl, seed: int):
+    case = wl.make_disto_case(seed)
+    pairs = ptk.disto_pairs(case["refx"], case["refy"], 0.0, 1000.0)  # equiProj_dist_range defaults
+    X0 = case["X"].copy()
+    X0[2] = X0[3] = 0.0  # centres at the frame centre, no distortion
+    return case, pairs, X0
+
+
+def _disto_cpu(case, pairs, X0, reference: bool, budget_s: float = 10.0):
+    """Seconds per objective evaluation of the CPU checker (single-threaded,
+    as the reference's objective loop): the oracle restatement, or the loop
+    around the reference's own undistor."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import bind
+    if not reference and not bind.PORT_SO.exists():
+        bind.build(ref=False)
+    times, v = [], None
+    while not times or (sum(times) < budget_s and len(times) < 5):
+        t0 = time.perf_counter()
+        v = bind.disto_objective(X0, case["refx"], case["refy"], case["dx"], case["dy"], case["ncc"], 0.7, pairs,
+                                 reference=reference)
+        times.append(time.perf_counter() - t0)
+    return statistics.mean(times), v, len(times)
+
+
+def run_disto(args, rank: int, world: int, local: int) -> int:
+    """Distortion-parameter fit workload (correction_distortion's
+    minimisation): 2000 grains of a 5616x3744 frame tracked into 3 images,
+    pairs 0..1000 px apart (268,944 pairs, 806,832 residuals per objective
+    evaluation).  One step = one objective evaluation.  A fit is one small
+    problem, so N > 1 runs nothing on ranks other than 0 (replicas only).
+
+      value  device time of the objective's kernels (per-point undistortion,
+             pair residuals, fixed-order sum), inputs resident, L2 flushed
+             before every step (the inputs are smaller than L2);
+      e2e    ptk_disto_objective from the host: parameters in, value out;
+      fit    one POWELL fit of K1 and K2 through ptk_disto_fit, wall time."""
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    ptk = importlib.import_module("p-tracker_b200")
+    wl = importlib.import_module("p-tracker_b200.workloads")
+    case, pairs, X0 = _disto_setup(ptk, wl, seed=rank_seed(rank))
+    n, nimg1, P = case["refx"].shape[0], case["dx"].shape[0], pairs.shape[0]
+    m = nimg1 * P
+    if args.impl == "reference":
+        sec, _, k = _disto_cpu(case, pairs, X0, reference=True)
+        line = {"metric": DISTO_METRIC, "value": m / sec, "unit": DISTO_UNIT, "n_gpus": world, "steps": k,
+                "warmup": 0, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "replicas",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": f"disto: {n} grains of a 5616x3744 frame, {nimg1} tracked images, {P} "
+                                       f"pairs 0..1000 px apart, {m} residuals per evaluation"},
+                "cpu_baseline": {"value": m / sec, "unit": DISTO_UNIT, "cores": 1, "kind": "reference",
+                                 "sample": f"{k} objective evaluations"},
+                "e2e": {"value": m / sec, "unit": DISTO_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+    fit = ptk.DistoFit(case["dimx"], case["dimy"], case["refx"], case["refy"], case["dx"], case["dy"], case["ncc"],
+                       0.7, pairs)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    try:
+        pr = torch.cuda.get_device_properties(local)
+        gpu_id = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+    except Exception:
+        gpu_id = str(local)
+    sampler = ClockSampler(gpu_id)
+    # the timed steps last well under the sampler's 200 ms period: the clocks
+    # are sampled over a warm-up of at least 1.5 s of evaluations before them
+    t_w = time.perf_counter()
+    k = 0
+    while k < args.warmup or time.perf_counter() - t_w < 1.5:
+        fit.objective_timed(X0, 200)
+        k += 1
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ms.append(fit.objective_timed(X0, 1))
+    ms_step = statistics.mean(ms)
+    clocks = sampler.stop()
+    gpu_value = fit.objective(X0)
+    e2e = []
+    for it in range(args.warmup + max(args.e2e_steps, args.steps)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fit.objective(X0)
+        if it >= args.warmup:
+            e2e.append(time.perf_counter() - t0)
+    e2e_ms = statistics.mean(e2e) * 1e3
+    DX = np.zeros(14)
+    DX[2], DX[3] = 1e-10, 1e-17
+    t0 = time.perf_counter()
+    x, ini, end, _ = fit.fit(X0, DX, ptk.DISTO_POWELL)
+    fit_s = time.perf_counter() - t0
+    fit.close()
+    # compulsory bytes of one evaluation after an L2 flush: the pair list, the
+    # per-(image, grain) inputs, the undistorted points written and read back
+    alg_bytes = 8 * P + (8 + 16) * nimg1 * n + 8 * n + 2 * 16 * (nimg1 + 1) * n
+    peaks = measured_peaks()
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    line = {
+        "metric": DISTO_METRIC, "value": m / (ms_step * 1e-3), "unit": DISTO_UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "replicas", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"disto: {n} grains of a 5616x3744 frame, {nimg1} tracked images, {P} pairs "
+                               f"0..1000 px apart, {m} residuals per evaluation",
+                   "l2": "flushed (256 MiB write) before each timed step",
+                   "clocks": "sampled over 1.5 s of evaluations right before the timed steps"},
+        "e2e": {"value": m / (e2e_ms * 1e-3), "unit": DISTO_UNIT, "h2d_bytes_per_step": 14 * 8,
+                "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms},
+        "gpu_launches": 3 * args.steps,
+        "roofline": {"kernel": "k_disto_points + k_disto_residuals + k_disto_sum (one evaluation)", "bound": "hbm",
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "algorithmic_bytes_per_launch": alg_bytes,
+                     "peak_source": peaks["source"] + " copy bandwidth"},
+        "fit": {"algo": "POWELL over K1, K2", "seconds": fit_s, "index_ini": ini, "index_end": end,
+                "K1": x[2], "K2": x[3], "K1_rendered": case["X"][2], "K2_rendered": case["X"][3]},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        sec, cpu_v, k = _disto_cpu(case, pairs, X0, reference=False)
+        line["cpu_baseline"] = {"value": m / sec, "unit": DISTO_UNIT, "cores": 1, "kind": "port",
+                                "sample": f"{k} full objective evaluations"}
+        line["accuracy"] = {"objective_rel_diff_vs_oracle": abs(gpu_value - cpu_v) / cpu_v}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_sequence(args, rank: int, world: int, local: int) -> int:
     """Full-sequence workload (cfg5): every frame of the sequence is brought
     into the current slot, resampled by the on-device lens-distortion remap and
@@ -482,6 +616,8 @@ def main() -> int:
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
     local = _env_int("LOCAL_RANK", 0)
+    if args.workload == "disto":
+        return run_disto(args, rank, world, local)
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
     if args.workload == "cfg5":

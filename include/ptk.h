@@ -285,7 +285,10 @@ const char* ptk_image_error(void);
  *   history (may be NULL) = num_iter x 15 (index, 14 parameters) for
  *   POWELL_ITER.  The reference's LEVMAR uses lmdif1 from the absent toofus
  *   library and is rejected (PTK_ERR_ARG).
- * ptk_disto_tracked: the displacements after POWELL_ITER's re-anchoring. */
+ * ptk_disto_tracked: the displacements after POWELL_ITER's re-anchoring.
+ * ptk_disto_objective_timed (no reference counterpart): `reps` evaluations of
+ *   the objective's kernels between two CUDA events, without read-back;
+ *   *ms_per_eval = their average device time. */
 typedef struct ptk_disto ptk_disto;
 enum { PTK_DISTO_POWELL = 0, PTK_DISTO_POWELL_ITER = 1, PTK_DISTO_LEVMAR = 2 };
 int ptk_disto_pairs(const int32_t* refx, const int32_t* refy, int n, double dmin, double dmax, int32_t* pairs_ij,
@@ -300,6 +303,7 @@ int ptk_disto_residuals(ptk_disto* d, const double* params14, double* value, dou
 int ptk_disto_fit(ptk_disto* d, double* params14, const double* perturb14, int algo, int num_iter,
                   double* index_ini, double* index_end, double* history);
 int ptk_disto_tracked(ptk_disto* d, double* dx, double* dy);
+int ptk_disto_objective_timed(ptk_disto* d, const double* params14, int reps, double* ms_per_eval);
 
 #ifdef __cplusplus
 }

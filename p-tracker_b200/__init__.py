@@ -111,6 +111,7 @@ _SIGS = {
     "ptk_disto_residuals": (C.c_int, [_P, _P, C.POINTER(C.c_double), _P]),
     "ptk_disto_fit": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), _P]),
     "ptk_disto_tracked": (C.c_int, [_P, _P, _P]),
+    "ptk_disto_objective_timed": (C.c_int, [_P, _P, C.c_int, _P]),
 }
 
 _lib = None
@@ -502,6 +503,13 @@ class DistoFit:
         dy = np.zeros((self.nimg1, self.n))
         self._check(self._L.ptk_disto_tracked(self.h, _ptr(dx), _ptr(dy)))
         return dx, dy
+
+    def objective_timed(self, params14, reps: int) -> float:
+        """Average device time (ms) of one objective evaluation's kernels."""
+        x = np.ascontiguousarray(params14, dtype=np.float64)
+        ms = C.c_double()
+        self._check(self._L.ptk_disto_objective_timed(self.h, _ptr(x), int(reps), C.byref(ms)))
+        return ms.value
 
 
 def cli_path() -> Path:

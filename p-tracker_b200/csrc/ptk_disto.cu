@@ -10,10 +10,13 @@
 // undistorted tracked positions, over the pairs whose reference positions lie
 // equiProj_dist_min .. equiProj_dist_max apart (precompute_paires, :63-81) and
 // skipping pairs with a subpixel NCC below NCC_min.  One evaluation is
-// (images - 1) x pairs residuals, four undistor calls each: a grid-stride
-// kernel in FP64 (this file is compiled with -fmad=false, so each residual is
-// the CPU's value bit for bit), reduced in a fixed order over a fixed grid so
-// the sum is reproducible.  The minimiser runs on the host and calls the
+// (images - 1) x pairs residuals.  The reference undistorts four points per
+// residual; here every (image, grain) point is undistorted once (a per-point
+// kernel, images x grains undistor calls instead of 4 x images x pairs) and
+// the residual kernel gathers the four positions of each pair, which stay in
+// L2.  Both run in FP64 (this file is compiled with -fmad=false, so each
+// residual is the CPU's value bit for bit) and the sum is reduced in a fixed
+// order over a fixed grid, so it is reproducible.  The minimiser runs on the host and calls the
 // kernel for every objective value: POWELL (one minimisation, ftol 1e-12,
 // initial directions the perturbations) and POWELL_ITER (num_iter
 // minimisations, each followed by re-anchoring A1/B1 and the displacements on
@@ -38,6 +41,7 @@ struct ptk_disto {
   double *d_dx{nullptr}, *d_dy{nullptr}, *d_dx0{nullptr}, *d_dy0{nullptr}, *d_ncc{nullptr};
   double *d_origx{nullptr}, *d_origy{nullptr};
   double *d_partial{nullptr}, *d_sum{nullptr}, *d_fvec{nullptr};
+  double2* d_pos{nullptr};  // undistorted points: slot 0 A1 (reference), slot 1 + im the tracked ones
   cudaStream_t stream{nullptr};
   std::string err;
 };
@@ -60,8 +64,32 @@ struct DistoData {
   int use_orig;
 };
 
-// One residual per (image, pair); partial[block] = the block's sum of err^2.
-__global__ void __launch_bounds__(kDThreads) k_disto_residuals(DistoData d, Disto X, double* fvec, double* partial) {
+// The undistorted points of one evaluation: pos[g] = A1 of grain g (undistor
+// of its reference position, or the re-anchored position of POWELL_ITER) and
+// pos[(1 + im) * n + g] = undistor of its tracked position in image im.
+__global__ void __launch_bounds__(kDThreads) k_disto_points(DistoData d, Disto X, double2* pos) {
+  const long long k = (long long)blockIdx.x * kDThreads + threadIdx.x;
+  if (k >= (long long)(d.nimg1 + 1) * d.n) return;
+  const int s = (int)(k / d.n), g = (int)(k - (long long)s * d.n);
+  double x, y;
+  if (s == 0) {
+    if (d.use_orig) {
+      x = d.origx[g];
+      y = d.origy[g];
+    } else {
+      undistor_d(X, (double)d.refx[g], (double)d.refy[g], &x, &y);
+    }
+  } else {
+    const size_t o = (size_t)(s - 1) * d.n + g;
+    undistor_d(X, (double)d.refx[g] + d.dx[o], (double)d.refy[g] + d.dy[o], &x, &y);
+  }
+  pos[k] = make_double2(x, y);
+}
+
+// One residual per (image, pair) from the undistorted points;
+// partial[block] = the block's sum of err^2.
+__global__ void __launch_bounds__(kDThreads) k_disto_residuals(DistoData d, const double2* __restrict__ pos,
+                                                               double* fvec, double* partial) {
   __shared__ double red[kDThreads / 32];
   double acc = 0.0;
   const long long m = (long long)d.nimg1 * d.npairs;
@@ -73,24 +101,14 @@ __global__ void __launch_bounds__(kDThreads) k_disto_residuals(DistoData d, Dist
     const size_t oi = (size_t)im * d.n + i, oj = (size_t)im * d.n + j;
     double e = 0.0;
     if (!(d.ncc[oi] < d.NCC_min || d.ncc[oj] < d.NCC_min)) {
-      double A1x, A1y, A2x, A2y, B1x, B1y, B2x, B2y;
-      if (d.use_orig) {
-        A1x = d.origx[i];
-        A1y = d.origy[i];
-        B1x = d.origx[j];
-        B1y = d.origy[j];
-      } else {
-        undistor_d(X, (double)d.refx[i], (double)d.refy[i], &A1x, &A1y);
-        undistor_d(X, (double)d.refx[j], (double)d.refy[j], &B1x, &B1y);
-      }
-      undistor_d(X, (double)d.refx[i] + d.dx[oi], (double)d.refy[i] + d.dy[oi], &A2x, &A2y);
-      undistor_d(X, (double)d.refx[j] + d.dx[oj], (double)d.refy[j] + d.dy[oj], &B2x, &B2y);
-      double ABx = B1x - A1x, ABy = B1y - A1y;
+      const double2 A1 = pos[i], B1 = pos[j];
+      const double2 A2 = pos[(size_t)d.n + oi], B2 = pos[(size_t)d.n + oj];
+      double ABx = B1.x - A1.x, ABy = B1.y - A1.y;
       const double AB = sqrt(ABx * ABx + ABy * ABy);
       ABx /= AB;
       ABy /= AB;
-      const double BBx = B2x - B1x, BBy = B2y - B1y;
-      const double AAx = A2x - A1x, AAy = A2y - A1y;
+      const double BBx = B2.x - B1.x, BBy = B2.y - B1.y;
+      const double AAx = A2.x - A1.x, AAy = A2.y - A1.y;
       e = (ABx * (BBx - AAx)) + (ABy * (BBy - AAy));
       acc += e * e;
     }
@@ -322,7 +340,10 @@ int disto_eval(ptk_disto* d, const double* X14, int use_orig, double* value, dou
       return dfail(d, PTK_ERR_CUDA, "cudaMalloc(residuals)");
     fv = d->d_fvec;
   }
-  k_disto_residuals<<<kDBlocks, kDThreads, 0, d->stream>>>(data_of(d, use_orig), X, fv, d->d_partial);
+  const DistoData dd = data_of(d, use_orig);
+  const long long npts = (long long)(d->nimg1 + 1) * d->n;
+  if (npts > 0) k_disto_points<<<(unsigned)((npts + kDThreads - 1) / kDThreads), kDThreads, 0, d->stream>>>(dd, X, d->d_pos);
+  k_disto_residuals<<<kDBlocks, kDThreads, 0, d->stream>>>(dd, d->d_pos, fv, d->d_partial);
   k_disto_sum<<<1, kDThreads, 0, d->stream>>>(d->d_partial, kDBlocks, d->d_sum);
   cudaError_t e = cudaMemcpyAsync(value, d->d_sum, sizeof(double), cudaMemcpyDeviceToHost, d->stream);
   if (e == cudaSuccess && fv) e = cudaMemcpyAsync(fvec_host, fv, sizeof(double) * m, cudaMemcpyDeviceToHost, d->stream);
@@ -394,6 +415,7 @@ int ptk_disto_create(ptk_disto** out, int dimx, int dimy, const int32_t* refx, c
   alloc((void**)&d->d_origy, sizeof(double) * n);
   alloc((void**)&d->d_partial, sizeof(double) * kDBlocks);
   alloc((void**)&d->d_sum, sizeof(double));
+  alloc((void**)&d->d_pos, sizeof(double2) * (size_t)(n_tracked + 1) * n);
   if (ok) {
     std::vector<double> ox(n), oy(n);
     for (int g = 0; g < n; ++g) {
@@ -435,6 +457,7 @@ int ptk_disto_destroy(ptk_disto* d) {
   cudaFree(d->d_partial);
   cudaFree(d->d_sum);
   cudaFree(d->d_fvec);
+  cudaFree(d->d_pos);
   if (d->stream) cudaStreamDestroy(d->stream);
   delete d;
   return PTK_OK;
@@ -494,6 +517,35 @@ int ptk_disto_fit(ptk_disto* d, double* params14, const double* perturb14, int a
   if (!f(X, &v)) return rc;
   *index_end = v / nb;
   for (int k = 0; k < 14; ++k) params14[k] = X[k];
+  return PTK_OK;
+}
+
+int ptk_disto_objective_timed(ptk_disto* d, const double* params14, int reps, double* ms_per_eval) {
+  if (!d || !params14 || !ms_per_eval || reps < 1) return dfail(d, PTK_ERR_ARG, "null argument or reps < 1");
+  const Disto X = make_disto(params14);
+  const DistoData dd = data_of(d, 0);
+  const long long npts = (long long)(d->nimg1 + 1) * d->n;
+  cudaEvent_t ev[2];
+  if (cudaEventCreate(&ev[0]) != cudaSuccess) return dfail(d, PTK_ERR_CUDA, "cudaEventCreate");
+  if (cudaEventCreate(&ev[1]) != cudaSuccess) {
+    cudaEventDestroy(ev[0]);
+    return dfail(d, PTK_ERR_CUDA, "cudaEventCreate");
+  }
+  cudaEventRecord(ev[0], d->stream);
+  for (int k = 0; k < reps; ++k) {
+    k_disto_points<<<(unsigned)((npts + kDThreads - 1) / kDThreads), kDThreads, 0, d->stream>>>(dd, X, d->d_pos);
+    k_disto_residuals<<<kDBlocks, kDThreads, 0, d->stream>>>(dd, d->d_pos, nullptr, d->d_partial);
+    k_disto_sum<<<1, kDThreads, 0, d->stream>>>(d->d_partial, kDBlocks, d->d_sum);
+  }
+  cudaEventRecord(ev[1], d->stream);
+  cudaError_t e = cudaEventSynchronize(ev[1]);
+  float ms = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (e != cudaSuccess) return dfail(d, PTK_ERR_CUDA, std::string("timed objective: ") + cudaGetErrorString(e));
+  *ms_per_eval = (double)ms / reps;
   return PTK_OK;
 }
 

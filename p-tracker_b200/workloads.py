@@ -207,3 +207,43 @@ def make_sequence(name_or_params, seed: int = 1, frames: int | None = None) -> d
            for k, (dx, dy, th) in enumerate(motion)]
     return dict(params=p, frames=out, rec=start_records(grains), grains=grains, disto=disto, motion=motion,
                 jumpers=jumpers, jump_frame=jump_frame)
+
+
+def make_disto_case(seed: int = 1, n: int = 2000, n_tracked: int = 3, dimx: int = 5616, dimy: int = 3744,
+                    k1: float = -2e-9, k2: float = 1e-16, noise: float = 0.01, low_ncc: float = 0.03) -> dict:
+    """Inputs of the distortion-parameter fit (correction_distortion): n grains
+    at integer reference positions of a dimx x dimy frame seen through the
+    radial lens (k1, k2) about the frame centre, and the displacements a
+    tracker reports in n_tracked images where the scene moved by one
+    translation each (+-20 px, equiprojective), plus Gaussian tracking noise
+    (px) and a fraction of failed grains (NCC_subpix 0.3; the others 0.98).
+    The distorted positions invert the radial model by fixed-point iteration."""
+    rng = np.random.default_rng(seed)
+    X = distortion_params(dict(dimx=dimx, dimy=dimy, disto=(k1, k2)))
+    xc, yc = X[0], X[1]
+    w = dimx - 200
+    cell = rng.choice(w * (dimy - 200), size=n, replace=False)  # distinct positions: no pair of length 0
+    refx = (100 + cell % w).astype(np.int32)
+    refy = (100 + cell // w).astype(np.int32)
+
+    def radial(x, y):
+        r2 = (x - xc) ** 2 + (y - yc) ** 2
+        return k1 * r2 + k2 * r2 * r2
+
+    f = radial(refx.astype(np.float64), refy.astype(np.float64))
+    ux = refx + (refx - xc) * f
+    uy = refy + (refy - yc) * f
+    dx = np.zeros((n_tracked, n))
+    dy = np.zeros((n_tracked, n))
+    for im in range(n_tracked):
+        t = rng.uniform(-20.0, 20.0, 2)
+        tx, ty = ux + t[0], uy + t[1]
+        xd, yd = tx.copy(), ty.copy()
+        for _ in range(30):  # xu = xd + (xd - xc) f(xd): contraction, |f| < 0.03 on the frame
+            g = radial(xd, yd)
+            xd = xc + (tx - xc) / (1.0 + g)
+            yd = yc + (ty - yc) / (1.0 + g)
+        dx[im] = xd - refx + rng.normal(0.0, noise, n)
+        dy[im] = yd - refy + rng.normal(0.0, noise, n)
+    ncc = np.where(rng.random((n_tracked, n)) < low_ncc, 0.3, 0.98)
+    return dict(X=X, refx=refx, refy=refy, dx=dx, dy=dy, ncc=ncc, dimx=dimx, dimy=dimy)
