@@ -349,6 +349,130 @@ def run_disto(args, rank: int, world: int, local: int) -> int:
     return 0
 
 
+RAW_METRIC = "RAW frames demosaiced/s (5616x3744, DemosaicModel -2 + rescaleGrayLevels)"
+RAW_UNIT = "frames/s"
+
+
+def run_raw(args, rank: int, world: int, local: int) -> int:
+    """RAW ingest workload: a 5616x3744 frame in a 5680x3760 16-bit sensor
+    mosaic (margins 24 / 8), DemosaicModel -2 (3x3 binomial) with the grey
+    rescale, into a frame slot of the context.  One step = one frame.  Frames
+    are independent: N > 1 runs nothing on ranks other than 0 (replicas).
+
+      value  ptk_load_frame_raw_device on a device-resident mosaic: the
+             demosaic pass (with MinGray/MaxGray) and the rescale pass, CUDA
+             events on the context stream, L2 flushed before each step;
+      e2e    ptk_load_frame_raw from a pinned host mosaic (upload included)
+             returning MinGray/MaxGray to the host."""
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    ptk = importlib.import_module("p-tracker_b200")
+    W, H, RW, RH, L, T, MODE = 5616, 3744, 5680, 3760, 24, 8, -2
+    rng = np.random.default_rng(rank_seed(rank))
+    raw = rng.integers(0, 16384, (RH, RW)).astype(np.uint16)
+    raw_pin = torch.from_numpy(raw.view(np.int16)).pin_memory()
+    if args.impl == "reference":
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import bind
+        ref = bind.have_reference()
+        times = []
+        for _ in range(max(1, min(args.steps, 5))):
+            t0 = time.perf_counter()
+            bind.raw_demosaic(raw, W, H, L, T, MODE, True, reference=ref)
+            times.append(time.perf_counter() - t0)
+        sec = statistics.mean(times)
+        line = {"metric": RAW_METRIC, "value": 1.0 / sec, "unit": RAW_UNIT, "n_gpus": world, "steps": len(times),
+                "warmup": 0, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "replicas",
+                "vs_baseline": None, "dtype": "u16", "data": "synthetic", "impl": "reference",
+                "config": {"workload": "raw: 5616x3744 frame of a 5680x3760 u16 mosaic, mode -2, rescale"},
+                "cpu_baseline": {"value": 1.0 / sec, "unit": RAW_UNIT, "cores": 1,
+                                 "kind": "reference" if ref else "port", "sample": f"{len(times)} whole frames"},
+                "e2e": {"value": 1.0 / sec, "unit": RAW_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+    stream = torch.cuda.Stream()
+    t = ptk.Tracker(W, H)
+    t.set_stream(stream.cuda_stream)
+    d_raw = raw_pin.cuda()
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    try:
+        pr = torch.cuda.get_device_properties(local)
+        gpu_id = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+    except Exception:
+        gpu_id = str(local)
+    with torch.cuda.stream(stream):
+        sampler = ClockSampler(gpu_id)
+        t_w = time.perf_counter()
+        k = 0
+        while k < args.warmup or time.perf_counter() - t_w < 1.5:  # clocks sampled over >= 1.5 s of frames
+            t.load_frame_raw_device(0, d_raw.data_ptr(), RW, RH, L, T, MODE, True)
+            stream.synchronize()
+            k += 1
+        ms = []
+        l0 = t.launches()
+        for _ in range(args.steps):
+            flush.zero_()
+            stream.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t.load_frame_raw_device(0, d_raw.data_ptr(), RW, RH, L, T, MODE, True)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        launches = t.launches() - l0
+        clocks = sampler.stop()
+        e2e = []
+        for it in range(args.warmup + max(args.e2e_steps, args.steps)):
+            flush.zero_()
+            stream.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            mm = t.load_frame_raw(0, raw_pin.numpy().view(np.uint16), L, T, MODE, True)
+            e1.record(stream)
+            e1.synchronize()
+            if it >= args.warmup:
+                e2e.append(e0.elapsed_time(e1))
+        frame = t.read_frame(0)
+    t.close()
+    ms_step, e2e_ms = statistics.mean(ms), statistics.mean(e2e)
+    alg_bytes = 2 * W * H * 2 + 2 * W * H * 2  # demosaic: mosaic read + frame write; rescale: frame read + write
+    peaks = measured_peaks()
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    line = {
+        "metric": RAW_METRIC, "value": 1e3 / ms_step, "unit": RAW_UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "replicas",
+        "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": f"raw: {W}x{H} frame of a {RW}x{RH} u16 mosaic (margins {L}/{T}), DemosaicModel "
+                               f"{MODE}, rescaleGrayLevels", "l2": "flushed (256 MiB write) before each timed step",
+                   "clocks": "sampled over 1.5 s of frames right before the timed steps"},
+        "e2e": {"value": 1e3 / e2e_ms, "unit": RAW_UNIT, "h2d_bytes_per_step": int(raw.nbytes),
+                "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": "k_raw_demosaic + k_raw_rescale (one frame)", "bound": "hbm", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peaks["source"] + " copy bandwidth"},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import bind
+        if not bind.PORT_SO.exists():
+            bind.build(ref=False)
+        t0 = time.perf_counter()
+        want, mm_want = bind.raw_demosaic(raw, W, H, L, T, MODE, True)
+        sec = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": RAW_UNIT, "cores": 1, "kind": "port",
+                                "sample": "one whole frame"}
+        line["accuracy"] = {"frame_equal_to_oracle": bool(np.array_equal(frame, want)),
+                            "min_max_equal_to_oracle": list(mm) == list(mm_want)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_sequence(args, rank: int, world: int, local: int) -> int:
     """Full-sequence workload (cfg5): every frame of the sequence is brought
     into the current slot, resampled by the on-device lens-distortion remap and
@@ -618,6 +742,8 @@ def main() -> int:
     local = _env_int("LOCAL_RANK", 0)
     if args.workload == "disto":
         return run_disto(args, rank, world, local)
+    if args.workload == "raw":
+        return run_raw(args, rank, world, local)
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
     if args.workload == "cfg5":

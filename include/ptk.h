@@ -147,6 +147,25 @@ int ptk_load_frame(ptk_ctx* ctx, int slot, const void* pix, int dimx, int dimy, 
                    size_t pitch_bytes);
 /* Same with a device pointer (uint16, row-major, pitch in bytes). */
 int ptk_load_frame_device(ptk_ctx* ctx, int slot, const void* dev_pix, size_t pitch_bytes);
+/* A frame from an unpacked RAW sensor mosaic, demosaiced on the GPU as
+ * read_raw_image does after libraw's unpack (src/p-tracker.cpp:288-383):
+ * `raw` is libraw's rawdata.raw_image (raw_width x raw_height uint16,
+ * row-major), the frame (the context's dimx x dimy = sizes.width x height)
+ * starts at (left_margin, top_margin).  mode = DemosaicModel:
+ * PTK_DEMOSAIC_BOX2 (-1) floor of the 2x2 mean, PTK_DEMOSAIC_BINOMIAL3 (-2)
+ * floor of the 1-2-1 x 1-2-1 / 16 mean, PTK_DEMOSAIC_GREY (-20) the raw
+ * values.  Neighbours are taken in the flat raw array as the reference does;
+ * a call whose stencil reaches outside it is rejected (PTK_ERR_ARG), and so
+ * are libraw's own modes (>= 0).  rescale != 0 is rescaleGrayLevels:
+ * floor((v - MinGray) * 65535 / (MaxGray - MinGray)), skipped when all
+ * pixels are equal (the reference divides by zero there).  min_max, when not
+ * NULL, receives MinGray and MaxGray (and the call waits for the stream). */
+enum { PTK_DEMOSAIC_BOX2 = -1, PTK_DEMOSAIC_BINOMIAL3 = -2, PTK_DEMOSAIC_GREY = -20 };
+int ptk_load_frame_raw(ptk_ctx* ctx, int slot, const uint16_t* raw, int raw_width, int raw_height, int left_margin,
+                       int top_margin, int mode, int rescale, uint16_t* min_max);
+/* Same with the mosaic already in device memory. */
+int ptk_load_frame_raw_device(ptk_ctx* ctx, int slot, const uint16_t* dev_raw, int raw_width, int raw_height,
+                              int left_margin, int top_margin, int mode, int rescale, uint16_t* min_max);
 /* Copies a slot back to the host as uint16 rows of dimx values. */
 int ptk_read_frame(ptk_ctx* ctx, int slot, uint16_t* out);
 

@@ -322,6 +322,30 @@ def remap(params14, src: np.ndarray, threads: int = 1) -> np.ndarray:
     return out
 
 
+def raw_demosaic(raw: np.ndarray, width: int, height: int, left: int, top: int, mode: int, rescale: bool,
+                 reference: bool = False):
+    """Grey frame (height, width) from an unpacked RAW mosaic (raw_height,
+    raw_width) with DemosaicModel `mode` (-1, -2, -20): the port's
+    restatement (returns (frame, (MinGray, MaxGray)), or None when a stencil
+    leaves the array), or the reference's own read_raw_image on the mosaic
+    (returns (frame, None))."""
+    r = np.ascontiguousarray(raw, dtype=np.uint16)
+    out = np.zeros((height, width), dtype=np.uint16)
+    if reference:
+        L = C.CDLL(str(REF_SO))
+        L.ref_create.restype = _P
+        h = C.c_void_p(L.ref_create(8, 8))
+        L.ref_raw_demosaic(h, _p(r), _I(r.shape[1]), _I(r.shape[0]), _I(width), _I(height), _I(left), _I(top),
+                           _I(mode), _I(int(rescale)), _p(out))
+        L.ref_destroy(h)
+        return out, None
+    L = C.CDLL(str(PORT_SO))
+    mm = np.zeros(2, dtype=np.uint16)
+    rc = L.orc_raw_demosaic(_p(r), _I(r.shape[1]), _I(r.shape[0]), _I(width), _I(height), _I(left), _I(top),
+                            _I(mode), _I(int(rescale)), _p(out), _p(mm))
+    return None if rc != 0 else (out, (int(mm[0]), int(mm[1])))
+
+
 def setup(cls, pair: dict, threads: int = 1, zones=None, params: dict | None = None, pattern=("grain_diameter", 1.0, 1.0)):
     """Builds a checker (Port or Reference) for a workload pair."""
     p = pair["params"]

@@ -931,4 +931,57 @@ int orc_save_grains(void* p, const char* path, const char* from_name, const char
   return 0;
 }
 
+// Grey frame from an unpacked RAW sensor mosaic (read_raw_image,
+// src/p-tracker.cpp:288-372): -1 the floor of the 2x2 mean of the pixel and
+// its right/lower neighbours, -2 the floor of the 1-2-1 x 1-2-1 / 16 weighted
+// mean of the 3x3 block around it, -20 the raw value; neighbours are found
+// in the flat raw array (index (left + x + i) + raw_width (top + y + j)).
+// Then (:374-383) with rescale: floor((v - min) * (65535 / (max - min))).
+// Returns 0, or -1 when a stencil index leaves the array or the mode is
+// not one of the three; min_max receives the frame's MinGray/MaxGray.
+int orc_raw_demosaic(const uint16_t* raw, int raw_width, int raw_height, int width, int height, int left, int top,
+                     int mode, int rescale, uint16_t* out, uint16_t* min_max) {
+  int lo = 0, hi = 0;
+  static const double w2[2][2] = {{0.25, 0.25}, {0.25, 0.25}};
+  static const double w3[3][3] = {{0.0625, 0.125, 0.0625}, {0.125, 0.25, 0.125}, {0.0625, 0.125, 0.0625}};
+  if (mode == -1) {
+    lo = 0;
+    hi = 1;
+  } else if (mode == -2) {
+    lo = -1;
+    hi = 1;
+  } else if (mode != -20) {
+    return -1;
+  }
+  const long long n = (long long)raw_width * raw_height;
+  const long long first = (long long)(left + lo) + (long long)raw_width * (top + lo);
+  const long long last = (long long)(left + width - 1 + hi) + (long long)raw_width * (top + height - 1 + hi);
+  if (first < 0 || last >= n) return -1;
+  unsigned mn = 65535, mx = 0;
+  for (int y = 0; y < height; ++y) {
+    for (int x = 0; x < width; ++x) {
+      double v = 0.0;
+      for (int j = lo; j <= hi; ++j)
+        for (int i = lo; i <= hi; ++i) {
+          const double w = mode == -1 ? w2[j][i] : mode == -2 ? w3[j + 1][i + 1] : 1.0;
+          v += w * (double)raw[(long long)(left + x + i) + (long long)raw_width * (top + y + j)];
+        }
+      const uint16_t g = (uint16_t)(unsigned)std::floor(v);
+      out[(size_t)y * width + x] = g;
+      if (g < mn) mn = g;
+      if (g > mx) mx = g;
+    }
+  }
+  if (rescale && mx > mn) {
+    const double fact = 65535.0 / (double)(int)(mx - mn);
+    for (size_t k = 0; k < (size_t)width * height; ++k)
+      out[k] = (uint16_t)std::floor((double)((int)out[k] - (int)mn) * fact);
+  }
+  if (min_max) {
+    min_max[0] = (uint16_t)mn;
+    min_max[1] = (uint16_t)mx;
+  }
+  return 0;
+}
+
 }  // extern "C"

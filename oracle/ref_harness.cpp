@@ -426,4 +426,29 @@ int ref_read_grains(void* p, const char* path, int ptracker_format) {
 
 int ref_num_grains(void* p) { return static_cast<Handle*>(p)->trk.num_grains; }
 
+// ptracker::read_raw_image (src/p-tracker.cpp:214-387) run on an unpacked
+// sensor mosaic (raw_width x raw_height, row-major) registered with the
+// libraw stub; the visible width x height frame is read back row-major into
+// out (slot 0; first_time, so the reference also sizes dimx/dimy from it).
+void ref_raw_demosaic(void* p, const uint16_t* raw, int raw_width, int raw_height, int width, int height,
+                      int left_margin, int top_margin, int mode, int rescale, uint16_t* out) {
+  ptracker& t = static_cast<Handle*>(p)->trk;
+  std::vector<uint16_t> copy(raw, raw + (size_t)raw_width * raw_height);
+  libraw_stub_data& src = libraw_stub_source();
+  src = libraw_stub_data{};
+  src.sizes.width = width;
+  src.sizes.height = height;
+  src.sizes.raw_width = raw_width;
+  src.sizes.left_margin = left_margin;
+  src.sizes.top_margin = top_margin;
+  src.color.maximum = 65535;
+  src.rawdata.raw_image = copy.data();
+  t.DemosaicModel = mode;
+  t.rescaleGrayLevels = rescale;
+  t.read_raw_image(0, "mosaic", true);
+  src.rawdata.raw_image = nullptr;
+  for (int y = 0; y < height; ++y)
+    for (int x = 0; x < width; ++x) out[(size_t)y * width + x] = t.image[0][x][y];
+}
+
 }  // extern "C"

@@ -29,6 +29,7 @@ ST_RESCUED, ST_SUPER_RESCUED, ST_FAILED, ST_OUT_OF_BOUNDS, ST_MASKED, ST_SUBPIX_
 INTERP = {"linear": 0, "cubic": 1, "quintic": 2}
 SUBPIX_POWELL, SUBPIX_ADJOINT_LM = 0, 1
 SEARCH_EXACT, SEARCH_BF16 = 0, 1
+DEMOSAIC_BOX2, DEMOSAIC_BINOMIAL3, DEMOSAIC_GREY = -1, -2, -20
 PATTERN = {"circ": 0, "ring": 1, "rect": 2, "grain_diameter": 3}
 
 
@@ -74,6 +75,8 @@ _SIGS = {
     "ptk_pattern_size": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "ptk_load_frame": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int, C.c_int, C.c_size_t]),
     "ptk_load_frame_device": (C.c_int, [_P, C.c_int, _P, C.c_size_t]),
+    "ptk_load_frame_raw": (C.c_int, [_P, C.c_int, _P] + [C.c_int] * 6 + [_P]),
+    "ptk_load_frame_raw_device": (C.c_int, [_P, C.c_int, _P] + [C.c_int] * 6 + [_P]),
     "ptk_read_frame": (C.c_int, [_P, C.c_int, _P]),
     "ptk_precompute": (C.c_int, [_P]),
     "ptk_search": (C.c_int, [_P, C.c_int]),
@@ -301,6 +304,23 @@ class Tracker:
 
     def load_frame_device(self, slot: int, dev_ptr: int, pitch_bytes: int):
         self._check(self._L.ptk_load_frame_device(self.h, slot, C.c_void_p(dev_ptr), pitch_bytes), self.h)
+
+    def load_frame_raw(self, slot: int, raw: np.ndarray, left_margin: int, top_margin: int, mode: int,
+                       rescale: bool = False) -> tuple[int, int]:
+        """A frame from an unpacked RAW mosaic (raw_height, raw_width) uint16,
+        demosaiced on the GPU with DemosaicModel `mode` (-1, -2, -20);
+        returns (MinGray, MaxGray)."""
+        r = np.ascontiguousarray(raw, dtype=np.uint16)
+        mm = np.zeros(2, dtype=np.uint16)
+        self._check(self._L.ptk_load_frame_raw(self.h, slot, _ptr(r), r.shape[1], r.shape[0], left_margin,
+                                               top_margin, mode, int(rescale), _ptr(mm)), self.h)
+        return int(mm[0]), int(mm[1])
+
+    def load_frame_raw_device(self, slot: int, dev_ptr: int, raw_width: int, raw_height: int, left_margin: int,
+                              top_margin: int, mode: int, rescale: bool = False):
+        """Same with the mosaic in device memory; does not wait for the GPU."""
+        self._check(self._L.ptk_load_frame_raw_device(self.h, slot, C.c_void_p(dev_ptr), raw_width, raw_height,
+                                                      left_margin, top_margin, mode, int(rescale), None), self.h)
 
     def read_frame(self, slot: int) -> np.ndarray:
         out = np.zeros((self.cfg.dimy, self.cfg.dimx), dtype=np.uint16)

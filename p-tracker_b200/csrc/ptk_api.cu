@@ -58,6 +58,9 @@ struct ptk_ctx {
   uint16_t* d_img[2]{nullptr, nullptr};
   uint16_t* d_tmp{nullptr};
   uint8_t* d_u8{nullptr};
+  uint16_t* d_raw{nullptr};  // staging of a host RAW mosaic (ptk_load_frame_raw)
+  size_t raw_cap{0};         // elements
+  unsigned* d_minmax{nullptr};
   int ref_slot{0}, cur_slot{1};
   bool loaded[2]{false, false};
 
@@ -689,6 +692,8 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_img[1]);
   cudaFree(c->d_tmp);
   cudaFree(c->d_u8);
+  cudaFree(c->d_raw);
+  cudaFree(c->d_minmax);
   cudaFree(c->d_block);
   cudaFree(c->d_snap);
   if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -950,6 +955,60 @@ int ptk_load_frame_device(ptk_ctx* c, int slot, const void* dev_pix, size_t pitc
   c->loaded[slot] = true;
   if (slot == 0) c->need_precompute = true;
   return PTK_OK;
+}
+
+static int load_frame_raw(ptk_ctx* c, int slot, const uint16_t* raw, bool raw_on_device, int raw_width,
+                          int raw_height, int left, int top, int mode, int rescale, uint16_t* min_max) {
+  if (!c || !raw || slot < 0 || slot > 1) return fail(c, PTK_ERR_ARG, "bad frame arguments");
+  if (mode != -1 && mode != -2 && mode != -20)
+    return fail(c, PTK_ERR_ARG, "DemosaicModel must be -1, -2 or -20 (libraw's own modes need libraw)");
+  if (raw_width < 1 || raw_height < 1 || left < 0 || top < 0) return fail(c, PTK_ERR_ARG, "bad mosaic geometry");
+  const long long n = (long long)raw_width * raw_height;
+  const int lo = raw_stencil_lo(mode), hi = raw_stencil_hi(mode);
+  const long long first = (long long)(left + lo) + (long long)raw_width * (top + lo);
+  const long long last =
+      (long long)(left + c->cfg.dimx - 1 + hi) + (long long)raw_width * (top + c->cfg.dimy - 1 + hi);
+  if (first < 0 || last >= n)
+    return fail(c, PTK_ERR_ARG, "the demosaic stencil reaches outside the raw mosaic (check margins and sizes)");
+  if (!c->d_minmax) CK(cudaMalloc(&c->d_minmax, 2 * sizeof(unsigned)));
+  const uint16_t* src = raw;
+  if (!raw_on_device) {
+    if ((size_t)n > c->raw_cap) {
+      cudaFree(c->d_raw);
+      c->d_raw = nullptr;
+      c->raw_cap = 0;
+      CK(cudaMalloc(&c->d_raw, (size_t)n * 2));
+      c->raw_cap = (size_t)n;
+    }
+    CK(cudaMemcpyAsync(c->d_raw, raw, (size_t)n * 2, cudaMemcpyHostToDevice, c->stream));
+    src = c->d_raw;
+  }
+  const int phys = slot == 0 ? c->ref_slot : c->cur_slot;
+  launch_raw_demosaic(src, raw_width, left, top, mode, rescale, c->d_img[phys], c->pitch, c->cfg.dimx, c->cfg.dimy,
+                      c->d_minmax, c->num_sms, c->stream);
+  CK(cudaGetLastError());
+  c->launches += rescale ? 2 : 1;
+  if (min_max) {
+    unsigned mm[2];
+    CK(cudaMemcpyAsync(mm, c->d_minmax, sizeof(mm), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    min_max[0] = (uint16_t)mm[0];
+    min_max[1] = (uint16_t)mm[1];
+  }
+  c->loaded[slot] = true;
+  if (slot == 0) c->need_precompute = true;
+  return PTK_OK;
+}
+
+int ptk_load_frame_raw(ptk_ctx* c, int slot, const uint16_t* raw, int raw_width, int raw_height, int left_margin,
+                       int top_margin, int mode, int rescale, uint16_t* min_max) {
+  return load_frame_raw(c, slot, raw, false, raw_width, raw_height, left_margin, top_margin, mode, rescale, min_max);
+}
+
+int ptk_load_frame_raw_device(ptk_ctx* c, int slot, const uint16_t* dev_raw, int raw_width, int raw_height,
+                              int left_margin, int top_margin, int mode, int rescale, uint16_t* min_max) {
+  return load_frame_raw(c, slot, dev_raw, true, raw_width, raw_height, left_margin, top_margin, mode, rescale,
+                        min_max);
 }
 
 int ptk_read_frame(ptk_ctx* c, int slot, uint16_t* out) {

@@ -163,5 +163,11 @@ void launch_remap_build(const double* params14, const double* trig4, double2* ma
                         cudaStream_t s);
 void launch_remap_apply(const double2* map, const uint16_t* src, uint16_t* dst, int pitch, int dimx, int dimy,
                         cudaStream_t s);
+// RAW mosaic -> grey frame (ptk_raw.cu): stencil offsets of a mode, and the
+// demosaic (+ rescale) launches; min_max = 2 unsigned of device scratch.
+int raw_stencil_lo(int mode);
+int raw_stencil_hi(int mode);
+void launch_raw_demosaic(const uint16_t* raw, int raw_width, int left, int top, int mode, int rescale, uint16_t* dst,
+                         int pitch, int dimx, int dimy, unsigned* min_max, int num_sms, cudaStream_t s);
 
 }  // namespace ptk

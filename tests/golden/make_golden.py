@@ -3,7 +3,8 @@ reference's own tracking code, compiled from its sources into
 oracle/_ref/libptk_ref.so (oracle/Makefile, target `ref`).
 
 Run where the reference sources exist:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py             (all fixtures)
+    python tests/golden/make_golden.py --raw-only  (raw_demosaic.npz only)
 Inputs are seeded synthetic frames (p-tracker_b200/workloads.py); every
 output stored here is what the compiled reference returned.
 """
@@ -85,7 +86,34 @@ def run_case(cls, pair, c):
     return t, out
 
 
+# RAW mosaics: (mode, rescale, raw (height, width), frame (width, height), left, top); the third case
+# puts the frame at column 0, so the -2 stencil of column 0 reads the previous row's last pixel and
+# the last column's right neighbour is the next row's first pixel (the flat indexing of the reference)
+RAW_CASES = [(-1, 0, (61, 83), (80, 58), 1, 2), (-2, 1, (64, 100), (98, 61), 1, 1), (-2, 0, (50, 70), (70, 46), 0, 2),
+             (-20, 1, (40, 60), (57, 37), 3, 3), (-1, 1, (33, 47), (45, 30), 0, 0), (-2, 1, (48, 66), (61, 44), 2, 2)]
+
+
+def raw_demosaic_fixtures():
+    """read_raw_image (src/p-tracker.cpp:214-387) of the reference, run on
+    seeded mosaics through the libraw stand-in: raw_demosaic.npz."""
+    rng = np.random.default_rng(77)
+    out = {}
+    for k, (mode, resc, (rh, rw), (w, h), left, top) in enumerate(RAW_CASES):
+        raw = rng.integers(0, 4096, (rh, rw)).astype(np.uint16)
+        raw[rng.random((rh, rw)) < 0.05] = 65535
+        raw[rh // 3: rh // 3 + 4, 5:25] = rng.integers(50000, 65536, (4, 20))
+        frame, _ = bind.raw_demosaic(raw, w, h, left, top, mode, bool(resc), reference=True)
+        out[f"raw_{k}"] = raw
+        out[f"frame_{k}"] = frame
+        out[f"case_{k}"] = np.array([mode, resc, w, h, left, top])
+    np.savez_compressed(HERE / "raw_demosaic.npz", **out)
+
+
 def main():
+    if "--raw-only" in sys.argv:
+        bind.build()
+        raw_demosaic_fixtures()
+        return
     assert bind.REF_SO.exists() or (bind.REF_SRC / "p-tracker.cpp").exists(), "reference sources needed"
     bind.build()
     sys.path.insert(0, str(ROOT))
@@ -138,6 +166,7 @@ def main():
     np.savez_compressed(HERE / "patterns.npz", **pats)
     np.savez_compressed(HERE / "rotation_steps.npz",
                         **{f"inc{inc}_num{num}": rotation_steps(inc, num) for inc, num in STEP_CASES})
+    raw_demosaic_fixtures()
     print("golden fixtures written to", HERE)
 
 
