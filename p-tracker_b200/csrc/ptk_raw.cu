@@ -17,10 +17,10 @@
 // done in double with one correctly rounded division and one product, as on
 // the CPU (this file is compiled with -fmad=false).
 //
-// One pass reads the mosaic (2 bytes per pixel, the 3x3 neighbours come from
-// L1) and writes the frame (2 bytes per pixel), two pixels per thread, rows
-// grid-strided over a grid of a few CTAs per SM; each CTA folds its pixels'
-// minimum and maximum into one atomicMin/atomicMax.  The rescale, when
+// One pass reads the mosaic (2 bytes per pixel, plus the halo rows of 8-row
+// strips, which L2 serves) and writes the frame (2 bytes per pixel), two
+// pixels per thread; each CTA folds its pixels' minimum and maximum into one
+// atomicMin/atomicMax.  The rescale, when
 // asked for, is a second pass over the frame that reads the extremes from
 // device memory, so nothing returns to the host in between.
 #include "ptk_internal.cuh"
@@ -29,45 +29,83 @@ namespace ptk {
 
 namespace {
 
-constexpr int kRawThreads = 128;  // 2 pixels each: 256 columns per CTA row
+constexpr int kRawThreads = 128;  // demosaic: 2 pixels each (256 columns per CTA); rescale: 8 pixels each
+constexpr int kRawRows = 8;       // rows of one demosaic CTA's strip
 
+// Horizontal sums of one mosaic row for the thread's two pixels a (column c)
+// and b (column c + 1), c the flat index of pixel a in that row:
+// -1: v[c] + v[c+1], v[c+1] + v[c+2];  -2: v[c-1] + 2 v[c] + v[c+1], v[c] + 2 v[c+1] + v[c+2];
+// -20: v[c], v[c+1].  `two` = pixel b exists.
 template <int MODE>
-__device__ __forceinline__ unsigned raw_pixel(const uint16_t* __restrict__ raw, long long idx, int w) {
-  if (MODE == -20) return __ldg(raw + idx);
-  if (MODE == -1) {
-    const unsigned s = (unsigned)__ldg(raw + idx) + __ldg(raw + idx + 1) + __ldg(raw + idx + w + 1) +
-                       __ldg(raw + idx + w);
-    return s >> 2;
+__device__ __forceinline__ void raw_hsum(const uint16_t* __restrict__ raw, long long c, bool two, unsigned& ha,
+                                         unsigned& hb) {
+  if (MODE == -20) {
+    ha = __ldg(raw + c);
+    hb = two ? __ldg(raw + c + 1) : 0u;
+  } else if (MODE == -1) {
+    const unsigned v0 = __ldg(raw + c), v1 = __ldg(raw + c + 1);
+    ha = v0 + v1;
+    hb = two ? v1 + __ldg(raw + c + 2) : 0u;
+  } else {
+    const unsigned vm = __ldg(raw + c - 1), v0 = __ldg(raw + c), v1 = __ldg(raw + c + 1);
+    ha = vm + 2u * v0 + v1;
+    hb = two ? v0 + 2u * v1 + __ldg(raw + c + 2) : 0u;
   }
-  const uint16_t* r0 = raw + idx - w;
-  const uint16_t* r1 = raw + idx;
-  const uint16_t* r2 = raw + idx + w;
-  const unsigned s = (unsigned)__ldg(r0 - 1) + 2u * __ldg(r0) + __ldg(r0 + 1) + 2u * __ldg(r1 - 1) + 4u * __ldg(r1) +
-                     2u * __ldg(r1 + 1) + __ldg(r2 - 1) + 2u * __ldg(r2) + __ldg(r2 + 1);
-  return s >> 4;
 }
 
+// One CTA = 256 columns x kRawRows rows.  Each thread requests the
+// horizontal sums of all mosaic rows its two columns of the strip need (the
+// strip plus the stencil's halo rows) before any arithmetic, so a thread has
+// some 40 loads in flight instead of one chain of dependent rows; each CTA
+// folds its pixels' min/max into two atomics.
 template <int MODE>
 __global__ void __launch_bounds__(kRawThreads) k_raw_demosaic(const uint16_t* __restrict__ raw, int raw_width,
                                                               int left, int top, uint16_t* __restrict__ dst,
                                                               int pitch, int dimx, int dimy, unsigned* min_max) {
   unsigned mn = 0xffffffffu, mx = 0u;
   const int x = (blockIdx.x * kRawThreads + threadIdx.x) * 2;
+  const int y0 = blockIdx.y * kRawRows;
+  const int y1 = min(dimy, y0 + kRawRows);
   if (x < dimx) {
-    for (int y = blockIdx.y; y < dimy; y += gridDim.y) {
-      const long long idx = (long long)(left + x) + (long long)raw_width * (top + y);
-      const unsigned a = raw_pixel<MODE>(raw, idx, raw_width);
-      mn = min(mn, a);
-      mx = max(mx, a);
-      uint16_t* row = dst + (size_t)y * pitch;
-      if (x + 1 < dimx) {
-        const unsigned b = raw_pixel<MODE>(raw, idx + 1, raw_width);
-        mn = min(mn, b);
-        mx = max(mx, b);
-        *reinterpret_cast<unsigned*>(row + x) = a | (b << 16);  // x even, rows 128-byte aligned
-      } else {
-        row[x] = (uint16_t)a;
+    const bool two = x + 1 < dimx;
+    const long long w = raw_width;
+    // rows of the stencil relative to the pixel's row: -1 .. 1 (-2), 0 .. 1 (-1), 0 (-20)
+    constexpr int kLo = MODE == -2 ? -1 : 0, kHi = MODE == -20 ? 0 : 1;
+    constexpr int kIn = kRawRows + kHi - kLo;  // mosaic rows the strip reads
+    const long long c = (long long)(left + x) + w * (top + y0 + kLo);  // flat index, first mosaic row
+    // every mosaic row of the strip is requested before any arithmetic
+    unsigned ha[kIn], hb[kIn];
+#pragma unroll
+    for (int r = 0; r < kIn; ++r) {
+      ha[r] = hb[r] = 0u;
+      if (y0 + r + kLo <= y1 - 1 + kHi) raw_hsum<MODE>(raw, c + w * r, two, ha[r], hb[r]);
+    }
+    uint16_t* row = dst + (size_t)y0 * pitch + x;
+#pragma unroll
+    for (int r = 0; r < kRawRows; ++r) {
+      if (y0 + r < y1) {
+        unsigned a, b;
+        if (MODE == -20) {
+          a = ha[r];
+          b = hb[r];
+        } else if (MODE == -1) {
+          a = (ha[r] + ha[r + 1]) >> 2;
+          b = (hb[r] + hb[r + 1]) >> 2;
+        } else {
+          a = (ha[r] + 2u * ha[r + 1] + ha[r + 2]) >> 4;
+          b = (hb[r] + 2u * hb[r + 1] + hb[r + 2]) >> 4;
+        }
+        mn = min(mn, a);
+        mx = max(mx, a);
+        if (two) {
+          mn = min(mn, b);
+          mx = max(mx, b);
+          *reinterpret_cast<unsigned*>(row) = a | (b << 16);  // x even, rows 128-byte aligned
+        } else {
+          *row = (uint16_t)a;
+        }
       }
+      row += pitch;
     }
   }
   mn = __reduce_min_sync(0xffffffffu, mn);
@@ -90,19 +128,30 @@ __global__ void __launch_bounds__(kRawThreads) k_raw_demosaic(const uint16_t* __
   }
 }
 
+__device__ __forceinline__ unsigned rescale1(unsigned v, unsigned mn, double fact) {
+  return (unsigned)floor((double)((int)v - (int)mn) * fact);
+}
+
+// Rescale: 8 pixels per thread (16-byte accesses; rows are 128-byte
+// aligned), the row's last dimx % 8 pixels one by one; a CTA row per frame row.
 __global__ void __launch_bounds__(kRawThreads) k_raw_rescale(uint16_t* __restrict__ dst, int pitch, int dimx,
                                                              int dimy, const unsigned* min_max) {
   const unsigned mn = min_max[0], mx = min_max[1];
   if (mx <= mn) return;  // all pixels equal: left as they are
   const double fact = 65535.0 / (double)(int)(mx - mn);
-  const int x = (blockIdx.x * kRawThreads + threadIdx.x) * 2;
+  const int x = (blockIdx.x * kRawThreads + threadIdx.x) * 8;
   if (x >= dimx) return;
   for (int y = blockIdx.y; y < dimy; y += gridDim.y) {
     uint16_t* row = dst + (size_t)y * pitch;
-    const int n = x + 1 < dimx ? 2 : 1;
-    for (int k = 0; k < n; ++k) {
-      const double v = (double)((int)row[x + k] - (int)mn) * fact;
-      row[x + k] = (uint16_t)(unsigned)floor(v);
+    if (x + 8 <= dimx) {
+      uint4 v = *reinterpret_cast<const uint4*>(row + x);
+      unsigned* u = reinterpret_cast<unsigned*>(&v);
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        u[k] = rescale1(u[k] & 0xffffu, mn, fact) | (rescale1(u[k] >> 16, mn, fact) << 16);
+      *reinterpret_cast<uint4*>(row + x) = v;
+    } else {
+      for (int k = x; k < dimx; ++k) row[k] = (uint16_t)rescale1(row[k], mn, fact);
     }
   }
 }
@@ -114,19 +163,21 @@ int raw_stencil_hi(int mode) { return mode == -20 ? 0 : 1; }
 
 void launch_raw_demosaic(const uint16_t* raw, int raw_width, int left, int top, int mode, int rescale, uint16_t* dst,
                          int pitch, int dimx, int dimy, unsigned* min_max, int num_sms, cudaStream_t s) {
+  (void)num_sms;
   cudaMemsetAsync(min_max, 0xff, sizeof(unsigned), s);
   cudaMemsetAsync(min_max + 1, 0, sizeof(unsigned), s);
-  const int gx = (dimx + 2 * kRawThreads - 1) / (2 * kRawThreads);
-  int gy = (num_sms * 16 + gx - 1) / gx;  // 16 CTAs of 128 threads per SM
-  if (gy > dimy) gy = dimy;
-  const dim3 grid(gx, gy);
+  const dim3 grid((dimx + 2 * kRawThreads - 1) / (2 * kRawThreads), (dimy + kRawRows - 1) / kRawRows);
   if (mode == -1)
     k_raw_demosaic<-1><<<grid, kRawThreads, 0, s>>>(raw, raw_width, left, top, dst, pitch, dimx, dimy, min_max);
   else if (mode == -2)
     k_raw_demosaic<-2><<<grid, kRawThreads, 0, s>>>(raw, raw_width, left, top, dst, pitch, dimx, dimy, min_max);
   else
     k_raw_demosaic<-20><<<grid, kRawThreads, 0, s>>>(raw, raw_width, left, top, dst, pitch, dimx, dimy, min_max);
-  if (rescale) k_raw_rescale<<<grid, kRawThreads, 0, s>>>(dst, pitch, dimx, dimy, min_max);
+  if (rescale) {
+    const int rx = (dimx + 8 * kRawThreads - 1) / (8 * kRawThreads);
+    const int ry = dimy < 65535 ? dimy : 65535;  // one frame row per CTA row (grid-strided beyond)
+    k_raw_rescale<<<dim3(rx, ry), kRawThreads, 0, s>>>(dst, pitch, dimx, dimy, min_max);
+  }
 }
 
 }  // namespace ptk
