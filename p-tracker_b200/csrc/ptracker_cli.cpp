@@ -494,7 +494,9 @@ int main(int argc, char** argv) {
   }
   const bool corr = s.procedure == "correction_distortion";
   if (!corr && s.procedure != "particle_tracking") die("procedure " + s.procedure + " is not part of this build");
-  if (s.raw_images) die("RAW images (libraw) are not supported: convert the frames to TIFF or PGM");
+  if (s.raw_images)
+    die("RAW camera files need libraw, which this build does not have: convert the frames to TIFF or PGM, or "
+        "pass libraw's unpacked mosaic to ptk_load_frame_raw");
   if (s.grains.empty()) die("no grains (grains_to_follow / start_file / restart_file)");
   if (corr) {
     if (s.corr_images.size() < 2) die("image_numbers_corrDisto needs the reference image and at least one more");
