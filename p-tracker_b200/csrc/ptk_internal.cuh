@@ -114,6 +114,7 @@ struct Bf16Launch {
   const size_t* wofs;       // per grain: offset of its weight slot in wslots (16-byte units)
   unsigned char* wslots;    // BF16 weights of every rotation step, per grain
   int2* topk;               // [list entry][tile][kBf16KeepMax] kept (u, v), INT_MIN when none
+  unsigned* topk_rot;       // same layout: bit r = rotation step r is rescored at that candidate
   SearchBest* rescored;     // [list entry][tile][kBf16KeepMax] exact best per kept candidate
   int* error;               // set when a bounded wait gave up
 };

@@ -207,6 +207,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
+  uint32_t v;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(v) : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  return v;
+}
+
 // rotate_pixel_pattern (src/p-tracker.cpp:615-621): FP64 without contraction,
 // round half away from zero - identical to the exact search's rotation.
 __device__ __forceinline__ short2 rotate_round_b(short2 p, double c, double s) {
@@ -378,6 +385,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   __shared__ float2 s_csf[kNRot];
   __shared__ float s_cv[kWarps * kBf16KeepMax];
   __shared__ int s_ci[kWarps * kBf16KeepMax];
+  __shared__ int s_kept[kBf16KeepMax], s_nkept;  // the tile's kept candidates (packed u, v) and their count
+  __shared__ float s_rel;
   __shared__ unsigned char s_rng[2 * kMaxFoot];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t mbar = smem_u32(&s_mbar);
@@ -753,8 +762,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
           // candidates scoring more than `rel` below the tile's best are not rescored
           const bool near = !(top > 0.0f) || key2f(mkey) >= top * (1.0f - rel);
           if (k >= keep || !near || mkey == INT_MIN) {
-            if (lane == 0)
+            if (lane == 0) {
               for (int r = k; r < kBf16KeepMax; ++r) topk[r] = make_int2(INT_MIN, INT_MIN);
+              s_nkept = k;
+              s_rel = rel;
+            }
             break;
           }
           const unsigned who = __ballot_sync(0xffffffffu, key == mkey && bi >= 0);
@@ -770,9 +782,38 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
               }
           }
           packed = __shfl_sync(0xffffffffu, packed, wl >= 0 ? wl : 0);
-          if (lane == 0)
+          if (lane == 0) {
             topk[k] = (wl >= 0 && packed >= 0) ? make_int2(u0 + (packed >> 8), v0 + (packed & 0xff))
                                                : make_int2(INT_MIN, INT_MIN);
+            s_kept[k] = (wl >= 0 && packed >= 0) ? packed : -1;
+            if (k == kBf16KeepMax - 1) {
+              s_nkept = kBf16KeepMax;
+              s_rel = rel;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      // rotation steps to rescore at each kept candidate: those whose score lies
+      // within the tile's keep margin of that candidate's best step.  A
+      // candidate's 32 rotation lanes sit in TMEM lane quadrant 3 - (u >> 3),
+      // column 8 v + (u & 7); the warp of that quadrant reads them back.
+      if (warp < 4) {
+        unsigned* rot_g = p.topk_rot + ((size_t)li * tiles + t) * kBf16KeepMax;
+        const int nk = s_nkept;
+        const float rel_t = s_rel;
+        for (int k = 0; k < nk; ++k) {
+          const int pk = s_kept[k];
+          if (pk < 0 || 3 - ((pk >> 8) >> 3) != warp) continue;
+          const int ul = pk >> 8, vl = pk & 0xff;
+          const uint32_t col = (uint32_t)(8 * vl + (ul & 7));
+          const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) + col;
+          const float d = __uint_as_float(tmem_ld1(ta)), s2 = __uint_as_float(tmem_ld1(ta + 256u));
+          const bool ok = lane < p.nrot && s2 > 0.0f;
+          const float sv = ok ? d * rsqrtf(s2) : -INFINITY;
+          const float best = key2f(__reduce_max_sync(0xffffffffu, ok ? f2key(sv) : INT_MIN));
+          const unsigned m = __ballot_sync(0xffffffffu, ok && (!(best > 0.0f) || sv >= best * (1.0f - rel_t)));
+          if (lane == 0) rot_g[k] = m;
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;");
@@ -792,17 +833,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 // ---------------------------------------------------------------------------
-// 3. Exact rescoring: every rotation step at each kept candidate of a tile,
-//    with the exact search's integer sums and NCC expression.  One block per
-//    (grain, tile); a work unit is one rotation step for two kept candidates,
-//    taken by one warp whose lanes share the pattern points; per candidate the
-//    best record over the rotation steps in the reference's order.
+// 3. Exact rescoring of the kept candidates of a tile, at the rotation steps
+//    the search marked for each (those within the keep margin of the
+//    candidate's best step), with the exact search's integer sums and NCC
+//    expression.  One block per (grain, tile); a work unit is one rotation
+//    step for two candidates that both need it (or one), taken by one warp
+//    whose lanes share the pattern points; per candidate the best record over
+//    its rotation steps in the reference's order.
 __global__ void __launch_bounds__(256, 4) k_rescore_bf16(Bf16Launch p) {
   constexpr int kW = 8;
   __shared__ double s_bn[kBf16KeepMax][kW];
   __shared__ int s_bi[kBf16KeepMax][kW];
   __shared__ int s_base[kBf16KeepMax], s_uv[kBf16KeepMax];
-  __shared__ int s_nk;
+  __shared__ int s_nk, s_nu;
+  __shared__ int s_unit[kNRot * kBf16KeepMax / 2];  // rotation | first candidate << 8 | second << 16 (255: none)
   const int item = blockIdx.x;
   const int tiles = p.tiles_u * p.tiles_v;
   const int li = item / tiles;
@@ -815,19 +859,37 @@ __global__ void __launch_bounds__(256, 4) k_rescore_bf16(Bf16Launch p) {
   const bool skip = g.masked[gi] || (g.flags[gi] & 7) || P <= 0 || P > kMaxPatternPoints;
   const int NU = p.left + p.right + 1, NV = p.up + p.down + 1;
   if (tid == 0) {  // the kept candidates, compacted: anchor pixel index and order index without the rotation
-    int nk = 0;
+    int nk = 0, nu = 0;
     if (!skip) {
       const int2* cand = p.topk + (size_t)item * kBf16KeepMax;
+      const unsigned* rots = p.topk_rot + (size_t)item * kBf16KeepMax;
       const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
+      unsigned rm[kBf16KeepMax];
       for (int k = 0; k < p.keep && k < kBf16KeepMax; ++k) {
         const int2 c = cand[k];
         if (c.x == INT_MIN) continue;
         s_base[nk] = (g.refy[gi] + gdy + c.y) * p.cur.pitch + (g.refx[gi] + gdx + c.x);
         s_uv[nk] = (c.x + p.left) * NV + (c.y + p.up);
+        rm[nk] = rots[k];
         ++nk;
+      }
+      // units: per rotation step, the candidates that need it, two at a time
+      for (int r = 0; r < p.nrot; ++r) {
+        int first = -1;
+        for (int k = 0; k < nk; ++k) {
+          if (!((rm[k] >> r) & 1u)) continue;
+          if (first < 0) {
+            first = k;
+          } else {
+            s_unit[nu++] = r | (first << 8) | (k << 16);
+            first = -1;
+          }
+        }
+        if (first >= 0) s_unit[nu++] = r | (first << 8) | (255 << 16);
       }
     }
     s_nk = nk;
+    s_nu = nu;
   }
   if (tid < kBf16KeepMax * kW) {
     s_bn[tid / kW][tid % kW] = 0.0;
@@ -843,13 +905,14 @@ __global__ void __launch_bounds__(256, 4) k_rescore_bf16(Bf16Launch p) {
   const double den1 = (double)(Pl * g.s00[gi] - S0 * S0);
   const int pitch = p.cur.pitch;
   const double base_rot = g.refrot[gi] + g.drot[gi];
-  const int npair = (nk + 1) >> 1;
-  for (int u = warp; u < p.nrot * npair; u += kW) {
-    const int r = u % p.nrot, k0 = 2 * (u / p.nrot), k1 = k0 + 1;
+  const int nu = s_nu;
+  for (int u = warp; u < nu; u += kW) {
+    const int unit = s_unit[u];
+    const int r = unit & 0xff, k0 = (unit >> 8) & 0xff, k1 = (unit >> 16) & 0xff;
     double sr, cr;
     sincos(base_rot + p.steps[r], &sr, &cr);
     const float cf = (float)cr, sf = (float)sr;
-    const bool two = k1 < nk;
+    const bool two = k1 != 255;
     const uint16_t* pa = p.cur.pix + s_base[k0];
     const uint16_t* pb = p.cur.pix + s_base[two ? k1 : k0];
     unsigned s1a = 0, s1b = 0;
