@@ -426,6 +426,22 @@ int ref_read_grains(void* p, const char* path, int ptracker_format) {
 
 int ref_num_grains(void* p) { return static_cast<Handle*>(p)->trk.num_grains; }
 
+// ptracker::check_distortion (src/check_distortion.cpp:25-100) in the current
+// directory: reads the dic files dic_name % iref and % ibeg..iend (step iinc)
+// and writes len_variation.txt.
+void ref_check_distortion(void* p, const char* dic_name, int iref, int ibeg, int iend, int iinc,
+                          const double* params14) {
+  ptracker& t = static_cast<Handle*>(p)->trk;
+  std::strncpy(t.dic_name, dic_name, sizeof(t.dic_name) - 1);
+  t.dic_name[sizeof(t.dic_name) - 1] = '\0';
+  t.iref = iref;
+  t.ibeg = ibeg;
+  t.iend = iend;
+  t.iinc = iinc;
+  t.disto_parameters.assign(params14, params14 + 14);
+  t.check_distortion();
+}
+
 // ptracker::read_raw_image (src/p-tracker.cpp:214-387) run on an unpacked
 // sensor mosaic (raw_width x raw_height, row-major) registered with the
 // libraw stub; the visible width x height frame is read back row-major into

@@ -32,6 +32,12 @@
 // corrDisto_log.txt, errors.txt, distobox.txt and, for POWELL_ITER,
 // convergence.txt as the reference does.
 //
+// `procedure check_distortion` (src/check_distortion.cpp:25-100; declared by
+// the reference but neither dispatched by its run() nor built by its
+// Makefile) reads dic_name % iref and % ibeg..iend and writes the mean length
+// drift of the segments joining grains 0-1, 2-3, ..., raw and undistorted, to
+// len_variation.txt.  It needs no GPU.
+//
 //   ptracker_b200 [command_file]     (default: commands.txt)
 //   ptracker_b200 --check file       parse only; print the settings as JSON
 #include <chrono>
@@ -471,6 +477,55 @@ void write_disto_outputs(const double* X, double index_ini, double index_end, in
   box(0.0, 0.0);
 }
 
+// check_distortion (src/check_distortion.cpp:25-100): per dic file, the
+// mean over segments (grains 2k, 2k + 1) of (L - L0) / L0, with L0 the
+// segment's length in the file of image iref, for the positions as tracked
+// and through undistor with the *_corrDistor / *_corrParallax parameters as
+// given; one line "idic mean mean_undistorted" per file.  A last grain
+// without a partner is left out (the reference reads past its grain array).
+int check_distortion(const Settings& s) {
+  const std::string pat = s.dic_name.empty() ? std::string("dic_out_%d.txt") : s.dic_name;
+  auto lengths = [&](int num, std::vector<double>& raw, std::vector<double>& und) {
+    char name[512];
+    std::snprintf(name, sizeof(name), pat.c_str(), num);
+    int n = 0;
+    if (ptk_read_grains_file(name, 1, nullptr, 0, &n)) die(std::string("cannot read ") + name);
+    std::vector<ptk_grain> g((size_t)n);
+    if (n > 0 && ptk_read_grains_file(name, 1, g.data(), n, &n)) die(std::string("cannot read ") + name);
+    raw.clear();
+    und.clear();
+    for (int k = 0; k + 1 < n; k += 2) {
+      double xb = (double)g[k].refcoord_xpix + g[k].dx, yb = (double)g[k].refcoord_ypix + g[k].dy;
+      double xe = (double)g[k + 1].refcoord_xpix + g[k + 1].dx, ye = (double)g[k + 1].refcoord_ypix + g[k + 1].dy;
+      double sx = xe - xb, sy = ye - yb;
+      raw.push_back(std::sqrt(sx * sx + sy * sy));
+      undistor_host(s.disto, (double)g[k].refcoord_xpix + g[k].dx, (double)g[k].refcoord_ypix + g[k].dy, &xb, &yb);
+      undistor_host(s.disto, (double)g[k + 1].refcoord_xpix + g[k + 1].dx,
+                    (double)g[k + 1].refcoord_ypix + g[k + 1].dy, &xe, &ye);
+      sx = xe - xb;
+      sy = ye - yb;
+      und.push_back(std::sqrt(sx * sx + sy * sy));
+    }
+  };
+  std::printf("*** PROCEDURE CHECK DISTORTION ***\n");
+  std::ofstream file("len_variation.txt");
+  std::vector<double> L0, L0u, L, Lu;
+  lengths(s.iref, L0, L0u);
+  for (int idic = s.ibeg; idic <= s.iend; idic += s.iinc) {
+    lengths(idic, L, Lu);
+    if (L.size() != L0.size()) die("dic files with different grain counts");
+    double m = 0.0, mu = 0.0;
+    for (size_t k = 0; k < L0.size(); ++k) {
+      m += (L[k] - L0[k]) / L0[k];
+      mu += (Lu[k] - L0u[k]) / L0u[k];
+    }
+    m /= (double)L0.size();
+    mu /= (double)L0.size();
+    file << idic << ' ' << m << ' ' << mu << std::endl;
+  }
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -491,6 +546,10 @@ int main(int argc, char** argv) {
   if (check) {
     print_json(s);
     return 0;
+  }
+  if (s.procedure == "check_distortion") {
+    if (s.iinc <= 0 && s.ibeg <= s.iend) die("iinc must be > 0 (the reference loops forever otherwise)");
+    return check_distortion(s);
   }
   const bool corr = s.procedure == "correction_distortion";
   if (!corr && s.procedure != "particle_tracking") die("procedure " + s.procedure + " is not part of this build");
