@@ -582,11 +582,18 @@ def run_sequence(args, rank: int, world: int, local: int) -> int:
             per.append((before[idx], rh[idx], rp[idx]))
         return {"worst": worst, "over": over, "per": per, "remapped": remapped}
 
+    try:
+        pr = torch.cuda.get_device_properties(local)
+        gpu_id = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+    except Exception:
+        gpu_id = str(local)
     with torch.cuda.stream(stream):
         head = tracker(search_method=ptk.SEARCH_BF16, subpix_method=ptk.SUBPIX_ADJOINT_LM)
         for _ in range(max(1, args.warmup // 3)):
             device_run(head)
+        sampler = ClockSampler(gpu_id if rank == 0 else None)
         ms_head = min(device_run(head) for _ in range(max(1, args.steps // 5)))
+        clocks = sampler.stop()
         head_rec = head.get_grains()
         res_counts = head.rescue_counts()
         e2e_ms, _ = host_run(head)
@@ -623,6 +630,7 @@ def run_sequence(args, rank: int, world: int, local: int) -> int:
                          "trajectory_max_abs_dev_px_vs_plain_after_sequence":
                          float(np.abs(pos(head_rec)[:, :2] - pos(plain_rec)[:, :2]).max()),
                          "rescued_last_frame": int(res_counts[0]), "jumping_grains": int(s["jumpers"].sum())},
+            "clocks": clocks,
         }
         if not args.no_cpu_baseline:
             sys.path.insert(0, str(ROOT / "oracle"))
