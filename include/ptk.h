@@ -269,8 +269,9 @@ int ptk_read_grains_file(const char* path, int format13, ptk_grain* out, int cap
 int ptk_save_grains_file(const char* path, const ptk_grain* grains, int n, const char* from_image,
                          const char* from_datetime, const char* to_image, const char* to_datetime);
 
-/* Image files (host only, no GPU).  ptk_read_image_file decodes an
- * uncompressed baseline TIFF into the grey levels that read_tiff_image
+/* Image files (host only, no GPU).  ptk_read_image_file decodes a strip
+ * TIFF (uncompressed, LZW, Deflate or PackBits, optional horizontal
+ * predictor; 8/16-bit grey or RGB) into the grey levels that read_tiff_image
  * computes through libtiff's RGBA reader (src/p-tracker.cpp:86-187): 8-bit
  * channels r, g, b scaled by 1/255, grey = (uint16)(65535 (0.299 r + 0.587 g
  * + 0.114 b)), rows top-down (16-bit grey keeps its high byte, as that reader

@@ -90,7 +90,7 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> dict:
         list(ex.map(_run, jobs))
     lib = HERE / "libptk.so"
     if jobs or _stale(lib, objs):
-        _run([nvcc, *ARCH, "-shared", "-ccbin", cxx, "-o", str(lib), *map(str, objs), "-lcudart"])
+        _run([nvcc, *ARCH, "-shared", "-ccbin", cxx, "-o", str(lib), *map(str, objs), "-lcudart", "-lz"])
     synth = HERE / "libptk_synth.so"
     s = CSRC / "synth.cpp"
     if _stale(synth, [s]):

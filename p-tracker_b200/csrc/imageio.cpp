@@ -6,18 +6,26 @@
 //     r, g, b = 8-bit channel * (1 / 255)          (double)
 //     grey    = (uint16)(65535 * (0.299 r + 0.587 g + 0.114 b))
 // with the rows restored to top-down order.  libtiff is not part of this
-// build, so an uncompressed baseline TIFF is decoded here and its samples go
-// through the same 8-bit channels the RGBA reader produces: 8-bit grey v ->
-// (v, v, v) (MinIsWhite: 255 - v), 16-bit grey -> its high byte, 16-bit
-// colour channels -> (v + 128) / 257, 8-bit RGB / RGBA as stored.  Binary
-// PGM (P5) frames are an addition of this build and are returned as stored.
+// build, so strip TIFFs are decoded here - uncompressed, LZW (compression 5,
+// as the TIFF 6.0 specification describes it: MSB-first codes of 9 to 12
+// bits, Clear 256, EndOfInformation 257, the width growing when the next code
+// to assign reaches 511 / 1023 / 2047), PackBits (32773) and Deflate (8 and
+// 32946, through zlib), with horizontal-differencing prediction (Predictor 2)
+// undone per row - and their samples go through the same 8-bit channels the
+// RGBA reader produces: 8-bit grey v -> (v, v, v) (MinIsWhite: 255 - v),
+// 16-bit grey -> its high byte, 16-bit colour channels -> (v + 128) / 257,
+// 8-bit RGB / RGBA as stored.  Binary PGM (P5) frames are an addition of this
+// build and are returned as stored.
 #include <cctype>
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <fstream>
 #include <string>
 #include <vector>
+
+#include <zlib.h>
 
 #include "../../include/ptk.h"
 
@@ -62,6 +70,97 @@ bool value(const Reader& r, const Entry& e, uint32_t k, uint32_t* v) {
   return true;
 }
 
+// TIFF LZW: decodes src into dst (at most cap bytes); *out = bytes written.
+bool lzw_decode(const unsigned char* src, size_t n, unsigned char* dst, size_t cap, size_t* out) {
+  static thread_local uint16_t prefix[4096];
+  static thread_local unsigned char suffix[4096], first[4096];
+  static thread_local uint16_t length[4096];
+  for (int c = 0; c < 256; ++c) {
+    prefix[c] = 0xffff;
+    suffix[c] = first[c] = (unsigned char)c;
+    length[c] = 1;
+  }
+  size_t bit = 0, o = 0;
+  int width = 9, next = 258, prev = -1;
+  auto read = [&](int* code) -> bool {
+    if (bit + (size_t)width > 8 * n) return false;
+    int v = 0;
+    for (int k = 0; k < width; ++k, ++bit) v = (v << 1) | ((src[bit >> 3] >> (7 - (bit & 7))) & 1);
+    *code = v;
+    return true;
+  };
+  auto emit = [&](int code) -> bool {  // the string of `code`, written back to front
+    const size_t len = length[code];
+    if (o + len > cap) return false;
+    for (size_t k = len; k-- > 0;) {
+      dst[o + k] = suffix[code];
+      code = prefix[code];
+    }
+    o += len;
+    return true;
+  };
+  int code;
+  while (read(&code)) {
+    if (code == 257) break;
+    if (code == 256) {
+      width = 9;
+      next = 258;
+      prev = -1;
+      continue;
+    }
+    if (prev < 0) {
+      if (code > 255 || !emit(code)) return false;
+      prev = code;
+      continue;
+    }
+    if (next >= 4096) return false;
+    if (code < next) {
+      if (code >= 256 && code < 258) return false;
+      if (!emit(code)) return false;
+      prefix[next] = (uint16_t)prev;
+      suffix[next] = first[code];
+    } else if (code == next) {
+      prefix[next] = (uint16_t)prev;
+      suffix[next] = first[prev];
+      first[next] = first[prev];
+      length[next] = (uint16_t)(length[prev] + 1);
+      if (!emit(next)) return false;
+    } else {
+      return false;
+    }
+    first[next] = first[prev];
+    length[next] = (uint16_t)(length[prev] + 1);
+    ++next;
+    if (next == 511) width = 10;
+    else if (next == 1023) width = 11;
+    else if (next == 2047) width = 12;
+    prev = code;
+  }
+  *out = o;
+  return true;
+}
+
+// PackBits: a header byte h, then h + 1 literal bytes (h >= 0) or one byte
+// repeated 1 - h times (-127 <= h <= -1); -128 is skipped.
+bool packbits_decode(const unsigned char* src, size_t n, unsigned char* dst, size_t cap, size_t* out) {
+  size_t i = 0, o = 0;
+  while (i < n && o < cap) {
+    const int h = (signed char)src[i++];
+    if (h >= 0) {
+      if (i + (size_t)h + 1 > n || o + (size_t)h + 1 > cap) return false;
+      std::memcpy(dst + o, src + i, (size_t)h + 1);
+      i += (size_t)h + 1;
+      o += (size_t)h + 1;
+    } else if (h != -128) {
+      if (i >= n || o + (size_t)(1 - h) > cap) return false;
+      std::memset(dst + o, src[i++], (size_t)(1 - h));
+      o += (size_t)(1 - h);
+    }
+  }
+  *out = o;
+  return true;
+}
+
 uint16_t grey_of(double R, double G, double B) {
   const double fact = 1.0 / 255.0;
   const double rr = R * fact, gg = G * fact, bb = B * fact;
@@ -97,18 +196,20 @@ int read_tiff(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, s
   };
   const uint32_t w = get(256, 0), h = get(257, 0);
   const uint32_t spp = get(277, 1), comp = get(259, 1), photo = get(262, 1), planar = get(284, 1);
-  const uint32_t orient = get(274, 1), fmt = get(339, 1);
+  const uint32_t orient = get(274, 1), fmt = get(339, 1), pred = get(317, 1);
   uint32_t bps = 8;
   if (have[258] && !value(r, ent[258], 0, &bps)) bps = 8;
   if (w == 0 || h == 0 || w > 65535 || h > 65535) return (*err = "bad TIFF image size", PTK_ERR_IO);
-  if (comp != 1) return (*err = "compressed TIFF is not supported (baseline uncompressed only)", PTK_ERR_IO);
+  if (comp != 1 && comp != 5 && comp != 8 && comp != 32946 && comp != 32773)
+    return (*err = "TIFF compression not supported (none, LZW, Deflate or PackBits)", PTK_ERR_IO);
+  if (pred != 1 && pred != 2) return (*err = "TIFF predictor not supported (none or horizontal)", PTK_ERR_IO);
   if (planar != 1 || orient != 1 || fmt != 1)
     return (*err = "TIFF layout not supported (chunky, top-left, unsigned samples only)", PTK_ERR_IO);
   if (bps != 8 && bps != 16) return (*err = "TIFF sample depth must be 8 or 16 bits", PTK_ERR_IO);
   const bool grey = photo == 0 || photo == 1;
   if (!(grey && spp >= 1) && !(photo == 2 && spp >= 3))
     return (*err = "TIFF photometric interpretation not supported (grey or RGB)", PTK_ERR_IO);
-  if (!have[273] || !have[279]) return (*err = "TIFF without strips", PTK_ERR_IO);
+  if (!have[273] || !have[279]) return (*err = "TIFF without strips (tiled TIFF is not supported)", PTK_ERR_IO);
   *dimx = (int)w;
   *dimy = (int)h;
   if (have[306]) {
@@ -121,20 +222,58 @@ int read_tiff(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, s
   }
   if (!out) return PTK_OK;
   if (capacity < (size_t)w * h) return (*err = "output buffer too small", PTK_ERR_ARG);
-  // the strips, concatenated, hold the rows top-down
+  // the strips, decoded and concatenated, hold the rows top-down
   const size_t bpp = (size_t)spp * (bps / 8), row_bytes = bpp * w;
-  std::vector<unsigned char> pix;
-  pix.reserve(row_bytes * h);
-  for (uint32_t k = 0; k < ent[273].count; ++k) {
+  uint32_t rps = get(278, h);
+  if (rps == 0 || rps > h) rps = h;
+  std::vector<unsigned char> pix(row_bytes * h);
+  size_t filled = 0;
+  for (uint32_t k = 0; k < ent[273].count && filled < pix.size(); ++k) {
     uint32_t off = 0, len = 0;
     if (!value(r, ent[273], k, &off) || !value(r, ent[279], k, &len) || !r.ok(off, len))
       return (*err = "truncated TIFF strip", PTK_ERR_IO);
-    pix.insert(pix.end(), r.d.begin() + off, r.d.begin() + off + len);
+    const size_t want = std::min(pix.size() - filled, (size_t)rps * row_bytes);
+    const unsigned char* src = r.d.data() + off;
+    unsigned char* dst = pix.data() + filled;
+    size_t got = 0;
+    bool good = true;
+    if (comp == 1) {
+      got = std::min((size_t)len, want);
+      std::memcpy(dst, src, got);
+    } else if (comp == 5) {
+      good = lzw_decode(src, len, dst, want, &got);
+    } else if (comp == 32773) {
+      good = packbits_decode(src, len, dst, want, &got);
+    } else {
+      uLongf dl = (uLongf)want;
+      const int zr = uncompress(dst, &dl, src, (uLong)len);
+      good = zr == Z_OK || zr == Z_BUF_ERROR;  // Z_BUF_ERROR: the strip holds more than the image needs
+      got = good && zr == Z_OK ? (size_t)dl : want;
+    }
+    if (!good || got < want) return (*err = "corrupt or short TIFF strip", PTK_ERR_IO);
+    filled += want;
   }
-  if (pix.size() < row_bytes * h) return (*err = "TIFF strips shorter than the image", PTK_ERR_IO);
+  if (filled < pix.size()) return (*err = "TIFF strips shorter than the image", PTK_ERR_IO);
   auto sample = [&](size_t o) -> uint32_t {
     return bps == 8 ? pix[o] : (r.le ? (uint32_t)(pix[o] | (pix[o + 1] << 8)) : (uint32_t)((pix[o] << 8) | pix[o + 1]));
   };
+  if (pred == 2) {  // horizontal differencing: each sample adds the same channel's sample to its left
+    for (uint32_t y = 0; y < h; ++y) {
+      unsigned char* row = pix.data() + (size_t)y * row_bytes;
+      for (uint32_t x = 1; x < w; ++x)
+        for (uint32_t c = 0; c < spp; ++c) {
+          const size_t o = ((size_t)x * spp + c) * (bps / 8), q = o - bpp;
+          if (bps == 8) {
+            row[o] = (unsigned char)(row[o] + row[q]);
+          } else {
+            const size_t ro = (size_t)y * row_bytes;
+            const uint32_t v = (sample(ro + o) + sample(ro + q)) & 0xffffu;
+            row[o] = (unsigned char)(r.le ? v & 0xff : v >> 8);
+            row[o + 1] = (unsigned char)(r.le ? v >> 8 : v & 0xff);
+          }
+        }
+    }
+  }
   for (uint32_t y = 0; y < h; ++y)
     for (uint32_t x = 0; x < w; ++x) {
       const size_t o = (size_t)y * row_bytes + (size_t)x * bpp;
@@ -223,7 +362,7 @@ int ptk_read_image_file(const char* path, uint16_t* out, size_t capacity, int* d
     rc = read_pgm(r, out, capacity, dimx, dimy, &err);
   } else {
     rc = PTK_ERR_IO;
-    err = "unknown image format (uncompressed TIFF or binary PGM)";
+    err = "unknown image format (TIFF or binary PGM)";
   }
   if (rc) {
     g_image_error = std::string(path) + ": " + err;

@@ -18,8 +18,9 @@
 //                                          parameters before tracking
 //
 // Frames: image_name is a printf pattern of the frame number (read_image,
-// src/p-tracker.cpp:75-83); frames are uncompressed TIFF (converted as the
-// reference's libtiff RGBA path) or binary PGM.  The next frame is decoded on
+// src/p-tracker.cpp:75-83); frames are strip TIFF (uncompressed, LZW,
+// Deflate or PackBits; converted as the reference's libtiff RGBA path) or
+// binary PGM.  The next frame is decoded on
 // a host thread while the GPU tracks the current one.  After every frame the
 // grains go to dic_out_<num>.txt in the working directory, byte for byte as
 // save_grains (src/p-tracker.cpp:1313-1367).

@@ -5,6 +5,7 @@ oracle/_ref/libptk_ref.so (oracle/Makefile, target `ref`).
 Run where the reference sources exist:
     python tests/golden/make_golden.py             (all fixtures)
     python tests/golden/make_golden.py --raw-only  (raw_demosaic.npz only)
+    python tests/golden/make_golden.py --example-only  (example_rods.npz only)
 Inputs are seeded synthetic frames (p-tracker_b200/workloads.py); every
 output stored here is what the compiled reference returned.
 """
@@ -109,10 +110,54 @@ def raw_demosaic_fixtures():
     np.savez_compressed(HERE / "raw_demosaic.npz", **out)
 
 
+# the reference's example (examples/ParticleImageTracking/commands.txt): 9 rods between TEST01 and TEST02
+EXAMPLE_ZONES = [(6, 6, 6, 6, 6, 0.0454), (30, 30, 30, 30, 69, 0.0454), (200, 200, 200, 200, 69, 0.045)]
+EXAMPLE_PARAMS = {"rescue_level": 2, "NCC_min": 0.8, "NCC_min_super": 0.7, "iraz": 20000}
+
+
+def example_fixture():
+    """The reference's shipped example: examples/ImageData/TEST01.tiff and
+    TEST02.tiff (LZW RGB) decoded with Pillow through the reference's grey
+    conversion, the 9 rods of examples/ParticleImageTracking/recentered.data
+    read by the reference's own read_grains (4-column form), tracked with that
+    example's settings (pattern circ 10; zones and thresholds above) by the
+    reference's own code from image 1 to image 1, then to image 2:
+    example_rods.npz."""
+    from PIL import Image
+    sys.path.insert(0, str(HERE.parent))
+    from imagefiles import reference_grey
+    ex = bind.REF_SRC.parent / "examples"
+    frames = []
+    for k in (1, 2):
+        a = np.asarray(Image.open(ex / "ImageData" / f"TEST{k:02d}.tiff").convert("RGB"))
+        frames.append(reference_grey(a[..., 0], a[..., 1], a[..., 2]))
+    h, w = frames[0].shape
+    t = bind.Reference(w, h, 1)
+    t.n = t._f("read_grains")(t.h, str(ex / "ParticleImageTracking" / "recentered.data").encode(), 0)
+    rec = t.get_grains()
+    t.close()
+    pair = dict(params=dict(dimx=w, dimy=h), ref=frames[0], cur=frames[0], rec=rec)
+    c = bind.setup(bind.Reference, pair, threads=4, zones=EXAMPLE_ZONES, params=EXAMPLE_PARAMS, pattern=("circ", 10))
+    c.track_frame(1)
+    g1 = c.get_grains()
+    c.load_current(frames[1])
+    c.track_frame(2)
+    g2 = c.get_grains()
+    res, sup = c.lists()
+    c.close()
+    np.savez_compressed(HERE / "example_rods.npz", frame1=frames[0], frame2=frames[1], rec=rec, grains1=g1,
+                        grains2=g2, rescued2=np.array(res, dtype=np.int32),
+                        super_rescued2=np.array(sup, dtype=np.int32))
+
+
 def main():
     if "--raw-only" in sys.argv:
         bind.build()
         raw_demosaic_fixtures()
+        return
+    if "--example-only" in sys.argv:
+        bind.build()
+        example_fixture()
         return
     assert bind.REF_SO.exists() or (bind.REF_SRC / "p-tracker.cpp").exists(), "reference sources needed"
     bind.build()
@@ -167,6 +212,7 @@ def main():
     np.savez_compressed(HERE / "rotation_steps.npz",
                         **{f"inc{inc}_num{num}": rotation_steps(inc, num) for inc, num in STEP_CASES})
     raw_demosaic_fixtures()
+    example_fixture()
     print("golden fixtures written to", HERE)
 
 

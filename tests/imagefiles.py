@@ -5,13 +5,17 @@ restated in numpy with the same double operations."""
 from __future__ import annotations
 
 import struct
+import zlib
 
 import numpy as np
 
 
 def write_tiff(path, data: np.ndarray, photometric: int | None = None, big_endian: bool = False,
-               rows_per_strip: int | None = None, compression: int = 1, datetime: str | None = None):
-    """data: (h, w) grey or (h, w, spp) colour, uint8 or uint16."""
+               rows_per_strip: int | None = None, compression: int = 1, datetime: str | None = None,
+               predictor: int | None = None):
+    """data: (h, w) grey or (h, w, spp) colour, uint8 or uint16, stored as
+    given (compression 8 deflates each strip with zlib; other values only set
+    the tag); predictor sets tag 317 (the caller stores differences)."""
     a = np.asarray(data)
     h, w = a.shape[:2]
     spp = 1 if a.ndim == 2 else a.shape[2]
@@ -23,6 +27,8 @@ def write_tiff(path, data: np.ndarray, photometric: int | None = None, big_endia
     rps = rows_per_strip or h
     row_bytes = w * spp * bps // 8
     strips = [raw[r * row_bytes:min(h, r + rps) * row_bytes] for r in range(0, h, rps)]
+    if compression == 8:
+        strips = [zlib.compress(s) for s in strips]
     header = 8
     data_off = header
     offsets = []
@@ -60,6 +66,8 @@ def write_tiff(path, data: np.ndarray, photometric: int | None = None, big_endia
     add(278, 4, [rps])
     add(279, 4, [len(s) for s in strips])
     add(284, 3, [1])
+    if predictor is not None:
+        add(317, 3, [predictor])
     if datetime is not None:
         add(306, 2, list(datetime.encode() + b"\0"))
     entries.sort()

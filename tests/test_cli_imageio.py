@@ -76,9 +76,16 @@ def test_pgm_as_stored(ptk, tmp_path, rng, dtype):
 
 def test_unsupported_and_missing_files(ptk, tmp_path, rng):
     a = rng.integers(0, 256, (8, 8), dtype=np.uint8)
+    p = tmp_path / "jpeg.tif"
+    write_tiff(p, a, compression=7)  # JPEG-in-TIFF
+    with pytest.raises(ptk.PtkError, match="compression not supported"):
+        ptk.read_image_file(str(p))
     p = tmp_path / "lzw.tif"
-    write_tiff(p, a, compression=5)
-    with pytest.raises(ptk.PtkError, match="compressed"):
+    write_tiff(p, a, compression=5)  # raw bytes under an LZW tag: not a valid code stream
+    with pytest.raises(ptk.PtkError, match="corrupt"):
+        ptk.read_image_file(str(p))
+    write_tiff(p, a, predictor=3)  # floating-point prediction
+    with pytest.raises(ptk.PtkError, match="predictor"):
         ptk.read_image_file(str(p))
     with pytest.raises(ptk.PtkError, match="cannot open"):
         ptk.read_image_file(str(tmp_path / "absent.tif"))
@@ -188,3 +195,55 @@ def test_levmar_is_refused(ptk, tmp_path):
                                            "image_numbers_corrDisto 2 0 1\noptim_algo LEVMAR\n")
     r = subprocess.run([str(ptk.cli_path()), "commands.txt"], capture_output=True, text=True, cwd=tmp_path, timeout=60)
     assert r.returncode != 0 and "LEVMAR" in r.stderr
+
+
+@pytest.mark.parametrize("compression", ["tiff_lzw", "tiff_adobe_deflate", "tiff_deflate", "packbits"])
+@pytest.mark.parametrize("kind", ["rgb", "grey8", "grey16"])
+def test_compressed_tiff_matches_reference_grey(ptk, tmp_path, compression, kind):
+    """Compressed TIFFs written by another encoder (Pillow's libtiff) decode
+    to the grey levels the reference's libtiff RGBA path gives."""
+    PIL = pytest.importorskip("PIL.Image")
+    rng = np.random.default_rng(len(compression) * 7 + len(kind))
+    h, w = 157, 211  # several strips of uneven size
+    if kind == "rgb":
+        a = rng.integers(0, 256, (h, w, 3)).astype(np.uint8)
+        a[40:90, 30:150] = (200, 120, 40)  # runs, so the dictionary and PackBits repeats get used
+        im = PIL.fromarray(a)
+        want = reference_grey(a[..., 0], a[..., 1], a[..., 2])
+    elif kind == "grey8":
+        a = rng.integers(0, 256, (h, w)).astype(np.uint8)
+        a[::3, 50:120] = 17
+        im = PIL.fromarray(a)
+        want = reference_grey(a, a, a)
+    else:
+        a = rng.integers(0, 65536, (h, w)).astype(np.uint16)
+        a[20:60] = 40000
+        im = PIL.fromarray(a)
+        hi = (a >> 8).astype(np.uint8)
+        want = reference_grey(hi, hi, hi)
+    path = tmp_path / "f.tif"
+    im.save(path, compression=compression, tiffinfo={278: 16})  # 16 rows per strip
+    got, _ = ptk.read_image_file(str(path))
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("big_endian", [False, True])
+def test_tiff_horizontal_predictor(ptk, tmp_path, big_endian):
+    """Predictor 2 (horizontal differencing) with Deflate, written here: each
+    sample stored as the difference to the same channel's left neighbour
+    (8-bit RGB and 16-bit grey, both byte orders, several strips)."""
+    rng = np.random.default_rng(4)
+    a = rng.integers(0, 256, (23, 31, 3)).astype(np.uint8)
+    d = a.copy()
+    d[:, 1:] = (a[:, 1:].astype(np.int16) - a[:, :-1].astype(np.int16)).astype(np.uint8)
+    path = tmp_path / "p.tif"
+    write_tiff(path, d, predictor=2, compression=8, rows_per_strip=5, big_endian=big_endian)
+    got, _ = ptk.read_image_file(str(path))
+    np.testing.assert_array_equal(got, reference_grey(a[..., 0], a[..., 1], a[..., 2]))
+    g = rng.integers(0, 65536, (19, 27)).astype(np.uint16)
+    dg = g.copy()
+    dg[:, 1:] = (g[:, 1:].astype(np.int32) - g[:, :-1].astype(np.int32)).astype(np.uint16)
+    write_tiff(path, dg, predictor=2, compression=8, rows_per_strip=4, big_endian=big_endian)
+    got, _ = ptk.read_image_file(str(path))
+    hi = (g >> 8).astype(np.uint8)
+    np.testing.assert_array_equal(got, reference_grey(hi, hi, hi))
