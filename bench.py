@@ -774,7 +774,7 @@ def main() -> int:
     stream = torch.cuda.Stream()
     head = dict(search_method=ptk.SEARCH_BF16, subpix_method=ptk.SUBPIX_ADJOINT_LM)
     t = ptk.Tracker(p["dimx"], p["dimy"], rescue_level=opts["rescue_level"], NCC_min=opts["NCC_min"], iraz=1 << 30,
-                    **head)
+                    autotune=1, **head)
     t.set_stream(stream.cuda_stream)
     for lvl, z in enumerate(opts["zones"]):
         if z is not None:
@@ -786,6 +786,7 @@ def main() -> int:
     t.load_frame(0, ref_pin)
     t.load_frame(1, cur_pin)
     t.snapshot_grains()
+    tune = {"headline": t.autotune()}  # search shapes timed on this pair, before any timing
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
     def barrier():
@@ -845,6 +846,8 @@ def main() -> int:
 
         # ---- the other forms on the same pair
         t.configure(search_method=ptk.SEARCH_EXACT, subpix_method=ptk.SUBPIX_POWELL)
+        t.restore_grains()
+        tune["plain"] = t.autotune()
         plain_ms, _ = time_frames(args.steps)
         plain_rec = t.get_grains()
         exact_pix = pixel_stage()
@@ -904,6 +907,7 @@ def main() -> int:
                                    f" {nsteps} rotation steps",
                        "form": "BF16 tensor-core search + exact rescoring + adjoint LM (headline)",
                        "grains_per_gpu": n, "l2": "flushed (256 MiB write) before each timed step",
+                       "autotune": tune,
                        "parallelism": f"grain shards x{world}"},
             "e2e": {"value": aggregate_rate(n, world, e2e_step), "unit": UNIT,
                     "h2d_bytes_per_step": int(frame_bytes + block), "d2h_bytes_per_step": int(block)},

@@ -99,6 +99,7 @@ typedef struct ptk_config {
   int32_t topk;                  /* BF16 search: candidates per 32x32 tile rescored exactly, those within 3 % of its best score (1..8, default 8) */
   int32_t lm_max_iter;           /* adjoint LM: iteration cap                 */
   double lm_tol;                 /* adjoint LM: step tolerance (pixels, default 1e-4) */
+  int32_t autotune;              /* 1: ptk_track_frame runs ptk_autotune once, before its first frame (default 0) */
 } ptk_config;
 
 typedef struct ptk_ctx ptk_ctx;
@@ -268,6 +269,26 @@ const char* ptk_last_error(ptk_ctx* ctx);
 int ptk_read_grains_file(const char* path, int format13, ptk_grain* out, int capacity, int* n);
 int ptk_save_grains_file(const char* path, const ptk_grain* grains, int n, const char* from_image,
                          const char* from_datetime, const char* to_image, const char* to_datetime);
+
+/* Autotuner (no reference counterpart): times the admissible shapes of the
+ * level-0 search on the loaded frame pair - the BF16 kernel's operand-row
+ * ring depth (2, 3, 4 or 6 buffers; the strip height follows from the
+ * shared-memory budget) or, in the exact form, the register-tiled against
+ * the direct kernel - with CUDA events, five runs each (the first a
+ * warm-up), each after a 256 MiB write that evicts L2 (when that much memory
+ * is free), from the same grain state (restored after every run and at the
+ * end), and keeps the fastest for this context until its search method or
+ * level-0 zone changes; the built-in shape (4 buffers, the tiled kernel)
+ * stays unless another is more than 2 % faster.  Every candidate gives the same results.  With
+ * ptk_config.autotune = 1, ptk_track_frame calls it once before building its
+ * first graph.  report (may be NULL): method 1 = BF16 (values = ring depths),
+ * 0 = exact (1 tiled, 2 direct); the candidates' best times in ms. */
+typedef struct ptk_tune_report {
+  int32_t method, choice, n;
+  int32_t values[8];
+  float ms[8];
+} ptk_tune_report;
+int ptk_autotune(ptk_ctx* ctx, ptk_tune_report* report);
 
 /* Image files (host only, no GPU).  ptk_read_image_file decodes a strip
  * TIFF (uncompressed, LZW, Deflate or PackBits, optional horizontal

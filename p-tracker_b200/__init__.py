@@ -51,7 +51,13 @@ class Config(C.Structure):
                 ("image_interpolator", C.c_int32), ("overflow_stiffness", C.c_double),
                 ("subpix_displacement_max", C.c_double), ("rotations", C.c_int32), ("zone", Zone * 3),
                 ("iraz", C.c_int32), ("subpix_method", C.c_int32), ("search_method", C.c_int32),
-                ("topk", C.c_int32), ("lm_max_iter", C.c_int32), ("lm_tol", C.c_double)]
+                ("topk", C.c_int32), ("lm_max_iter", C.c_int32), ("lm_tol", C.c_double),
+                ("autotune", C.c_int32)]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("method", C.c_int32), ("choice", C.c_int32), ("n", C.c_int32), ("values", C.c_int32 * 8),
+                ("ms", C.c_float * 8)]
 
 
 GRAIN_DTYPE = np.dtype({"names": ["refx", "refy"] + list(COLUMNS[2:]) + ["masked", "status", "pad"],
@@ -75,6 +81,7 @@ _SIGS = {
     "ptk_pattern_size": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "ptk_load_frame": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int, C.c_int, C.c_size_t]),
     "ptk_load_frame_device": (C.c_int, [_P, C.c_int, _P, C.c_size_t]),
+    "ptk_autotune": (C.c_int, [_P, C.POINTER(TuneReport)]),
     "ptk_load_frame_raw": (C.c_int, [_P, C.c_int, _P] + [C.c_int] * 6 + [_P]),
     "ptk_load_frame_raw_device": (C.c_int, [_P, C.c_int, _P] + [C.c_int] * 6 + [_P]),
     "ptk_read_frame": (C.c_int, [_P, C.c_int, _P]),
@@ -333,6 +340,15 @@ class Tracker:
 
     def search(self, level: int = 0):
         self._check(self._L.ptk_search(self.h, level), self.h)
+
+    def autotune(self) -> dict:
+        """Times the level-0 search shapes on the loaded frames and keeps the
+        fastest (ptk_autotune): {"method": "bf16"|"exact", "choice": value,
+        "candidates": {value: best ms}}."""
+        r = TuneReport()
+        self._check(self._L.ptk_autotune(self.h, C.byref(r)), self.h)
+        return {"method": "bf16" if r.method else "exact", "choice": int(r.choice),
+                "candidates": {int(r.values[k]): float(r.ms[k]) for k in range(r.n)}}
 
     def search_timed(self, level: int = 0) -> list:
         """The level's search with CUDA events between its kernels: per-kernel

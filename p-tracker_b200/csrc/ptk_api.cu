@@ -122,6 +122,11 @@ struct ptk_ctx {
   cudaGraphExec_t graph[8]{};
   bool graph_dirty{true};
 
+  // level-0 search shape chosen by ptk_autotune (0: the built-in choice)
+  int tune_ring{0};   // BF16 form: operand-row buffers of the search kernel
+  int tune_exact{0};  // exact form: 1 register-tiled kernel, 2 direct kernel
+  bool tuned{false};
+
   int iref{0};
   bool need_precompute{true};
 };
@@ -365,15 +370,16 @@ int search_geometry(ptk_ctx* c, int level, SearchGeom* sg, bool allow_bf16 = tru
   // pixel): a rotated pattern stacks at most 4 distinct offsets on one pixel,
   // so patterns whose offsets repeat more than 4 times use the direct kernel.
   const size_t tsmem = search_tiled_smem(c->max_R);
+  const int span = 2 * c->max_R + kTileU;
+  const bool direct_ok = search_smem_bytes(c->max_P, span * span) <= 227 * 1024;
   sg->tiled = c->cfg.search_method != PTK_SEARCH_EXACT_DIRECT && c->max_dup <= 4 && c->max_R <= 112 &&
-              tsmem <= 227 * 1024;
+              tsmem <= 227 * 1024 && !(level == 0 && c->tune_exact == 2 && direct_ok);
   if (sg->tiled) {
     sg->smem = tsmem;
     const int occ = search_tiled_occupancy(sg->smem, c->max_R);
     sg->grid = c->num_sms * (occ > 0 ? occ : 1);
     return PTK_OK;
   }
-  const int span = 2 * c->max_R + kTileU;
   sg->smem = search_smem_bytes(c->max_P, span * span);
   if (sg->smem > 227 * 1024) return fail(c, PTK_ERR_LIMIT, "pattern too large for the shared-memory search tile");
   const int occ = search_occupancy(sg->smem);
@@ -510,6 +516,7 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
     b.wslots = c->d_bf_wslots;
     b.topk = c->d_topk;
     b.topk_rot = c->d_topk_rot;
+    b.ring = c->tune_ring > 0 && bf16_ring_ok(c->max_R, c->tune_ring) ? c->tune_ring : kBf16RingDefault;
     b.rescored = c->d_rescored;
     b.error = c->d_counts + 3;
     launch_search_bf16(b, sg.grid, s, ev);
@@ -644,6 +651,7 @@ int ptk_config_default(ptk_config* cfg) {
   cfg->topk = 8;
   cfg->lm_max_iter = 30;
   cfg->lm_tol = 1e-4;
+  cfg->autotune = 0;
   return PTK_OK;
 }
 
@@ -733,6 +741,12 @@ int ptk_set_config(ptk_ctx* c, const ptk_config* cfg) {
   if (cfg->dimx != c->cfg.dimx || cfg->dimy != c->cfg.dimy)
     return fail(c, PTK_ERR_ARG, "frame size cannot change on a context");
   if (cfg->rescue_level < -1 || cfg->rescue_level > 2) return fail(c, PTK_ERR_ARG, "rescue_level must be -1..2");
+  const ptk_zone &z0 = cfg->zone[0], &o0 = c->cfg.zone[0];
+  if (cfg->search_method != c->cfg.search_method || z0.left != o0.left || z0.right != o0.right ||
+      z0.up != o0.up || z0.down != o0.down || z0.num_rot != o0.num_rot || z0.inc_rot != o0.inc_rot) {
+    c->tune_ring = c->tune_exact = 0;  // another form or level-0 zone is tuned afresh
+    c->tuned = false;
+  }
   c->cfg = *cfg;
   for (int l = 0; l < 3; ++l) {
     int rc = build_steps(c, l);
@@ -1083,6 +1097,96 @@ int ptk_search_timed(ptk_ctx* c, int level, float* kernel_ms, int max_kernels, i
   return PTK_OK;
 }
 
+int ptk_autotune(ptk_ctx* c, ptk_tune_report* report) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  int rc = check_ready(c, true);
+  if (rc) return rc;
+  if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
+  c->tune_ring = c->tune_exact = 0;
+  SearchGeom sg;
+  if ((rc = search_geometry(c, 0, &sg))) return rc;
+  // candidates of the level-0 search: ring depths of the BF16 kernel, or the
+  // exact kernels that can hold the patterns (every candidate gives the same
+  // results; only the time differs)
+  std::vector<int> cand;
+  const int method = sg.bf16 ? 1 : 0;
+  if (sg.bf16) {
+    for (int r : {2, 3, 4, 6})
+      if (bf16_ring_ok(c->max_R, r)) cand.push_back(r);
+  } else {
+    const int span = 2 * c->max_R + kTileU;
+    if (sg.tiled) cand.push_back(1);
+    if (search_smem_bytes(c->max_P, span * span) <= 227 * 1024) cand.push_back(2);
+  }
+  if (cand.empty()) return fail(c, PTK_ERR_STATE, "no admissible search shape");
+  BlockLayout L(c->n);
+  void* snap = nullptr;
+  void* flush = nullptr;  // written before every run: each starts with the L2 state a frame sees
+  const size_t flush_bytes = (size_t)256 << 20;
+  cudaEvent_t ev[2] = {};
+  auto cleanup = [&]() {
+    if (snap) cudaFree(snap);
+    if (flush) cudaFree(flush);
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+  };
+  if (cudaMalloc(&snap, L.total) != cudaSuccess || cudaEventCreate(&ev[0]) != cudaSuccess ||
+      cudaEventCreate(&ev[1]) != cudaSuccess) {
+    cleanup();
+    return fail(c, PTK_ERR_CUDA, "autotune scratch");
+  }
+  if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) {
+    flush = nullptr;  // no room: the runs go without the flush
+    cudaGetLastError();
+  }
+  cudaMemcpyAsync(snap, c->d_block, L.total, cudaMemcpyDeviceToDevice, c->stream);
+  std::vector<float> best((size_t)cand.size(), 1e30f);
+  cudaError_t e = cudaSuccess;
+  for (size_t k = 0; k < cand.size() && !rc && e == cudaSuccess; ++k) {
+    if (method) c->tune_ring = cand[k];
+    else c->tune_exact = cand[k];
+    SearchGeom g;
+    if ((rc = search_geometry(c, 0, &g)) || (rc = ensure_search_scratch(c, 0, g))) break;
+    for (int rep = 0; rep < 5 && !rc && e == cudaSuccess; ++rep) {  // the first run is a warm-up
+      cudaMemcpyAsync(c->d_block, snap, L.total, cudaMemcpyDeviceToDevice, c->stream);
+      if (flush) cudaMemsetAsync(flush, rep, flush_bytes, c->stream);
+      cudaEventRecord(ev[0], c->stream);
+      rc = enqueue_search(c, 0, c->stream);
+      cudaEventRecord(ev[1], c->stream);
+      e = cudaEventSynchronize(ev[1]);
+      float ms = 0.0f;
+      if (!rc && e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+      if (rep > 0 && ms < best[k]) best[k] = ms;
+    }
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_block, snap, L.total, cudaMemcpyDeviceToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cleanup();
+  c->tune_ring = c->tune_exact = 0;
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(c, e, "autotune");
+  // the built-in shape stays unless another is more than 2 % faster
+  size_t k_best = 0;
+  for (size_t k = 1; k < cand.size(); ++k)
+    if (best[k] < best[k_best]) k_best = k;
+  for (size_t k = 0; k < cand.size(); ++k)
+    if (cand[k] == (method ? kBf16RingDefault : 1) && best[k] <= 1.02f * best[k_best]) k_best = k;
+  if (method) c->tune_ring = cand[k_best];
+  else c->tune_exact = cand[k_best];
+  c->tuned = true;
+  invalidate(c);
+  if (report) {
+    report->method = method;
+    report->choice = cand[k_best];
+    report->n = (int)std::min<size_t>(cand.size(), 8);
+    for (int k = 0; k < report->n; ++k) {
+      report->values[k] = cand[(size_t)k];
+      report->ms[k] = best[(size_t)k];
+    }
+  }
+  return PTK_OK;
+}
+
 int ptk_subpixel(ptk_ctx* c, int method) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
   int rc = check_ready(c, true);
@@ -1127,6 +1231,7 @@ int ptk_track_frame(ptk_ctx* c, int num_image) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
   int rc = check_ready(c, true);
   if (rc) return rc;
+  if (c->cfg.autotune && !c->tuned && (rc = ptk_autotune(c, nullptr))) return rc;
   if ((rc = prepare_searches(c))) return rc;
   if (c->graph_dirty) drop_graphs(c);
   const bool pre = c->need_precompute;

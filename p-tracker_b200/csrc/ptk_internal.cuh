@@ -115,6 +115,7 @@ struct Bf16Launch {
   unsigned char* wslots;    // BF16 weights of every rotation step, per grain
   int2* topk;               // [list entry][tile][kBf16KeepMax] kept (u, v), INT_MIN when none
   unsigned* topk_rot;       // same layout: bit r = rotation step r is rescored at that candidate
+  int ring;                 // operand-row buffers of the search kernel's ring (2..8; the strips take the rest)
   SearchBest* rescored;     // [list entry][tile][kBf16KeepMax] exact best per kept candidate
   int* error;               // set when a bounded wait gave up
 };
@@ -148,6 +149,8 @@ int search_tiled_occupancy(size_t smem, int max_r);
 void launch_search_tiled(const SearchLaunch& p, int max_r, int grid, size_t smem, cudaStream_t s);
 void launch_finalize(const FinalizeLaunch& p, int n_grains, cudaStream_t s);
 bool bf16_supported(int max_r, int nrot, int max_dup);
+bool bf16_ring_ok(int max_half, int ring);
+constexpr int kBf16RingDefault = 4;
 size_t bf16_weight_entries(int half);
 void prepare_search_bf16();
 // ev (optional, 5 events): recorded before the first kernel and after each of the four

@@ -120,7 +120,7 @@ struct Geom {
   int nb;    // operand-row ring buffers
 };
 
-__host__ __device__ inline Geom geom_of(int half) {
+__host__ __device__ inline Geom geom_of(int half, int nb = kRingUsed) {
   Geom g;
   g.half = half;
   g.fw = 2 * half + 1;
@@ -132,7 +132,6 @@ __host__ __device__ inline Geom geom_of(int half) {
   // the operand-row ring, then two Hankel buffers and the staged image rows
   // with 31 rows of halo
   const int halo_row = 2 * g.hb * 128 + g.rp;
-  const int nb = kRingUsed;
   int rs = (kSmemBudget - nb * 2 * g.wb * 512) / halo_row - 31;
   if (rs > g.fw) rs = g.fw;
   g.rs = rs < 1 ? 1 : rs;
@@ -370,6 +369,9 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
 // ---------------------------------------------------------------------------
 // 2. Tensor-core cross terms and second moments, and the kept candidates of
 //    every tile.
+// RING: operand-row buffers (a compile-time constant, so the ring indexing
+// of the MMA-issuing thread folds; launched for 2, 3, 4 and 6).
+template <int RING>
 __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   extern __shared__ __align__(128) unsigned char smem_bf[];
   unsigned char* smem = smem_bf;
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
       s_cs[tid] = make_double2(cr, sr);
       s_csf[tid] = make_float2((float)cr, (float)sr);
     }
-    const Geom G = geom_of(p.half[gi]);
+    const Geom G = geom_of(p.half[gi], RING);
     const float mean0 = (float)g.mean0[gi];
     const float c00_rsqrt = g.c0c0[gi] > 0.0 ? (float)(1.0 / sqrt(g.c0c0[gi])) : 0.0f;
     const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
@@ -983,10 +985,22 @@ bool bf16_supported(int max_r, int nrot, int max_dup) {
   return 2 * max_r + 1 < kMaxFoot && nrot >= 1 && nrot <= kNRot && 4 * max_dup <= 255;
 }
 
+// A ring of `ring` operand-row buffers leaves strips of at least one row for
+// every footprint up to half-extent max_half within the shared-memory budget.
+bool bf16_ring_ok(int max_half, int ring) {
+  if (ring != 2 && ring != 3 && ring != 4 && ring != 6) return false;  // the instantiated kernels
+  const Geom G = geom_of(max_half, ring);
+  const int halo_row = 2 * G.hb * 128 + G.rp;
+  return (kSmemBudget - ring * 2 * G.wb * 512) / halo_row - 31 >= 1;
+}
+
 void prepare_search_bf16() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_search_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget);
+  cudaFuncSetAttribute(k_search_bf16<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget);
+  cudaFuncSetAttribute(k_search_bf16<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget);
+  cudaFuncSetAttribute(k_search_bf16<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget);
+  cudaFuncSetAttribute(k_search_bf16<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget);
   cudaFuncSetAttribute(k_weights_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, kWSmem);
   done = true;
 }
@@ -996,7 +1010,12 @@ void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent
   if (ev) cudaEventRecord(ev[0], s);
   k_weights_bf16<<<p.max_items / (p.tiles_u * p.tiles_v), kWThreads, kWSmem, s>>>(p);
   if (ev) cudaEventRecord(ev[1], s);
-  k_search_bf16<<<grid, kThreads, kSmemBudget, s>>>(p);
+  switch (p.ring) {
+    case 2: k_search_bf16<2><<<grid, kThreads, kSmemBudget, s>>>(p); break;
+    case 3: k_search_bf16<3><<<grid, kThreads, kSmemBudget, s>>>(p); break;
+    case 6: k_search_bf16<6><<<grid, kThreads, kSmemBudget, s>>>(p); break;
+    default: k_search_bf16<4><<<grid, kThreads, kSmemBudget, s>>>(p); break;
+  }
   if (ev) cudaEventRecord(ev[2], s);
   k_rescore_bf16<<<items, 256, 0, s>>>(p);
   if (ev) cudaEventRecord(ev[3], s);

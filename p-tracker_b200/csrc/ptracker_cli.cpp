@@ -13,6 +13,8 @@
 //     search_method  exact | bf16          integer search (default exact)
 //     subpix_method  powell | adjoint_lm   subpixel refinement (default powell)
 //     topk K, lm_max_iter N, lm_tol T      their parameters
+//     autotune 0 | 1                       time the level-0 search shapes
+//                                          before the first frame (ptk_autotune)
 //     undistort_images 0 | 1               resample every frame with the
 //                                          *_corrDistor / *_corrParallax
 //                                          parameters before tracking
@@ -314,6 +316,8 @@ Settings read_commands(const char* path) {
       in >> s.cfg.lm_max_iter;
     } else if (tok == "lm_tol") {
       in >> s.cfg.lm_tol;
+    } else if (tok == "autotune") {
+      in >> s.cfg.autotune;
     } else if (tok == "undistort_images") {
       in >> s.undistort;
     } else {
@@ -371,7 +375,8 @@ void print_json(const Settings& s) {
   for (size_t i = 0; i < s.patterns.size(); ++i)
     o << (i ? ", " : "") << "[" << s.patterns[i].kind << ", " << s.patterns[i].a << ", " << s.patterns[i].b << ", "
       << s.patterns[i].target << ", \"" << s.patterns[i].file << "\"]";
-  o << "], \"search_method\": " << c.search_method << ", \"subpix_method\": " << c.subpix_method
+  o << "], \"search_method\": " << c.search_method << ", \"autotune\": " << c.autotune
+    << ", \"subpix_method\": " << c.subpix_method
     << ", \"undistort_images\": " << s.undistort << ", \"disto\": [";
   for (int k = 0; k < 14; ++k) o << (k ? ", " : "") << s.disto[k];
   o << "], \"disto_perturb\": [";
