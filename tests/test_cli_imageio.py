@@ -125,7 +125,7 @@ pattern circ 7
 mask_rect 0 150 0 250
 use_neighbour_list 1 neighbour_dist_pix 100 wanted_num_threads 16
 K1_corrDistor -2e-9 xc_corrDistor 2808 dK1_corrDistor 1e-10
-search_method bf16 subpix_method adjoint_lm undistort_images 1
+search_method bf16 subpix_method adjoint_lm undistort_images 1 autotune 1
 no_such_token
 """)
     cfg, out, err = _check(ptk, tmp_path / "commands.txt", tmp_path)
@@ -142,6 +142,7 @@ no_such_token
     assert cfg["patterns"] == [[3, 0.9, 5, 30, ""], [0, 7, 0, -1, ""]]
     assert cfg["disto"][0] == 2808 and cfg["disto"][2] == -2e-9
     assert cfg["search_method"] == 1 and cfg["subpix_method"] == 1 and cfg["undistort_images"] == 1
+    assert cfg["autotune"] == 1
     assert cfg["unknown_tokens"] == 1 and "Unknown token: no_such_token" in out
 
 
