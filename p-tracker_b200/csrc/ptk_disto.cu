@@ -14,9 +14,10 @@
 // residual; here every (image, grain) point is undistorted once (a per-point
 // kernel, images x grains undistor calls instead of 4 x images x pairs) and
 // the residual kernel gathers the four positions of each pair, which stay in
-// L2.  Both run in FP64 (this file is compiled with -fmad=false, so each
-// residual is the CPU's value bit for bit) and the sum is reduced in a fixed
-// order over a fixed grid, so it is reproducible.  The minimiser runs on the host and calls the
+// L2, and adds the squares up (its last block to finish sums the blocks'
+// partial sums).  Both run in FP64 (this file is compiled with -fmad=false, so
+// each residual is the CPU's value bit for bit) and the sum is reduced in a
+// fixed order over a fixed grid, so it is reproducible.  The minimiser runs on the host and calls the
 // kernel for every objective value: POWELL (one minimisation, ftol 1e-12,
 // initial directions the perturbations) and POWELL_ITER (num_iter
 // minimisations, each followed by re-anchoring A1/B1 and the displacements on
@@ -41,6 +42,7 @@ struct ptk_disto {
   double *d_dx{nullptr}, *d_dy{nullptr}, *d_dx0{nullptr}, *d_dy0{nullptr}, *d_ncc{nullptr};
   double *d_origx{nullptr}, *d_origy{nullptr};
   double *d_partial{nullptr}, *d_sum{nullptr}, *d_fvec{nullptr};
+  unsigned* d_done{nullptr};  // blocks of the residual kernel finished (the last one sums and resets it)
   double2* d_pos{nullptr};  // undistorted points: slot 0 A1 (reference), slot 1 + im the tracked ones
   cudaStream_t stream{nullptr};
   std::string err;
@@ -86,33 +88,38 @@ __global__ void __launch_bounds__(kDThreads) k_disto_points(DistoData d, Disto X
   pos[k] = make_double2(x, y);
 }
 
-// One residual per (image, pair) from the undistorted points;
-// partial[block] = the block's sum of err^2.
+// One residual per (image, pair) from the undistorted points, images
+// outermost (no 64-bit division per residual); partial[block] = the block's
+// sum of err^2, and the block that finishes last adds the partial sums in
+// block order into *out (the same order whichever block is last).
 __global__ void __launch_bounds__(kDThreads) k_disto_residuals(DistoData d, const double2* __restrict__ pos,
-                                                               double* fvec, double* partial) {
+                                                               double* fvec, double* partial, unsigned* done,
+                                                               double* out) {
   __shared__ double red[kDThreads / 32];
+  __shared__ bool s_last;
   double acc = 0.0;
-  const long long m = (long long)d.nimg1 * d.npairs;
-  for (long long r = (long long)blockIdx.x * kDThreads + threadIdx.x; r < m; r += (long long)gridDim.x * kDThreads) {
-    const int im = (int)(r / d.npairs);
-    const long long il = r - (long long)im * d.npairs;
-    const int2 pr = d.pairs[il];
-    const int i = pr.x, j = pr.y;
-    const size_t oi = (size_t)im * d.n + i, oj = (size_t)im * d.n + j;
-    double e = 0.0;
-    if (!(d.ncc[oi] < d.NCC_min || d.ncc[oj] < d.NCC_min)) {
-      const double2 A1 = pos[i], B1 = pos[j];
-      const double2 A2 = pos[(size_t)d.n + oi], B2 = pos[(size_t)d.n + oj];
-      double ABx = B1.x - A1.x, ABy = B1.y - A1.y;
-      const double AB = sqrt(ABx * ABx + ABy * ABy);
-      ABx /= AB;
-      ABy /= AB;
-      const double BBx = B2.x - B1.x, BBy = B2.y - B1.y;
-      const double AAx = A2.x - A1.x, AAy = A2.y - A1.y;
-      e = (ABx * (BBx - AAx)) + (ABy * (BBy - AAy));
-      acc += e * e;
+  const long long stride = (long long)gridDim.x * kDThreads;
+  for (int im = 0; im < d.nimg1; ++im) {
+    const size_t io = (size_t)im * d.n;
+    const double2* pimg = pos + (size_t)d.n + io;
+    for (long long il = (long long)blockIdx.x * kDThreads + threadIdx.x; il < d.npairs; il += stride) {
+      const int2 pr = d.pairs[il];
+      const int i = pr.x, j = pr.y;
+      double e = 0.0;
+      if (!(d.ncc[io + i] < d.NCC_min || d.ncc[io + j] < d.NCC_min)) {
+        const double2 A1 = pos[i], B1 = pos[j];
+        const double2 A2 = pimg[i], B2 = pimg[j];
+        double ABx = B1.x - A1.x, ABy = B1.y - A1.y;
+        const double AB = sqrt(ABx * ABx + ABy * ABy);
+        ABx /= AB;
+        ABy /= AB;
+        const double BBx = B2.x - B1.x, BBy = B2.y - B1.y;
+        const double AAx = A2.x - A1.x, AAy = A2.y - A1.y;
+        e = (ABx * (BBx - AAx)) + (ABy * (BBy - AAy));
+        acc += e * e;
+      }
+      if (fvec) fvec[(size_t)im * d.npairs + il] = e;
     }
-    if (fvec) fvec[r] = e;
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
@@ -121,21 +128,22 @@ __global__ void __launch_bounds__(kDThreads) k_disto_residuals(DistoData d, cons
     double s = 0.0;
     for (int w = 0; w < kDThreads / 32; ++w) s += red[w];
     partial[blockIdx.x] = s;
+    __threadfence();
+    s_last = atomicAdd(done, 1u) == gridDim.x - 1;
   }
-}
-
-// out = the sum of the blocks' partial sums, in a fixed order.
-__global__ void __launch_bounds__(kDThreads) k_disto_sum(const double* partial, int nb, double* out) {
-  __shared__ double red[kDThreads / 32];
-  double acc = 0.0;
-  for (int k = threadIdx.x; k < nb; k += kDThreads) acc += partial[k];
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double a2 = 0.0;
+  for (int k = threadIdx.x; k < (int)gridDim.x; k += kDThreads) a2 += __ldcg(partial + k);
+  for (int o = 16; o > 0; o >>= 1) a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a2;
   __syncthreads();
   if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < kDThreads / 32; ++w) s += red[w];
-    *out = s;
+    double t = 0.0;
+    for (int w = 0; w < kDThreads / 32; ++w) t += red[w];
+    *out = t;
+    *done = 0u;  // ready for the next evaluation
   }
 }
 
@@ -343,8 +351,7 @@ int disto_eval(ptk_disto* d, const double* X14, int use_orig, double* value, dou
   const DistoData dd = data_of(d, use_orig);
   const long long npts = (long long)(d->nimg1 + 1) * d->n;
   if (npts > 0) k_disto_points<<<(unsigned)((npts + kDThreads - 1) / kDThreads), kDThreads, 0, d->stream>>>(dd, X, d->d_pos);
-  k_disto_residuals<<<kDBlocks, kDThreads, 0, d->stream>>>(dd, d->d_pos, fv, d->d_partial);
-  k_disto_sum<<<1, kDThreads, 0, d->stream>>>(d->d_partial, kDBlocks, d->d_sum);
+  k_disto_residuals<<<kDBlocks, kDThreads, 0, d->stream>>>(dd, d->d_pos, fv, d->d_partial, d->d_done, d->d_sum);
   cudaError_t e = cudaMemcpyAsync(value, d->d_sum, sizeof(double), cudaMemcpyDeviceToHost, d->stream);
   if (e == cudaSuccess && fv) e = cudaMemcpyAsync(fvec_host, fv, sizeof(double) * m, cudaMemcpyDeviceToHost, d->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
@@ -415,6 +422,7 @@ int ptk_disto_create(ptk_disto** out, int dimx, int dimy, const int32_t* refx, c
   alloc((void**)&d->d_origy, sizeof(double) * n);
   alloc((void**)&d->d_partial, sizeof(double) * kDBlocks);
   alloc((void**)&d->d_sum, sizeof(double));
+  alloc((void**)&d->d_done, sizeof(unsigned));
   alloc((void**)&d->d_pos, sizeof(double2) * (size_t)(n_tracked + 1) * n);
   if (ok) {
     std::vector<double> ox(n), oy(n);
@@ -432,7 +440,8 @@ int ptk_disto_create(ptk_disto** out, int dimx, int dimy, const int32_t* refx, c
          cudaMemcpy(d->d_dy0, dy, sizeof(double) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(d->d_ncc, ncc_subpix, sizeof(double) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(d->d_origx, ox.data(), sizeof(double) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(d->d_origy, oy.data(), sizeof(double) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+         cudaMemcpy(d->d_origy, oy.data(), sizeof(double) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(d->d_done, 0, sizeof(unsigned)) == cudaSuccess;
   }
   if (!ok) {
     ptk_disto_destroy(d);
@@ -456,6 +465,7 @@ int ptk_disto_destroy(ptk_disto* d) {
   cudaFree(d->d_origy);
   cudaFree(d->d_partial);
   cudaFree(d->d_sum);
+  cudaFree(d->d_done);
   cudaFree(d->d_fvec);
   cudaFree(d->d_pos);
   if (d->stream) cudaStreamDestroy(d->stream);
@@ -534,8 +544,8 @@ int ptk_disto_objective_timed(ptk_disto* d, const double* params14, int reps, do
   cudaEventRecord(ev[0], d->stream);
   for (int k = 0; k < reps; ++k) {
     k_disto_points<<<(unsigned)((npts + kDThreads - 1) / kDThreads), kDThreads, 0, d->stream>>>(dd, X, d->d_pos);
-    k_disto_residuals<<<kDBlocks, kDThreads, 0, d->stream>>>(dd, d->d_pos, nullptr, d->d_partial);
-    k_disto_sum<<<1, kDThreads, 0, d->stream>>>(d->d_partial, kDBlocks, d->d_sum);
+    k_disto_residuals<<<kDBlocks, kDThreads, 0, d->stream>>>(dd, d->d_pos, nullptr, d->d_partial, d->d_done,
+                                                             d->d_sum);
   }
   cudaEventRecord(ev[1], d->stream);
   cudaError_t e = cudaEventSynchronize(ev[1]);
