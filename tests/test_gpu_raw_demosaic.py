@@ -60,3 +60,27 @@ def test_rejections(ptk, cuda_device):
         t.load_frame_raw(0, raw, 0, 0, 0)
     assert t.load_frame_raw(0, raw, 0, 0, ptk.DEMOSAIC_GREY) == (0, 0)
     t.close()
+
+
+@pytest.mark.parametrize("mode", [-1, -2, -20])
+@pytest.mark.parametrize("geom", [((64, 96), (87, 60), 8, 1), ((40, 1040), (1031, 37), 8, 2),
+                                  ((33, 2072), (2057, 30), 16, 1)])
+def test_aligned_mosaics_vector_path(ptk, oracle, cuda_device, mode, geom):
+    """Mosaics whose rows start 16-byte aligned (left margin and raw width
+    multiples of 8) take the 8-column kernel: frames whose width is not a
+    multiple of 8, that span several CTAs, and whose last column reaches the
+    mosaic's last one, against the oracle, host and device mosaics."""
+    import torch
+    (rh, rw), (w, h), left, top = geom
+    rng = np.random.default_rng(rw + mode)
+    raw = rng.integers(0, 65536, (rh, rw)).astype(np.uint16)
+    raw[::5] //= 7
+    want = oracle.raw_demosaic(raw, w, h, left, top, mode, True)
+    assert want is not None
+    t = ptk.Tracker(w, h)
+    assert t.load_frame_raw(0, raw, left, top, mode, True) == want[1]
+    np.testing.assert_array_equal(t.read_frame(0), want[0])
+    d = torch.from_numpy(raw.view(np.int16)).cuda()
+    t.load_frame_raw_device(1, d.data_ptr(), rw, rh, left, top, mode, False)
+    np.testing.assert_array_equal(t.read_frame(1), oracle.raw_demosaic(raw, w, h, left, top, mode, False)[0])
+    t.close()
