@@ -50,6 +50,13 @@ struct ptk_ctx {
   cudaStream_t stream{nullptr};
   cudaStream_t own_stream{nullptr};
   cudaStream_t cap_stream{nullptr};
+  // Host uploads of the current frame go to copy_stream, after the work
+  // already on the context stream (main_mark), and record cur_ready; the
+  // frame's graph waits for cur_ready just before its first kernel that reads
+  // the current frame, every other reader at its entry (sync_cur).
+  cudaStream_t copy_stream{nullptr};
+  cudaEvent_t cur_ready{nullptr}, main_mark{nullptr};
+  bool cur_pending{false};
   std::string err;
   int64_t launches{0};
 
@@ -159,6 +166,15 @@ void drop_graphs(ptk_ctx* c) {
 }
 
 void invalidate(ptk_ctx* c) { c->graph_dirty = true; }
+
+// The context stream waits for a current-frame upload still in flight on the
+// copy stream (entry of every call that reads the current frame or reuses
+// its staging outside a frame's graph).
+void sync_cur(ptk_ctx* c) {
+  if (!c->cur_pending) return;
+  cudaStreamWaitEvent(c->stream, c->cur_ready, 0);
+  c->cur_pending = false;
+}
 
 FrameDev frame(const ptk_ctx* c, int phys) {
   return FrameDev{c->d_img[phys], c->pitch, c->cfg.dimx, c->cfg.dimy};
@@ -467,7 +483,10 @@ int ensure_search_scratch(ptk_ctx* c, int level, const SearchGeom& sg) {
 // grains the BF16 pass rejected.
 int level_launches(const SearchGeom& sg) { return sg.bf16 ? 6 : 2; }
 
-int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = nullptr) {
+// frame_ready: inside a frame's graph, the event of the current frame's
+// upload, waited for just before the first kernel that reads that frame.
+int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = nullptr,
+                   cudaEvent_t frame_ready = nullptr) {
   SearchGeom sg;
   int rc = search_geometry(c, level, &sg);
   if (rc) return rc;
@@ -519,7 +538,8 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
     b.ring = c->tune_ring > 0 && bf16_ring_ok(c->max_R, c->tune_ring) ? c->tune_ring : kBf16RingDefault;
     b.rescored = c->d_rescored;
     b.error = c->d_counts + 3;
-    launch_search_bf16(b, sg.grid, s, ev);
+    launch_search_bf16(b, sg.grid, s, ev, frame_ready);
+    frame_ready = nullptr;
     // The ranking finds the exact best wherever it is a match; a grain the
     // level rejects (best below the threshold, among candidates that all
     // match poorly) is searched again exactly, so that its recorded NCC and
@@ -551,6 +571,7 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
   p.tiles_v = sx.tiles_v;
   p.best = c->d_best;
   p.max_items = (int)c->best_cap;
+  if (frame_ready) cudaStreamWaitEvent(s, frame_ready, cudaEventWaitExternal);
   if (ev && !sg.bf16) cudaEventRecord(ev[0], s);
   if (sx.tiled) launch_search_tiled(p, c->max_R, sx.grid, sx.smem, s);
   else launch_search(p, sx.grid, sx.smem, s);
@@ -614,7 +635,8 @@ int prepare_searches(ptk_ctx* c) {
 int enqueue_frame(ptk_ctx* c, bool precompute, bool swap, cudaStream_t s) {
   int rc;
   if (precompute && (rc = enqueue_precompute(c, s))) return rc;
-  if (c->cfg.rescue_level >= 0 && (rc = enqueue_search(c, 0, s))) return rc;
+  if (c->cfg.rescue_level >= 0 && (rc = enqueue_search(c, 0, s, nullptr, c->cur_ready))) return rc;
+  if (c->cfg.rescue_level < 0) cudaStreamWaitEvent(s, c->cur_ready, cudaEventWaitExternal);
   if (c->cfg.rescue_level >= 1 && (rc = enqueue_search(c, 1, s))) return rc;
   if (c->cfg.rescue_level >= 2 && (rc = enqueue_search(c, 2, s))) return rc;
   if (c->cfg.subpixel && (rc = enqueue_subpixel(c, c->cfg.subpix_method, s))) return rc;
@@ -674,6 +696,11 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
   e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
+  e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
+  e = cudaEventCreateWithFlags(&c->cur_ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->main_mark, cudaEventDisableTiming);
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaEventCreate"));
   c->stream = c->own_stream;
   c->pitch = (cfg->dimx + 63) & ~63;
   const size_t bytes = (size_t)c->pitch * cfg->dimy * sizeof(uint16_t);
@@ -700,6 +727,7 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
 int ptk_destroy(ptk_ctx* c) {
   if (!c) return PTK_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   drop_graphs(c);
   cudaFree(c->d_img[0]);
   cudaFree(c->d_img[1]);
@@ -732,6 +760,9 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_gr);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->cur_ready) cudaEventDestroy(c->cur_ready);
+  if (c->main_mark) cudaEventDestroy(c->main_mark);
   delete c;
   return PTK_OK;
 }
@@ -951,15 +982,28 @@ int ptk_load_frame(ptk_ctx* c, int slot, const void* pix, int dimx, int dimy, in
   if (bpp != 1 && bpp != 2) return fail(c, PTK_ERR_ARG, "bytes_per_px must be 1 or 2");
   if (pitch_bytes < (size_t)dimx * bpp) return fail(c, PTK_ERR_ARG, "pitch smaller than a row");
   const int phys = slot == 0 ? c->ref_slot : c->cur_slot;
+  sync_cur(c);  // a previous current-frame upload (and its 8-bit staging) is done first
+  if (!c->d_u8 && bpp == 1) CK(cudaMalloc(&c->d_u8, (size_t)c->pitch * dimy));
+  // the current frame goes up on the copy stream, after the work queued so far
+  // (which may still read that slot); the reference frame on the context stream
+  cudaStream_t cs = c->stream;
+  if (slot == 1) {
+    CK(cudaEventRecord(c->main_mark, c->stream));
+    CK(cudaStreamWaitEvent(c->copy_stream, c->main_mark, 0));
+    cs = c->copy_stream;
+  }
   if (bpp == 2) {
     CK(cudaMemcpy2DAsync(c->d_img[phys], (size_t)c->pitch * 2, pix, pitch_bytes, (size_t)dimx * 2, dimy,
-                         cudaMemcpyHostToDevice, c->stream));
+                         cudaMemcpyHostToDevice, cs));
   } else {
-    if (!c->d_u8) CK(cudaMalloc(&c->d_u8, (size_t)c->pitch * dimy));
     CK(cudaMemcpy2DAsync(c->d_u8, (size_t)c->pitch, pix, pitch_bytes, (size_t)dimx, dimy, cudaMemcpyHostToDevice,
-                         c->stream));
-    launch_widen_u8(c->d_u8, (size_t)c->pitch, c->d_img[phys], c->pitch, dimx, dimy, c->stream);
+                         cs));
+    launch_widen_u8(c->d_u8, (size_t)c->pitch, c->d_img[phys], c->pitch, dimx, dimy, cs);
     c->launches += 1;
+  }
+  if (slot == 1) {
+    CK(cudaEventRecord(c->cur_ready, cs));
+    c->cur_pending = true;
   }
   c->loaded[slot] = true;
   if (slot == 0) c->need_precompute = true;
@@ -969,6 +1013,7 @@ int ptk_load_frame(ptk_ctx* c, int slot, const void* pix, int dimx, int dimy, in
 int ptk_load_frame_device(ptk_ctx* c, int slot, const void* dev_pix, size_t pitch_bytes) {
   if (!c || !dev_pix || slot < 0 || slot > 1) return fail(c, PTK_ERR_ARG, "bad frame arguments");
   if (pitch_bytes < (size_t)c->cfg.dimx * 2) return fail(c, PTK_ERR_ARG, "pitch smaller than a row");
+  sync_cur(c);
   const int phys = slot == 0 ? c->ref_slot : c->cur_slot;
   CK(cudaMemcpy2DAsync(c->d_img[phys], (size_t)c->pitch * 2, dev_pix, pitch_bytes, (size_t)c->cfg.dimx * 2,
                        c->cfg.dimy, cudaMemcpyDeviceToDevice, c->stream));
@@ -991,6 +1036,7 @@ static int load_frame_raw(ptk_ctx* c, int slot, const uint16_t* raw, bool raw_on
   if (first < 0 || last >= n)
     return fail(c, PTK_ERR_ARG, "the demosaic stencil reaches outside the raw mosaic (check margins and sizes)");
   if (!c->d_minmax) CK(cudaMalloc(&c->d_minmax, 2 * sizeof(unsigned)));
+  sync_cur(c);
   const uint16_t* src = raw;
   if (!raw_on_device) {
     if ((size_t)n > c->raw_cap) {
@@ -1033,6 +1079,7 @@ int ptk_load_frame_raw_device(ptk_ctx* c, int slot, const uint16_t* dev_raw, int
 
 int ptk_read_frame(ptk_ctx* c, int slot, uint16_t* out) {
   if (!c || !out || slot < 0 || slot > 1) return fail(c, PTK_ERR_ARG, "bad arguments");
+  sync_cur(c);
   const int phys = slot == 0 ? c->ref_slot : c->cur_slot;
   CK(cudaMemcpy2DAsync(out, (size_t)c->cfg.dimx * 2, c->d_img[phys], (size_t)c->pitch * 2, (size_t)c->cfg.dimx * 2,
                        c->cfg.dimy, cudaMemcpyDeviceToHost, c->stream));
@@ -1056,6 +1103,7 @@ int ptk_search(ptk_ctx* c, int level) {
   if (!c || level < 0 || level > 2) return fail(c, PTK_ERR_ARG, "bad search level");
   int rc = check_ready(c, true);
   if (rc) return rc;
+  sync_cur(c);
   if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
   SearchGeom sg;
   if ((rc = search_geometry(c, level, &sg))) return rc;
@@ -1070,6 +1118,7 @@ int ptk_search_timed(ptk_ctx* c, int level, float* kernel_ms, int max_kernels, i
     return fail(c, PTK_ERR_ARG, "bad argument");
   int rc = check_ready(c, true);
   if (rc) return rc;
+  sync_cur(c);
   if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
   SearchGeom sg;
   if ((rc = search_geometry(c, level, &sg))) return rc;
@@ -1101,6 +1150,7 @@ int ptk_autotune(ptk_ctx* c, ptk_tune_report* report) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
   int rc = check_ready(c, true);
   if (rc) return rc;
+  sync_cur(c);
   if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
   c->tune_ring = c->tune_exact = 0;
   SearchGeom sg;
@@ -1191,6 +1241,7 @@ int ptk_subpixel(ptk_ctx* c, int method) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
   int rc = check_ready(c, true);
   if (rc) return rc;
+  sync_cur(c);
   if (c->need_precompute && (rc = ptk_precompute(c))) return rc;
   if ((rc = enqueue_subpixel(c, method, c->stream))) return rc;
   CK(cudaGetLastError());
@@ -1200,6 +1251,7 @@ int ptk_subpixel(ptk_ctx* c, int method) {
 int ptk_end_frame(ptk_ctx* c, int num_image) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
   if (c->n <= 0) return fail(c, PTK_ERR_STATE, "no grains set");
+  sync_cur(c);
   const bool swap = num_image - c->iref >= c->cfg.iraz;
   launch_end_frame(c->g, swap ? 1 : 0, c->stream);
   c->launches += 1;
@@ -1260,6 +1312,7 @@ int ptk_track_frame(ptk_ctx* c, int num_image) {
     c->launches = before;  // counted again at each replay below
   }
   CK(cudaGraphLaunch(c->graph[key], c->stream));
+  c->cur_pending = false;  // the graph waited for the upload before reading the frame
   // launches of one frame: precompute, stage_begin, (search, finalize) per level,
   // subpixel, end_frame
   int64_t nk = (pre ? 1 : 0) + 1;
@@ -1294,6 +1347,7 @@ static int objective_common(ptk_ctx* c, const double* X3n, double* f, double* g3
   if (!c || !X3n || !f) return fail(c, PTK_ERR_ARG, "null argument");
   int rc = check_ready(c, true);
   if (rc) return rc;
+  sync_cur(c);
   if (g3n && c->cfg.image_interpolator != PTK_INTERP_CUBIC)
     return fail(c, PTK_ERR_ARG, "the gradient is implemented for the cubic interpolator");
   if (g3n && (size_t)c->max_P * 24 > 227 * 1024) return fail(c, PTK_ERR_LIMIT, "pattern too large for ptk_grad");
@@ -1335,6 +1389,7 @@ int ptk_set_distortion(ptk_ctx* c, const double* p14) {
 
 int ptk_remap_frame(ptk_ctx* c, int slot) {
   if (!c || slot < 0 || slot > 1) return fail(c, PTK_ERR_ARG, "bad arguments");
+  sync_cur(c);
   if (!c->have_disto) return fail(c, PTK_ERR_STATE, "no distortion parameters set");
   if (!c->loaded[slot]) return fail(c, PTK_ERR_STATE, "frame not loaded");
   const int dimx = c->cfg.dimx, dimy = c->cfg.dimy;
@@ -1358,6 +1413,7 @@ int ptk_remap_frame(ptk_ctx* c, int slot) {
 
 int ptk_set_stream(ptk_ctx* c, void* s) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  sync_cur(c);
   CK(cudaStreamSynchronize(c->stream));
   c->stream = s ? static_cast<cudaStream_t>(s) : c->own_stream;
   return PTK_OK;
@@ -1367,6 +1423,7 @@ void* ptk_get_stream(ptk_ctx* c) { return c ? static_cast<void*>(c->stream) : nu
 
 int ptk_synchronize(ptk_ctx* c) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  sync_cur(c);
   CK(cudaStreamSynchronize(c->stream));
   int flag = 0;  // set by a device wait that gave up (BF16 search)
   CK(cudaMemcpy(&flag, c->d_counts + 3, sizeof(int), cudaMemcpyDeviceToHost));

@@ -154,7 +154,10 @@ constexpr int kBf16RingDefault = 4;
 size_t bf16_weight_entries(int half);
 void prepare_search_bf16();
 // ev (optional, 5 events): recorded before the first kernel and after each of the four
-void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent_t* ev = nullptr);
+// frame_ready (may be null): an event the search waits for after the weights
+// kernel (recorded where the current frame's upload completes)
+void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent_t* ev = nullptr,
+                        cudaEvent_t frame_ready = nullptr);
 void launch_end_frame(const GrainsDev& g, int swap_reference, cudaStream_t s);
 void prepare_subpix(int max_points, int max_r);
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& ref,

@@ -1005,10 +1005,12 @@ void prepare_search_bf16() {
   done = true;
 }
 
-void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent_t* ev) {
+void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent_t* ev, cudaEvent_t frame_ready) {
   const int items = p.max_items;
   if (ev) cudaEventRecord(ev[0], s);
   k_weights_bf16<<<p.max_items / (p.tiles_u * p.tiles_v), kWThreads, kWSmem, s>>>(p);
+  // the weights need only the reference frame: the current one may still be uploading until here
+  if (frame_ready) cudaStreamWaitEvent(s, frame_ready, cudaEventWaitExternal);
   if (ev) cudaEventRecord(ev[1], s);
   switch (p.ring) {
     case 2: k_search_bf16<2><<<grid, kThreads, kSmemBudget, s>>>(p); break;
