@@ -246,9 +246,12 @@ int read_tiff(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, s
       good = packbits_decode(src, len, dst, want, &got);
     } else {
       uLongf dl = (uLongf)want;
-      const int zr = uncompress(dst, &dl, src, (uLong)len);
-      good = zr == Z_OK || zr == Z_BUF_ERROR;  // Z_BUF_ERROR: the strip holds more than the image needs
-      got = good && zr == Z_OK ? (size_t)dl : want;
+      uLong sl = (uLong)len;
+      const int zr = uncompress2(dst, &dl, src, &sl);
+      // Z_BUF_ERROR with the output full: the strip holds more than the image
+      // needs; short output (truncated or corrupt input) fails the check below
+      good = zr == Z_OK || zr == Z_BUF_ERROR;
+      got = (size_t)dl;
     }
     if (!good || got < want) return (*err = "corrupt or short TIFF strip", PTK_ERR_IO);
     filled += want;

@@ -12,7 +12,7 @@ import numpy as np
 
 def write_tiff(path, data: np.ndarray, photometric: int | None = None, big_endian: bool = False,
                rows_per_strip: int | None = None, compression: int = 1, datetime: str | None = None,
-               predictor: int | None = None):
+               predictor: int | None = None, truncate: int = 0):
     """data: (h, w) grey or (h, w, spp) colour, uint8 or uint16, stored as
     given (compression 8 deflates each strip with zlib; other values only set
     the tag); predictor sets tag 317 (the caller stores differences)."""
@@ -29,6 +29,8 @@ def write_tiff(path, data: np.ndarray, photometric: int | None = None, big_endia
     strips = [raw[r * row_bytes:min(h, r + rps) * row_bytes] for r in range(0, h, rps)]
     if compression == 8:
         strips = [zlib.compress(s) for s in strips]
+    if truncate:  # damaged files: every strip loses its last `truncate` bytes
+        strips = [s[:-truncate] for s in strips]
     header = 8
     data_off = header
     offsets = []

@@ -84,6 +84,9 @@ def test_unsupported_and_missing_files(ptk, tmp_path, rng):
     write_tiff(p, a, compression=5)  # raw bytes under an LZW tag: not a valid code stream
     with pytest.raises(ptk.PtkError, match="corrupt"):
         ptk.read_image_file(str(p))
+    write_tiff(p, a.astype(np.uint16) * 257, compression=8, rows_per_strip=4, truncate=6)  # cut Deflate strips
+    with pytest.raises(ptk.PtkError, match="corrupt or short"):
+        ptk.read_image_file(str(p))
     write_tiff(p, a, predictor=3)  # floating-point prediction
     with pytest.raises(ptk.PtkError, match="predictor"):
         ptk.read_image_file(str(p))
