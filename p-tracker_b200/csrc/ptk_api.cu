@@ -1283,7 +1283,10 @@ int ptk_track_frame(ptk_ctx* c, int num_image) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
   int rc = check_ready(c, true);
   if (rc) return rc;
-  if (c->cfg.autotune && !c->tuned && (rc = ptk_autotune(c, nullptr))) return rc;
+  if (c->cfg.autotune && !c->tuned && ptk_autotune(c, nullptr) != PTK_OK) {
+    c->tuned = true;  // tuning failed (e.g. no memory for its scratch): the built-in shapes track the frame
+    c->tune_ring = c->tune_exact = 0;
+  }
   if ((rc = prepare_searches(c))) return rc;
   if (c->graph_dirty) drop_graphs(c);
   const bool pre = c->need_precompute;
