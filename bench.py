@@ -596,6 +596,22 @@ def run_sequence(args, rank: int, world: int, local: int) -> int:
         clocks = sampler.stop()
         head_rec = head.get_grains()
         res_counts = head.rescue_counts()
+        # the undistortion remap of one frame (map gather + cubic, copy back), L2 flushed before each
+        flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+        rm = []
+        for it in range(6):
+            flush.zero_()
+            head.load_frame_device(1, dev[1].data_ptr(), p["dimx"] * 2)
+            stream.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            head.remap(1)
+            e1.record(stream)
+            e1.synchronize()
+            if it > 0:
+                rm.append(e0.elapsed_time(e1))
+        del flush
         e2e_ms, _ = host_run(head)
         plain = tracker()
         device_run(plain)
@@ -631,6 +647,9 @@ def run_sequence(args, rank: int, world: int, local: int) -> int:
                          float(np.abs(pos(head_rec)[:, :2] - pos(plain_rec)[:, :2]).max()),
                          "rescued_last_frame": int(res_counts[0]), "jumping_grains": int(s["jumpers"].sum())},
             "clocks": clocks,
+            "remap": {"ms": statistics.median(rm),
+                      # map 16 B + output 2 B + copy back 2 + 2 B per pixel; the 4x4 source gathers hit L2
+                      "algorithmic_gb_s": 22.0 * p["dimx"] * p["dimy"] / (statistics.median(rm) * 1e-3) / 1e9},
         }
         if not args.no_cpu_baseline:
             sys.path.insert(0, str(ROOT / "oracle"))

@@ -99,7 +99,8 @@ typedef struct ptk_config {
   int32_t topk;                  /* BF16 search: candidates per 32x32 tile rescored exactly, those within 3 % of its best score (1..8, default 8) */
   int32_t lm_max_iter;           /* adjoint LM: iteration cap                 */
   double lm_tol;                 /* adjoint LM: step tolerance (pixels, default 1e-4) */
-  int32_t autotune;              /* 1: ptk_track_frame runs ptk_autotune once, before its first frame (default 0) */
+  int32_t autotune;              /* 1: ptk_track_frame runs ptk_autotune once, before its first frame;
+                                    if tuning fails the built-in shapes are kept (default 0) */
 } ptk_config;
 
 typedef struct ptk_ctx ptk_ctx;
