@@ -11,6 +11,7 @@
 // functions for every computation.
 #include <omp.h>
 
+#include <cstdlib>
 #include <cstring>
 
 #include "p-tracker.hpp"
@@ -425,6 +426,21 @@ int ref_read_grains(void* p, const char* path, int ptracker_format) {
 }
 
 int ref_num_grains(void* p) { return static_cast<Handle*>(p)->trk.num_grains; }
+
+// ptracker::make_grid (src/p-tracker.cpp:1280-1311) from the C library's
+// first random numbers (srand(1), the sequence a fresh process starts with);
+// returns the grain count, positions in xy (2 ints per grain).
+int ref_make_grid(void* p, double xmin, double xmax, double ymin, double ymax, int nx, int ny, int alea_max,
+                  int32_t* xy) {
+  ptracker& t = static_cast<Handle*>(p)->trk;
+  std::srand(1);
+  t.make_grid(xmin, xmax, ymin, ymax, nx, ny, alea_max);
+  for (int g = 0; g < t.num_grains; ++g) {
+    xy[2 * g] = t.grain[g].refcoord_xpix;
+    xy[2 * g + 1] = t.grain[g].refcoord_ypix;
+  }
+  return t.num_grains;
+}
 
 // ptracker::check_distortion (src/check_distortion.cpp:25-100) in the current
 // directory: reads the dic files dic_name % iref and % ibeg..iend (step iinc)

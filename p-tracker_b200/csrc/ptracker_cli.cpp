@@ -6,8 +6,8 @@
 // Command file: the reference's token stream (read_data,
 // src/p-tracker.cpp:1487-1784): whitespace-separated tokens, '#' or '!' starts
 // a comment to the end of the line, unknown tokens are reported and skipped.
-// Grain files, `pattern`, `targetRadiusPattern` and `mask_rect` act on the
-// grains loaded so far, in file order, as they do in the reference.  Tokens of
+// Grain files, `make_grid`, `pattern`, `targetRadiusPattern` and `mask_rect`
+// act on the grains loaded so far, in file order, as they do in the reference.  Tokens of
 // other features (RAW decoding, neighbour lists, thread counts) are accepted
 // and have no effect.  Added tokens select the forms of this library:
 //     search_method  exact | bf16          integer search (default exact)
@@ -129,6 +129,32 @@ void load_grains(Settings& s, const std::string& path, bool format13) {
   s.patterns.clear();  // the reference rebuilds its grain vector: earlier patterns are gone
 }
 
+// make_grid (src/p-tracker.cpp:1280-1311): nx x ny grains on a grid of
+// integer steps floor((max - min) / (n - 1)) from (xmin, ymin), each moved
+// by round(alea (cos a, sin a)) with a and alea drawn from the C library's
+// rand() in the reference's order (an angle, then a distance up to aleaMax),
+// refcoord truncated to int as its assignment does; refrot 0, radius 2 px.
+// The grains replace the ones loaded so far (and their patterns).
+void make_grid(Settings& s, double xmin, double xmax, double ymin, double ymax, int nx, int ny, int alea_max) {
+  if (nx < 2 || ny < 2) die("make_grid needs at least 2 points in each direction");
+  const int dx = (int)std::floor((xmax - xmin) / (double)(nx - 1));
+  const int dy = (int)std::floor((ymax - ymin) / (double)(ny - 1));
+  s.grains.assign((size_t)nx * ny, ptk_grain{});
+  size_t i = 0;
+  for (int iy = 0; iy < ny; ++iy)
+    for (int ix = 0; ix < nx; ++ix) {
+      const double angle = (double)std::rand() / (double)RAND_MAX * (2.0 * M_PI);
+      const double alea = (double)std::rand() / (double)RAND_MAX * alea_max;
+      ptk_grain& g = s.grains[i++];
+      g.refcoord_xpix = (int32_t)(xmin + ix * dx + (int)std::round(alea * std::cos(angle)));
+      g.refcoord_ypix = (int32_t)(ymin + iy * dy + (int)std::round(alea * std::sin(angle)));
+      g.refrot = 0.0;
+      g.radius_pix = 2.0;
+    }
+  s.patterns.clear();
+  std::printf("Create grid with %d points\n", nx * ny);
+}
+
 // The reference's token loop (read_data); values are read with operator>> as
 // there.
 Settings read_commands(const char* path) {
@@ -171,9 +197,11 @@ Settings read_commands(const char* path) {
       std::string f;
       in >> f;
       load_grains(s, f, true);
-    } else if (tok == "make_grid") {
-      skip(7);
-      s.warnings.push_back("make_grid (grain seeding) is not part of this build: ignored");
+    } else if (tok == "make_grid") {  // src/p-tracker.cpp:1519-1525
+      double xmin, xmax, ymin, ymax;
+      int nx, ny, alea_max;
+      in >> xmin >> xmax >> ymin >> ymax >> nx >> ny >> alea_max;
+      make_grid(s, xmin, xmax, ymin, ymax, nx, ny, alea_max);
     } else if (tok == "iref") {
       in >> s.iref;
     } else if (tok == "ibeg") {
@@ -361,7 +389,10 @@ void print_json(const Settings& s) {
     << ", \"procedure\": \"" << s.procedure << "\", \"grains\": " << s.grains.size();
   int masked = 0;
   for (const ptk_grain& g : s.grains) masked += g.masked ? 1 : 0;
-  o << ", \"masked\": " << masked << ", \"rescue_level\": " << c.rescue_level << ", \"NCC_min\": " << c.NCC_min
+  o << ", \"grain_xy\": [";
+  for (size_t i = 0; i < s.grains.size(); ++i)
+    o << (i ? ", " : "") << "[" << s.grains[i].refcoord_xpix << ", " << s.grains[i].refcoord_ypix << "]";
+  o << "], \"masked\": " << masked << ", \"rescue_level\": " << c.rescue_level << ", \"NCC_min\": " << c.NCC_min
     << ", \"NCC_min_super\": " << c.NCC_min_super << ", \"subpixel\": " << c.subpixel
     << ", \"subpix_tol\": " << c.subpix_tol << ", \"initial_direction\": [" << c.initial_direction[0] << ", "
     << c.initial_direction[1] << ", " << c.initial_direction[2] << "], \"image_interpolator\": "

@@ -251,3 +251,25 @@ def test_tiff_horizontal_predictor(ptk, tmp_path, big_endian):
     got, _ = ptk.read_image_file(str(path))
     hi = (g >> 8).astype(np.uint8)
     np.testing.assert_array_equal(got, reference_grey(hi, hi, hi))
+
+
+@pytest.mark.parametrize("alea", [0, 9])
+def test_make_grid_matches_reference(ptk, oracle, tmp_path, alea):
+    """make_grid seeds the grains as the reference's make_grid does (grid
+    steps, the random displacement drawn from the C library's rand() in the
+    same order), compared with the reference's own function."""
+    (tmp_path / "commands.txt").write_text(f"make_grid 74 2507 75 1865 14 14 {alea}\npattern rect 23 23\n")
+    cfg, out, _ = _check(ptk, tmp_path / "commands.txt", tmp_path)
+    assert cfg["grains"] == 196 and "Create grid with 196 points" in "\n".join(out)
+    if not oracle.have_reference():
+        pytest.skip("compiled reference not built here")
+    import ctypes as C
+    L = C.CDLL(str(oracle.REF_SO))
+    L.ref_create.restype = C.c_void_p
+    h = C.c_void_p(L.ref_create(8, 8))
+    xy = np.zeros(2 * 196, dtype=np.int32)
+    n = L.ref_make_grid(h, C.c_double(74), C.c_double(2507), C.c_double(75), C.c_double(1865), 14, 14, alea,
+                        xy.ctypes.data_as(C.c_void_p))
+    L.ref_destroy(h)
+    assert n == 196
+    assert cfg["grain_xy"] == xy.reshape(-1, 2).tolist()
