@@ -149,6 +149,12 @@ int ptk_load_frame(ptk_ctx* ctx, int slot, const void* pix, int dimx, int dimy, 
                    size_t pitch_bytes);
 /* Same with a device pointer (uint16, row-major, pitch in bytes). */
 int ptk_load_frame_device(ptk_ctx* ctx, int slot, const void* dev_pix, size_t pitch_bytes);
+/* Page-locked host memory (no reference counterpart): frames uploaded from
+ * it with ptk_load_frame go up asynchronously at full link speed (from
+ * ordinary memory the copy is staged and the call returns only when it is
+ * done).  ptk_host_free releases it. */
+int ptk_host_alloc(void** ptr, size_t bytes);
+int ptk_host_free(void* ptr);
 /* A frame from an unpacked RAW sensor mosaic, demosaiced on the GPU as
  * read_raw_image does after libraw's unpack (src/p-tracker.cpp:288-383):
  * `raw` is libraw's rawdata.raw_image (raw_width x raw_height uint16,

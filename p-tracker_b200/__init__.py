@@ -81,6 +81,8 @@ _SIGS = {
     "ptk_pattern_size": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "ptk_load_frame": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int, C.c_int, C.c_size_t]),
     "ptk_load_frame_device": (C.c_int, [_P, C.c_int, _P, C.c_size_t]),
+    "ptk_host_alloc": (C.c_int, [C.POINTER(_P), C.c_size_t]),
+    "ptk_host_free": (C.c_int, [_P]),
     "ptk_autotune": (C.c_int, [_P, C.POINTER(TuneReport)]),
     "ptk_load_frame_raw": (C.c_int, [_P, C.c_int, _P] + [C.c_int] * 6 + [_P]),
     "ptk_load_frame_raw_device": (C.c_int, [_P, C.c_int, _P] + [C.c_int] * 6 + [_P]),

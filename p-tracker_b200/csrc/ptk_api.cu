@@ -1010,6 +1010,22 @@ int ptk_load_frame(ptk_ctx* c, int slot, const void* pix, int dimx, int dimy, in
   return PTK_OK;
 }
 
+int ptk_host_alloc(void** ptr, size_t bytes) {
+  if (!ptr || bytes == 0) return fail(nullptr, PTK_ERR_ARG, "bad host allocation arguments");
+  *ptr = nullptr;
+  const cudaError_t e = cudaMallocHost(ptr, bytes);
+  if (e != cudaSuccess) {
+    *ptr = nullptr;
+    return fail(nullptr, PTK_ERR_CUDA, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+  }
+  return PTK_OK;
+}
+
+int ptk_host_free(void* ptr) {
+  if (ptr && cudaFreeHost(ptr) != cudaSuccess) return fail(nullptr, PTK_ERR_CUDA, "cudaFreeHost");
+  return PTK_OK;
+}
+
 int ptk_load_frame_device(ptk_ctx* c, int slot, const void* dev_pix, size_t pitch_bytes) {
   if (!c || !dev_pix || slot < 0 || slot > 1) return fail(c, PTK_ERR_ARG, "bad frame arguments");
   if (pitch_bytes < (size_t)c->cfg.dimx * 2) return fail(c, PTK_ERR_ARG, "pitch smaller than a row");

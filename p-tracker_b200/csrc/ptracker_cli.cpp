@@ -52,6 +52,8 @@
 #include <future>
 #include <iomanip>
 #include <iostream>
+#include <memory>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -87,8 +89,56 @@ struct Settings {
   int unknown_tokens = 0;
 };
 
+// Frame buffers in page-locked memory, reused across frames (the decode
+// thread takes one while the GPU still uploads from another), so uploads are
+// asynchronous and run at full link speed; ordinary heap memory when pinned
+// memory cannot be had.
+class BufferPool {
+ public:
+  ~BufferPool() {
+    for (Buf& b : free_) release(b);
+  }
+  std::shared_ptr<uint16_t> get(size_t elems) {
+    Buf b{nullptr, 0, false};
+    {
+      std::lock_guard<std::mutex> lock(m_);
+      for (size_t i = 0; i < free_.size(); ++i)
+        if (free_[i].elems >= elems) {
+          b = free_[i];
+          free_.erase(free_.begin() + (long)i);
+          break;
+        }
+    }
+    if (!b.p) {
+      void* p = nullptr;
+      if (ptk_host_alloc(&p, elems * sizeof(uint16_t)) == PTK_OK) {
+        b = Buf{static_cast<uint16_t*>(p), elems, true};
+      } else {
+        b = Buf{new uint16_t[elems], elems, false};
+      }
+    }
+    return std::shared_ptr<uint16_t>(b.p, [this, b](uint16_t*) {
+      std::lock_guard<std::mutex> lock(m_);
+      free_.push_back(b);
+    });
+  }
+
+ private:
+  struct Buf {
+    uint16_t* p;
+    size_t elems;
+    bool pinned;
+  };
+  static void release(const Buf& b) {
+    if (b.pinned) ptk_host_free(b.p);
+    else delete[] b.p;
+  }
+  std::mutex m_;
+  std::vector<Buf> free_;
+};
+
 struct Frame {
-  std::vector<uint16_t> pix;
+  std::shared_ptr<uint16_t> pix;  // dimx x dimy grey levels, from the pool
   int dimx = 0, dimy = 0;
   std::string datetime, name;
   int rc = PTK_OK;
@@ -101,14 +151,15 @@ std::string frame_name(const std::string& pattern, int num) {
   return buf;
 }
 
-Frame read_frame(const std::string& pattern, int num) {
+Frame read_frame(BufferPool* pool, const std::string& pattern, int num) {
   Frame f;
   f.name = frame_name(pattern, num);
   char when[256];
   f.rc = ptk_read_image_file(f.name.c_str(), nullptr, 0, &f.dimx, &f.dimy, nullptr, 0);
   if (f.rc == PTK_OK) {
-    f.pix.resize((size_t)f.dimx * f.dimy);
-    f.rc = ptk_read_image_file(f.name.c_str(), f.pix.data(), f.pix.size(), &f.dimx, &f.dimy, when, sizeof(when));
+    const size_t elems = (size_t)f.dimx * f.dimy;
+    f.pix = pool->get(elems);
+    f.rc = ptk_read_image_file(f.name.c_str(), f.pix.get(), elems, &f.dimx, &f.dimy, when, sizeof(when));
     f.datetime = when;
   }
   if (f.rc) f.error = ptk_image_error();
@@ -610,7 +661,8 @@ int main(int argc, char** argv) {
 
   std::printf(corr ? "\n*** PROCEDURE CORRECTION OF DISTORTION (B200) ***\n\n"
                    : "*** PROCEDURE PARTICLE IMAGE TRACKING (B200) ***\n");
-  Frame ref = read_frame(s.image_name, s.iref);
+  BufferPool pool;  // outlives every frame (declared before them)
+  Frame ref = read_frame(&pool, s.image_name, s.iref);
   if (ref.rc) die(ref.error);
   s.cfg.dimx = ref.dimx;
   s.cfg.dimy = ref.dimy;
@@ -642,7 +694,7 @@ int main(int argc, char** argv) {
   }
   auto load = [&](int slot, const Frame& f) {
     if (f.dimx != s.cfg.dimx || f.dimy != s.cfg.dimy) die(f.name + ": frame size differs from the reference frame");
-    ck(ptk_load_frame(ctx, slot, f.pix.data(), f.dimx, f.dimy, 2, (size_t)f.dimx * 2), "ptk_load_frame");
+    ck(ptk_load_frame(ctx, slot, f.pix.get(), f.dimx, f.dimy, 2, (size_t)f.dimx * 2), "ptk_load_frame");
     if (s.undistort && disto) ck(ptk_remap_frame(ctx, slot), "ptk_remap_frame");
   };
   load(0, ref);
@@ -671,7 +723,7 @@ int main(int argc, char** argv) {
     std::vector<ptk_grain> cur_g((size_t)n);
     for (int im = 1; im <= nimg1; ++im) {
       const int num = s.corr_images[im];
-      Frame cur = read_frame(s.image_name, num);
+      Frame cur = read_frame(&pool, s.image_name, num);
       if (cur.rc) die(cur.error);
       load(1, cur);
       // the estimated displacement starts every grain's search (:173-178)
@@ -735,13 +787,14 @@ int main(int argc, char** argv) {
   }
 
   std::future<Frame> next;
-  if (s.ibeg <= s.iend) next = std::async(std::launch::async, read_frame, s.image_name, s.ibeg);
+  if (s.ibeg <= s.iend) next = std::async(std::launch::async, read_frame, &pool, s.image_name, s.ibeg);
   std::vector<ptk_grain> out((size_t)n);
   for (int num = s.ibeg; num <= s.iend; num += s.iinc) {
     const double t0 = now();
     Frame cur = next.get();
     if (cur.rc) die(cur.error);
-    if (num + s.iinc <= s.iend) next = std::async(std::launch::async, read_frame, s.image_name, num + s.iinc);
+    if (num + s.iinc <= s.iend)
+      next = std::async(std::launch::async, read_frame, &pool, s.image_name, num + s.iinc);
     std::printf("\n____ Correlations from image %d towards image %d (%d/%d)\n", iref, num, num - s.ibeg + 1,
                 s.iend - s.ibeg + 1);
     load(1, cur);
