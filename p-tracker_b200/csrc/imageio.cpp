@@ -23,6 +23,7 @@
 #include <cstring>
 #include <fstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <zlib.h>
@@ -161,6 +162,24 @@ bool packbits_decode(const unsigned char* src, size_t n, unsigned char* dst, siz
   return true;
 }
 
+// rows [0, h) of a per-row function, split over a few host threads when the
+// image is large (the rows are independent)
+template <class F>
+void for_rows(uint32_t h, size_t pixels, F&& f) {
+  unsigned nt = std::thread::hardware_concurrency();
+  nt = nt > 8 ? 8 : (nt < 1 ? 1 : nt);
+  if (pixels < ((size_t)1 << 20) || nt == 1) {
+    for (uint32_t y = 0; y < h; ++y) f(y);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < nt; ++t)
+    pool.emplace_back([&, t]() {
+      for (uint32_t y = t; y < h; y += nt) f(y);
+    });
+  for (std::thread& th : pool) th.join();
+}
+
 uint16_t grey_of(double R, double G, double B) {
   const double fact = 1.0 / 255.0;
   const double rr = R * fact, gg = G * fact, bb = B * fact;
@@ -277,7 +296,7 @@ int read_tiff(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, s
         }
     }
   }
-  for (uint32_t y = 0; y < h; ++y)
+  for_rows(h, (size_t)w * h, [&](uint32_t y) {
     for (uint32_t x = 0; x < w; ++x) {
       const size_t o = (size_t)y * row_bytes + (size_t)x * bpp;
       double R, G, B;
@@ -298,6 +317,7 @@ int read_tiff(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, s
       }
       out[(size_t)y * w + x] = grey_of(R, G, B);
     }
+  });
   return PTK_OK;
 }
 
@@ -334,8 +354,11 @@ int read_pgm(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, st
   if (capacity < (size_t)w * h) return (*err = "output buffer too small", PTK_ERR_ARG);
   const size_t bpp = maxv < 256 ? 1 : 2;
   if (!r.ok(p, (size_t)w * h * bpp)) return (*err = "truncated PGM data", PTK_ERR_IO);
-  for (size_t i = 0; i < (size_t)w * h; ++i)
-    out[i] = bpp == 1 ? r.d[p + i] : (uint16_t)((r.d[p + 2 * i] << 8) | r.d[p + 2 * i + 1]);
+  const unsigned char* src = r.d.data() + p;
+  for_rows((uint32_t)h, (size_t)w * h, [&](uint32_t y) {
+    const size_t i0 = (size_t)y * w, i1 = i0 + w;
+    for (size_t i = i0; i < i1; ++i) out[i] = bpp == 1 ? src[i] : (uint16_t)((src[2 * i] << 8) | src[2 * i + 1]);
+  });
   return PTK_OK;
 }
 
@@ -350,12 +373,22 @@ int ptk_read_image_file(const char* path, uint16_t* out, size_t capacity, int* d
   if (!path || !dimx || !dimy) return PTK_ERR_ARG;
   Reader r;
   {
-    std::ifstream f(path, std::ios::binary);
+    std::ifstream f(path, std::ios::binary | std::ios::ate);  // one sized read: frames are tens of MB
     if (!f) {
       g_image_error = std::string("cannot open ") + path;
       return PTK_ERR_IO;
     }
-    r.d.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+    const std::streamoff size = f.tellg();
+    if (size < 0) {
+      g_image_error = std::string("cannot read ") + path;
+      return PTK_ERR_IO;
+    }
+    r.d.resize((size_t)size);
+    f.seekg(0);
+    if (size > 0 && !f.read(reinterpret_cast<char*>(r.d.data()), size)) {
+      g_image_error = std::string("cannot read ") + path;
+      return PTK_ERR_IO;
+    }
   }
   std::string when = "dateTime unknown", err;
   int rc;

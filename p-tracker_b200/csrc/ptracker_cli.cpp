@@ -151,10 +151,21 @@ std::string frame_name(const std::string& pattern, int num) {
   return buf;
 }
 
-Frame read_frame(BufferPool* pool, const std::string& pattern, int num) {
+// expect: the size of the frames read so far (0: unknown); a frame of that
+// size is read from disk once, any other after a size query.
+Frame read_frame(BufferPool* pool, const std::string& pattern, int num, size_t expect) {
   Frame f;
   f.name = frame_name(pattern, num);
   char when[256];
+  if (expect > 0) {
+    f.pix = pool->get(expect);
+    f.rc = ptk_read_image_file(f.name.c_str(), f.pix.get(), expect, &f.dimx, &f.dimy, when, sizeof(when));
+    if (f.rc == PTK_OK) {
+      f.datetime = when;
+      return f;
+    }
+    f.pix.reset();
+  }
   f.rc = ptk_read_image_file(f.name.c_str(), nullptr, 0, &f.dimx, &f.dimy, nullptr, 0);
   if (f.rc == PTK_OK) {
     const size_t elems = (size_t)f.dimx * f.dimy;
@@ -662,7 +673,7 @@ int main(int argc, char** argv) {
   std::printf(corr ? "\n*** PROCEDURE CORRECTION OF DISTORTION (B200) ***\n\n"
                    : "*** PROCEDURE PARTICLE IMAGE TRACKING (B200) ***\n");
   BufferPool pool;  // outlives every frame (declared before them)
-  Frame ref = read_frame(&pool, s.image_name, s.iref);
+  Frame ref = read_frame(&pool, s.image_name, s.iref, 0);
   if (ref.rc) die(ref.error);
   s.cfg.dimx = ref.dimx;
   s.cfg.dimy = ref.dimy;
@@ -723,7 +734,7 @@ int main(int argc, char** argv) {
     std::vector<ptk_grain> cur_g((size_t)n);
     for (int im = 1; im <= nimg1; ++im) {
       const int num = s.corr_images[im];
-      Frame cur = read_frame(&pool, s.image_name, num);
+      Frame cur = read_frame(&pool, s.image_name, num, (size_t)ref.dimx * ref.dimy);
       if (cur.rc) die(cur.error);
       load(1, cur);
       // the estimated displacement starts every grain's search (:173-178)
@@ -787,14 +798,16 @@ int main(int argc, char** argv) {
   }
 
   std::future<Frame> next;
-  if (s.ibeg <= s.iend) next = std::async(std::launch::async, read_frame, &pool, s.image_name, s.ibeg);
+  const size_t frame_elems = (size_t)ref.dimx * ref.dimy;
+  if (s.ibeg <= s.iend)
+    next = std::async(std::launch::async, read_frame, &pool, s.image_name, s.ibeg, frame_elems);
   std::vector<ptk_grain> out((size_t)n);
   for (int num = s.ibeg; num <= s.iend; num += s.iinc) {
     const double t0 = now();
     Frame cur = next.get();
     if (cur.rc) die(cur.error);
     if (num + s.iinc <= s.iend)
-      next = std::async(std::launch::async, read_frame, &pool, s.image_name, num + s.iinc);
+      next = std::async(std::launch::async, read_frame, &pool, s.image_name, num + s.iinc, frame_elems);
     std::printf("\n____ Correlations from image %d towards image %d (%d/%d)\n", iref, num, num - s.ibeg + 1,
                 s.iend - s.ibeg + 1);
     load(1, cur);
