@@ -48,6 +48,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <fstream>
 #include <future>
 #include <iomanip>
@@ -797,17 +798,25 @@ int main(int argc, char** argv) {
     return 0;
   }
 
-  std::future<Frame> next;
+  // the next two frames are read and decoded on host threads while the GPU
+  // tracks the current one (one frame's file read overlaps the other's decode)
   const size_t frame_elems = (size_t)ref.dimx * ref.dimy;
-  if (s.ibeg <= s.iend)
-    next = std::async(std::launch::async, read_frame, &pool, s.image_name, s.ibeg, frame_elems);
+  std::deque<std::future<Frame>> ahead;
+  int queued = s.ibeg;
+  auto refill = [&]() {
+    while (ahead.size() < 2 && queued <= s.iend) {
+      ahead.push_back(std::async(std::launch::async, read_frame, &pool, s.image_name, queued, frame_elems));
+      queued += s.iinc;
+    }
+  };
+  refill();
   std::vector<ptk_grain> out((size_t)n);
   for (int num = s.ibeg; num <= s.iend; num += s.iinc) {
     const double t0 = now();
-    Frame cur = next.get();
+    Frame cur = ahead.front().get();
+    ahead.pop_front();
     if (cur.rc) die(cur.error);
-    if (num + s.iinc <= s.iend)
-      next = std::async(std::launch::async, read_frame, &pool, s.image_name, num + s.iinc, frame_elems);
+    refill();
     std::printf("\n____ Correlations from image %d towards image %d (%d/%d)\n", iref, num, num - s.ibeg + 1,
                 s.iend - s.ibeg + 1);
     load(1, cur);
