@@ -73,21 +73,25 @@ bool value(const Reader& r, const Entry& e, uint32_t k, uint32_t* v) {
 
 // TIFF LZW: decodes src into dst (at most cap bytes); *out = bytes written.
 bool lzw_decode(const unsigned char* src, size_t n, unsigned char* dst, size_t cap, size_t* out) {
-  static thread_local uint16_t prefix[4096];
-  static thread_local unsigned char suffix[4096], first[4096];
-  static thread_local uint16_t length[4096];
+  uint16_t prefix[4096], length[4096];  // the code table, on this thread's stack (24 KB)
+  unsigned char suffix[4096], first[4096];
   for (int c = 0; c < 256; ++c) {
     prefix[c] = 0xffff;
     suffix[c] = first[c] = (unsigned char)c;
     length[c] = 1;
   }
-  size_t bit = 0, o = 0;
+  size_t o = 0, pos = 0;  // output bytes, input bytes consumed into acc
+  uint64_t acc = 0;       // the next nbits input bits, most significant first
+  int nbits = 0;
   int width = 9, next = 258, prev = -1;
   auto read = [&](int* code) -> bool {
-    if (bit + (size_t)width > 8 * n) return false;
-    int v = 0;
-    for (int k = 0; k < width; ++k, ++bit) v = (v << 1) | ((src[bit >> 3] >> (7 - (bit & 7))) & 1);
-    *code = v;
+    while (nbits < width && pos < n) {
+      acc = (acc << 8) | src[pos++];
+      nbits += 8;
+    }
+    if (nbits < width) return false;
+    nbits -= width;
+    *code = (int)((acc >> nbits) & ((1u << width) - 1u));
     return true;
   };
   auto emit = [&](int code) -> bool {  // the string of `code`, written back to front
@@ -162,22 +166,29 @@ bool packbits_decode(const unsigned char* src, size_t n, unsigned char* dst, siz
   return true;
 }
 
-// rows [0, h) of a per-row function, split over a few host threads when the
-// image is large (the rows are independent)
+// items [0, n) of a per-item function (rows, strips), split over a few host
+// threads when there is enough work (`work` bytes or pixels); the items are
+// independent
 template <class F>
-void for_rows(uint32_t h, size_t pixels, F&& f) {
+void for_items(size_t n, size_t work, F&& f) {
   unsigned nt = std::thread::hardware_concurrency();
   nt = nt > 8 ? 8 : (nt < 1 ? 1 : nt);
-  if (pixels < ((size_t)1 << 20) || nt == 1) {
-    for (uint32_t y = 0; y < h; ++y) f(y);
+  if (work < ((size_t)1 << 20) || nt == 1 || n < 2) {
+    for (size_t i = 0; i < n; ++i) f(i);
     return;
   }
+  if ((size_t)nt > n) nt = (unsigned)n;
   std::vector<std::thread> pool;
   for (unsigned t = 0; t < nt; ++t)
     pool.emplace_back([&, t]() {
-      for (uint32_t y = t; y < h; y += nt) f(y);
+      for (size_t i = t; i < n; i += nt) f(i);
     });
   for (std::thread& th : pool) th.join();
+}
+
+template <class F>
+void for_rows(uint32_t h, size_t pixels, F&& f) {
+  for_items(h, pixels, [&](size_t y) { f((uint32_t)y); });
 }
 
 uint16_t grey_of(double R, double G, double B) {
@@ -246,14 +257,21 @@ int read_tiff(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, s
   uint32_t rps = get(278, h);
   if (rps == 0 || rps > h) rps = h;
   std::vector<unsigned char> pix(row_bytes * h);
-  size_t filled = 0;
-  for (uint32_t k = 0; k < ent[273].count && filled < pix.size(); ++k) {
+  const size_t strip_bytes = (size_t)rps * row_bytes;
+  const size_t nstrips = (pix.size() + strip_bytes - 1) / strip_bytes;  // strips the image needs
+  if (ent[273].count < nstrips || ent[279].count < nstrips)
+    return (*err = "TIFF strips shorter than the image", PTK_ERR_IO);
+  // strip k fills bytes [k strip_bytes, ...) of the image: strips decode independently
+  std::vector<unsigned char> bad(nstrips, 0);  // 1 truncated, 2 corrupt or short
+  auto strip = [&](size_t k) {
     uint32_t off = 0, len = 0;
-    if (!value(r, ent[273], k, &off) || !value(r, ent[279], k, &len) || !r.ok(off, len))
-      return (*err = "truncated TIFF strip", PTK_ERR_IO);
-    const size_t want = std::min(pix.size() - filled, (size_t)rps * row_bytes);
+    if (!value(r, ent[273], (uint32_t)k, &off) || !value(r, ent[279], (uint32_t)k, &len) || !r.ok(off, len)) {
+      bad[k] = 1;
+      return;
+    }
+    const size_t at = k * strip_bytes, want = std::min(pix.size() - at, strip_bytes);
     const unsigned char* src = r.d.data() + off;
-    unsigned char* dst = pix.data() + filled;
+    unsigned char* dst = pix.data() + at;
     size_t got = 0;
     bool good = true;
     if (comp == 1) {
@@ -272,15 +290,18 @@ int read_tiff(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, s
       good = zr == Z_OK || zr == Z_BUF_ERROR;
       got = (size_t)dl;
     }
-    if (!good || got < want) return (*err = "corrupt or short TIFF strip", PTK_ERR_IO);
-    filled += want;
+    if (!good || got < want) bad[k] = 2;
+  };
+  for_items(nstrips, comp == 1 ? pix.size() : pix.size() * 4, strip);
+  for (size_t k = 0; k < nstrips; ++k) {
+    if (bad[k] == 1) return (*err = "truncated TIFF strip", PTK_ERR_IO);
+    if (bad[k] == 2) return (*err = "corrupt or short TIFF strip", PTK_ERR_IO);
   }
-  if (filled < pix.size()) return (*err = "TIFF strips shorter than the image", PTK_ERR_IO);
   auto sample = [&](size_t o) -> uint32_t {
     return bps == 8 ? pix[o] : (r.le ? (uint32_t)(pix[o] | (pix[o + 1] << 8)) : (uint32_t)((pix[o] << 8) | pix[o + 1]));
   };
   if (pred == 2) {  // horizontal differencing: each sample adds the same channel's sample to its left
-    for (uint32_t y = 0; y < h; ++y) {
+    for_rows(h, (size_t)w * h, [&](uint32_t y) {
       unsigned char* row = pix.data() + (size_t)y * row_bytes;
       for (uint32_t x = 1; x < w; ++x)
         for (uint32_t c = 0; c < spp; ++c) {
@@ -294,28 +315,36 @@ int read_tiff(Reader& r, uint16_t* out, size_t capacity, int* dimx, int* dimy, s
             row[o + 1] = (unsigned char)(r.le ? v >> 8 : v & 0xff);
           }
         }
-    }
+    });
+  }
+  // every grey level comes from 8-bit channels: a grey image maps through a
+  // 256-entry table of grey_of(v, v, v); a colour one adds the channels'
+  // weighted terms, each precomputed per 8-bit value, in grey_of's order
+  uint16_t lut[256];
+  double tr[256], tg[256], tb[256];
+  for (int v = 0; v < 256; ++v) {
+    const double f = (double)v * (1.0 / 255.0);
+    lut[v] = grey_of(v, v, v);
+    tr[v] = 0.299 * f;
+    tg[v] = 0.587 * f;
+    tb[v] = 0.114 * f;
   }
   for_rows(h, (size_t)w * h, [&](uint32_t y) {
     for (uint32_t x = 0; x < w; ++x) {
       const size_t o = (size_t)y * row_bytes + (size_t)x * bpp;
-      double R, G, B;
       if (grey) {
         uint32_t v = sample(o);
         if (bps == 16) v >>= 8;  // the RGBA reader keeps the high byte of 16-bit grey
         if (photo == 0) v = 255 - v;
-        R = G = B = v;
+        out[(size_t)y * w + x] = lut[v];
       } else {
         uint32_t c[3];
         for (int k = 0; k < 3; ++k) {
           c[k] = sample(o + k * (bps / 8));
           if (bps == 16) c[k] = (c[k] + 128) / 257;
         }
-        R = c[0];
-        G = c[1];
-        B = c[2];
+        out[(size_t)y * w + x] = (uint16_t)(65535.0 * (tr[c[0]] + tg[c[1]] + tb[c[2]]));
       }
-      out[(size_t)y * w + x] = grey_of(R, G, B);
     }
   });
   return PTK_OK;
