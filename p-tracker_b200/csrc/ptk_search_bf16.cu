@@ -27,8 +27,8 @@
 //     per-candidate best records in the reference's order; the level's usual
 //     finalize applies the acceptance rule to them.
 //
-// Tensor-core formulation of step 2 (one work item = one grain, persistent
-// CTAs, one per SM, 512 threads):
+// Tensor-core formulation of step 2 (one work item = one 32 x 32 candidate
+// tile of one grain, persistent CTAs, one per SM, 512 threads):
 //   * A operands (M = 128 = 4 x-shifts j by 32 rotation slots r, K = 16
 //     footprint columns): W_r and M_r, stored in the grain's scratch slot as
 //     [footprint row][8-column block][rotation][8 values] (512 bytes per row
@@ -428,13 +428,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
       s_bb[1] = s_bb[3] = INT_MIN;
     }
     __syncthreads();
-    const int li = s_li;
+    // work item = (list entry, tile): the tiles of a large zone (rescues)
+    // spread over CTAs instead of running one after another in one
+    const int item = s_li;
+    const int li = item / tiles, t_item = item - li * tiles;
     if (li >= count || s_err) break;
     const int gi = p.list[li];
     const int b = g.pstart[gi], P = g.pstart[gi + 1] - b;
     int2* topk_g = p.topk + (size_t)li * tiles * kBf16KeepMax;
     if (g.masked[gi] || (g.flags[gi] & 2) || P <= 0 || P > kMaxPatternPoints) {
-      for (int e = tid; e < tiles * kBf16KeepMax; e += kThreads) topk_g[e] = make_int2(INT_MIN, INT_MIN);
+      if (tid < kBf16KeepMax) topk_g[(size_t)t_item * kBf16KeepMax + tid] = make_int2(INT_MIN, INT_MIN);
       continue;
     }
     // rotation cos/sin (total_rot = base_rot + step, as the exact search) and
@@ -482,7 +485,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     bool exact_bb = false;
     const float sub = 8388608.0f + rintf(mean0);  // pixel v -> (2^23 + v) - sub = v - m, exactly
 
-    for (int t = 0; t < tiles; ++t) {
+    for (int t = t_item; t <= t_item; ++t) {
       const int tu = t / p.tiles_v, tv = t - tu * p.tiles_v;
       const int u0 = -p.left + tu * kTileU, u1 = min(u0 + kTileU - 1, p.right);
       const int v0 = -p.up + tv * kTileV, v1 = min(v0 + kTileV - 1, p.down);
