@@ -911,6 +911,7 @@ def main() -> int:
         alg = 6.0 * ppc / (k_search_ms * 1e-3) / 1e12
         gemm = gemm_flops(pair["rec"]) / (k_search_ms * 1e-3) / 1e12
         truth_err = np.abs(head_rec[:, 4:6] - pair["truth"][:, :2])
+        plain_err = np.abs(plain_rec[:, 4:6] - pair["truth"][:, :2])
         agree = np.all(bf16_pix[:, 4:7] == exact_pix[:, 4:7], axis=1)
         frame_bytes = pair["ref"].nbytes + pair["cur"].nbytes
         nn = n
@@ -942,6 +943,8 @@ def main() -> int:
                          "peak_source": peaks["source"] + " bf16 dense (burst)"},
             "accuracy": {"median_abs_err_px_vs_truth": float(np.median(truth_err)),
                          "max_abs_err_px_vs_truth": float(truth_err.max()),
+                         "plain_median_abs_err_px_vs_truth": float(np.median(plain_err)),
+                         "plain_max_abs_err_px_vs_truth": float(plain_err.max()),
                          "integer_argmax_agreement_vs_exact_search": float(agree.mean()),
                          "max_abs_err_px_vs_plain": float(np.abs(head_rec[:, 4:6] - plain_rec[:, 4:6]).max()),
                          "max_abs_err_rad_vs_plain": float(np.abs(head_rec[:, 6] - plain_rec[:, 6]).max())},
