@@ -111,6 +111,7 @@ struct ptk_ctx {
   bool bf_geom_dirty{true};            // patterns changed since the slots were laid out
   int2* d_topk{nullptr};
   unsigned* d_topk_rot{nullptr};  // rotation steps of each kept candidate to rescore
+  float* d_tile_top{nullptr};     // best ranking score of each (grain, tile)
   SearchBest* d_rescored{nullptr};
   size_t bf_cap{0};  // (list entries x tiles) the per-tile buffers hold
 
@@ -453,13 +454,16 @@ int ensure_bf16(ptk_ctx* c, size_t items) {
   if (items > c->bf_cap) {
     cudaFree(c->d_topk);
     cudaFree(c->d_topk_rot);
+    cudaFree(c->d_tile_top);
     cudaFree(c->d_rescored);
     c->d_topk = nullptr;
     c->d_topk_rot = nullptr;
+    c->d_tile_top = nullptr;
     c->d_rescored = nullptr;
     c->bf_cap = 0;
     CK(cudaMalloc(&c->d_topk, sizeof(int2) * kBf16KeepMax * items));
     CK(cudaMalloc(&c->d_topk_rot, sizeof(unsigned) * kBf16KeepMax * items));
+    CK(cudaMalloc(&c->d_tile_top, sizeof(float) * items));
     CK(cudaMalloc(&c->d_rescored, sizeof(SearchBest) * kBf16KeepMax * items));
     c->bf_cap = items;
     invalidate(c);
@@ -535,6 +539,7 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
     b.wslots = c->d_bf_wslots;
     b.topk = c->d_topk;
     b.topk_rot = c->d_topk_rot;
+    b.tile_top = c->d_tile_top;
     b.ring = c->tune_ring > 0 && bf16_ring_ok(c->max_R, c->tune_ring) ? c->tune_ring : kBf16RingDefault;
     b.rescored = c->d_rescored;
     b.error = c->d_counts + 3;
@@ -753,6 +758,7 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_bf_wslots);
   cudaFree(c->d_topk);
   cudaFree(c->d_topk_rot);
+  cudaFree(c->d_tile_top);
   cudaFree(c->d_rescored);
   cudaFree(c->d_map);
   cudaFree(c->d_X);

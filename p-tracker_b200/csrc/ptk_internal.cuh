@@ -116,6 +116,7 @@ struct Bf16Launch {
   int2* topk;               // [list entry][tile][kBf16KeepMax] kept (u, v), INT_MIN when none
   unsigned* topk_rot;       // same layout: bit r = rotation step r is rescored at that candidate
   int ring;                 // operand-row buffers of the search kernel's ring (2..8; the strips take the rest)
+  float* tile_top;          // [list entry][tile] the tile's best ranking score (-inf: no candidate)
   SearchBest* rescored;     // [list entry][tile][kBf16KeepMax] exact best per kept candidate
   int* error;               // set when a bounded wait gave up
 };

@@ -438,6 +438,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     int2* topk_g = p.topk + (size_t)li * tiles * kBf16KeepMax;
     if (g.masked[gi] || (g.flags[gi] & 2) || P <= 0 || P > kMaxPatternPoints) {
       if (tid < kBf16KeepMax) topk_g[(size_t)t_item * kBf16KeepMax + tid] = make_int2(INT_MIN, INT_MIN);
+      if (tid == 0) p.tile_top[item] = -INFINITY;
       continue;
     }
     // rotation cos/sin (total_rot = base_rot + step, as the exact search) and
@@ -527,7 +528,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
           oob = X + bbx0 + u0 < 0 || Y + bby0 + v0 < 0 || X + bbx1 + u1 >= p.cur.dimx || Y + bby1 + v1 >= p.cur.dimy;
         }
         if (oob) {
-          if (tid == 0) atomicOr(&g.flags[gi], 1);
+          if (tid == 0) {
+            atomicOr(&g.flags[gi], 1);
+            p.tile_top[(size_t)li * tiles + t] = -INFINITY;
+          }
           if (tid < kBf16KeepMax) topk[tid] = make_int2(INT_MIN, INT_MIN);
           continue;
         }
@@ -761,6 +765,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
           const int mkey = __reduce_max_sync(0xffffffffu, key);
           if (k == 0) {
             top = key2f(mkey);
+            if (lane == 0) p.tile_top[(size_t)li * tiles + t] = mkey == INT_MIN ? -INFINITY : top;
             // D / sqrt(S) <= NCC sqrt(C0C0)
             if (!(top * c00_rsqrt >= kGoodMatch)) rel = kKeepRelWeak;
           }
@@ -841,7 +846,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
 // 3. Exact rescoring of the kept candidates of a tile, at the rotation steps
 //    the search marked for each (those within the keep margin of the
 //    candidate's best step), with the exact search's integer sums and NCC
-//    expression.  One block per (grain, tile); a work unit is one rotation
+//    expression; tiles of a multi-tile zone whose best score is more than the
+//    weak keep margin below the grain's best tile are not rescored.  One block per (grain, tile); a work unit is one rotation
 //    step for two candidates that both need it (or one), taken by one warp
 //    whose lanes share the pattern points; per candidate the best record over
 //    its rotation steps in the reference's order.
@@ -865,7 +871,16 @@ __global__ void __launch_bounds__(256, 4) k_rescore_bf16(Bf16Launch p) {
   const int NU = p.left + p.right + 1, NV = p.up + p.down + 1;
   if (tid == 0) {  // the kept candidates, compacted: anchor pixel index and order index without the rotation
     int nk = 0, nu = 0;
-    if (!skip) {
+    // a tile whose best score lies further below the grain's best tile than
+    // the weak keep margin cannot hold the exact best (the keep rule's bound)
+    bool far = false;
+    if (tiles > 1) {
+      const float* tt = p.tile_top + (size_t)li * tiles;
+      float best = -INFINITY;
+      for (int k = 0; k < tiles; ++k) best = fmaxf(best, tt[k]);
+      far = best > 0.0f && tt[item - li * tiles] < best * (1.0f - kKeepRelWeak);
+    }
+    if (!skip && !far) {
       const int2* cand = p.topk + (size_t)item * kBf16KeepMax;
       const unsigned* rots = p.topk_rot + (size_t)item * kBf16KeepMax;
       const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
