@@ -100,9 +100,10 @@ constexpr long kWaitLimit = 1L << 22;
 // operand rows in flight: W_r and M_r of one footprint row per ring buffer
 constexpr int kRing = 8;       // barrier slots
 constexpr int kRingUsed = 4;   // buffers
-// weights kernel: 512 threads, 64 KB of 32-bit maps
+// weights kernel: 512 threads, 108 KB of 32-bit maps (two blocks per SM, as
+// its registers allow)
 constexpr int kWThreads = 512;
-constexpr int kWSmem = 64 * 1024;
+constexpr int kWSmem = 108 * 1024;
 
 // A and B operand formats: BF16 x BF16 -> FP32, both K-major, M = 128, N = 256.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
