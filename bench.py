@@ -89,6 +89,38 @@ def aggregate_rate(units_per_rank: int, world: int, ms_per_step: float) -> float
     return units_per_rank * world / (ms_per_step * 1e-3)
 
 
+def ref_sample_size(n: int, threads: int) -> int:
+    """Grains per timed step of the reference arm: 32 per host thread (so the
+    reference's schedule(dynamic) OpenMP loops stay balanced over the bimodal
+    radii), at most the whole workload."""
+    return min(n, 32 * threads)
+
+
+def baseline_sample_size(n: int, threads: int) -> int:
+    """Grains of the one-off CPU baseline beside the GPU line: the whole
+    workload when it is at most 200 grains per host thread (cfg2 on 16 host
+    cores: all 2000 grains, about 17 s), else 200 per thread."""
+    return n if n <= 200 * threads else 200 * threads
+
+
+def pair_config(p: dict, n: int, zone, nsteps: int, world: int) -> dict:
+    """The `config` of a frame-pair workload, the same for both arms."""
+    return {"workload": f"{p['name']}: {p['dimx']}x{p['dimy']} {'u16' if p['maxval'] > 255 else 'u8'}, {n} grains "
+                        f"per GPU, search +-{zone[0]} px, {nsteps} rotation steps",
+            "grains_per_gpu": n, "l2": "flushed (256 MiB write) before each timed step",
+            "parallelism": f"grain shards x{world}"}
+
+
+def rotation_step_count(zone) -> int:
+    """Steps of the reference's rotation loop (double accumulation)."""
+    nsteps = 0
+    drot = -abs(zone[5] * zone[4])
+    while drot <= abs(zone[5] * zone[4]):
+        nsteps += 1
+        drot += zone[5]
+    return nsteps
+
+
 def sample_indices(n: int, k: int) -> np.ndarray:
     """Evenly spaced sample of k grains (keeps the radius mix)."""
     k = min(n, k)
@@ -194,21 +226,23 @@ def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return 0
     wl = importlib.import_module("p-tracker_b200.workloads")
-    pair = wl.make_pair(args.workload, seed=1000)
+    pair = wl.make_pair(args.workload, seed=rank_seed(rank))
     n = pair["rec"].shape[0]
-    idx = sample_indices(n, args.ref_sample)
     threads = cpu_threads()
+    idx = sample_indices(n, args.ref_sample if args.ref_sample > 0 else ref_sample_size(n, threads))
     kind, times, _ = cpu_track(pair, wl, idx, threads, steps=args.steps, warmup=args.warmup)
     per_step = statistics.mean(times)
     value = len(idx) / per_step
+    zone = wl.tracker_options(pair["params"])["zones"][0]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": args.workload, "grains": n, "sample_grains": int(len(idx)), "frame": "5616x3744 u16"
-                   if args.workload != "cfg1" else "2048x1536 u8", "pipeline": "precompute+pixel search+Powell"},
+        "config": pair_config(dict(pair["params"], name=args.workload), n, zone, rotation_step_count(zone), world),
+        "form": "the reference's own CPU path (precompute, exact pixel search, Powell subpixel), OpenMP",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": f"{len(idx)} of {n} grains (evenly spaced), full frame pipeline per step"},
+                         "sample": f"{len(idx)} of {n} grains ({len(idx) / threads:.0f} per host thread, evenly "
+                                   f"spaced over the radius mix), the whole frame pipeline per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -540,7 +574,7 @@ def run_sequence(args, rank: int, world: int, local: int) -> int:
         e1.synchronize()
         return e0.elapsed_time(e1) / (nf - 1), out
 
-    idx = sample_indices(n, args.cpu_sample)
+    idx = sample_indices(n, args.cpu_sample if args.cpu_sample > 0 else 48)
     levels = range(o["rescue_level"] + 1)
 
     def lockstep(t):
@@ -758,8 +792,9 @@ def main() -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg2")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--ref-sample", type=int, default=48)
-    ap.add_argument("--cpu-sample", type=int, default=48)
+    ap.add_argument("--ref-sample", type=int, default=0, help="grains per reference-arm step (0: 32 per host thread)")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="grains of the CPU baseline (0: all, up to 200 per host thread; cfg5: 48)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -900,11 +935,7 @@ def main() -> int:
 
     if rank == 0:
         zone = opts["zones"][0]
-        nsteps = 0
-        drot = -abs(zone[5] * zone[4])
-        while drot <= abs(zone[5] * zone[4]):  # the reference's rotation loop (double)
-            nsteps += 1
-            drot += zone[5]
+        nsteps = rotation_step_count(zone)
         ppc = search_ppc(t, pair["rec"], zone, nsteps)
         peaks = measured_peaks()
         k_search_ms = kms[1]
@@ -922,13 +953,9 @@ def main() -> int:
             "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16 ranking (f32 accumulate) + int64 exact rescoring + f32/f64 adjoint LM",
             "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {p['dimx']}x{p['dimy']} "
-                                   f"{'u16' if p['maxval'] > 255 else 'u8'}, {n} grains per GPU, search +-{zone[0]} px,"
-                                   f" {nsteps} rotation steps",
-                       "form": "BF16 tensor-core search + exact rescoring + adjoint LM (headline)",
-                       "grains_per_gpu": n, "l2": "flushed (256 MiB write) before each timed step",
-                       "autotune": tune,
-                       "parallelism": f"grain shards x{world}"},
+            "config": pair_config(dict(p, name=args.workload), n, zone, nsteps, world),
+            "form": "BF16 tensor-core search + exact rescoring + adjoint LM (headline)",
+            "autotune": tune,
             "e2e": {"value": aggregate_rate(n, world, e2e_step), "unit": UNIT,
                     "h2d_bytes_per_step": int(frame_bytes + block), "d2h_bytes_per_step": int(block)},
             "gpu_launches": int(launches),
@@ -960,12 +987,13 @@ def main() -> int:
             },
         }
         if not args.no_cpu_baseline:
-            idx = sample_indices(n, args.cpu_sample)
             threads = cpu_threads()
+            idx = sample_indices(n, args.cpu_sample if args.cpu_sample > 0 else baseline_sample_size(n, threads))
             kind, times, cpu_rec = cpu_track(pair, wl, idx, threads, steps=1)
             cpu_value = len(idx) / times[0]
             line["cpu_baseline"] = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": kind,
-                                    "sample": f"{len(idx)} of {n} grains (evenly spaced), full frame pipeline"}
+                                    "sample": f"{len(idx)} of {n} grains, the whole frame pipeline"}
+            line["accuracy"]["fp64_oracle_grains"] = int(len(idx))
             line["accuracy"]["max_abs_err_px_vs_fp64_oracle"] = float(np.abs(head_rec[idx][:, 4:6] -
                                                                              cpu_rec[:, 4:6]).max())
             line["accuracy"]["max_abs_err_rad_vs_fp64_oracle"] = float(np.abs(head_rec[idx][:, 6] -

@@ -233,6 +233,16 @@ int ptk_synchronize(ptk_ctx* ctx);
 /* Number of device kernels this context launched since creation. */
 int64_t ptk_kernel_launches(ptk_ctx* ctx);
 
+/* Failure-path test hook (no counterpart in the reference).  Every wait of the
+ * BF16 search kernel on its barriers is bounded; one that runs out sets a
+ * device flag that ptk_synchronize reports as PTK_ERR_TIMEOUT, and the kernel
+ * drains its own copies and MMAs, frees its tensor memory and returns.  With
+ * polls > 0, each later BF16 search launch of this context first waits on a
+ * barrier that nothing arrives on -- before it issues any copy or MMA -- and
+ * gives up after `polls` polls, so that path runs without a real fault.
+ * polls = 0 turns it off.  Frame graphs captured before the call are rebuilt. */
+int ptk_test_bf16_wait_timeout(ptk_ctx* ctx, int polls);
+
 /* Pixel-stage search that allocates nothing (no counterpart in the reference).
  * For callers that cannot call cudaMalloc -- a plug-in whose host application
  * owns all device memory, or a loop where an allocation and the device
@@ -243,11 +253,16 @@ int64_t ptk_kernel_launches(ptk_ctx* ctx);
  * pitch_bytes; pattern_starts: n_grains + 1 CSR offsets into pattern_xy,
  * int16 x,y pairs); `zone` is a host struct; rotations == 0 searches the
  * single step -0.0 as the reference's `rotations 0`.  max_points must bound
- * every pattern's size (<= 16384) and max_radius every |offset| after
- * rotation by refrot.  Outputs: best NCC, best x/y offset and rotation step
- * per grain (0, 0, 0, 0.0 when no NCC exceeds 0); a grain whose pattern
- * exceeds max_points/max_radius, or whose footprint leaves the frame, gets
- * NaN and an INT_MIN-based offset.  Scratch lives in one fixed 4 MiB device
+ * every pattern's size (<= 16384) and max_radius every |x| and |y| of a
+ * pattern offset after it is rotated by any searched angle (refrot + drot +
+ * step) and rounded; a pattern's Euclidean radius, rounded up, plus one
+ * always suffices.  Outputs: best NCC, best x/y offset and rotation step
+ * per grain (0, 0, 0, 0.0 when no NCC exceeds 0).  A grain gets NaN and
+ * best_u = best_v = INT_MIN + 1 when its pattern exceeds max_points or a
+ * rotated offset exceeds max_radius (the caller's limits), and NaN with
+ * INT_MIN when its footprint leaves the frame.  Each enqueue's own status is
+ * returned (PTK_ERR_CUDA when it fails); an error left pending by earlier
+ * work of the caller is neither reported nor cleared.  Scratch lives in one fixed 4 MiB device
  * array per GPU, kept for the life of the process: n_grains x rotation steps
  * x ceil(nu/32) x ceil(nv/32) must not exceed 260,080 (PTK_ERR_LIMIT
  * otherwise), with at most 4096 rotation steps.  Calls share that array, so
@@ -331,8 +346,14 @@ const char* ptk_image_error(void);
  *   re-anchoring on the undistorted reference positions, :300-386); params14
  *   in/out, index_ini / index_end = criterion / n_tracked before and after,
  *   history (may be NULL) = num_iter x 15 (index, 14 parameters) for
- *   POWELL_ITER.  The reference's LEVMAR uses lmdif1 from the absent toofus
- *   library and is rejected (PTK_ERR_ARG).
+ *   POWELL_ITER.  LEVMAR (src/distortion_correction.cpp:400-479): all 14
+ *   parameters by Levenberg-Marquardt over the residual vector, the
+ *   published MINPACK lmdif1 algorithm with tol = DBL_EPSILON (the reference
+ *   calls it from the absent toofus library; perturb14 is not used); history
+ *   (may be NULL) = 1 x 15, the final index and parameters.
+ * ptk_disto_levmar_info (no reference counterpart): exit state of the last
+ *   LEVMAR fit (lmdif's info code 0-8, or -2 when none ran), its residual
+ *   evaluations, and the text the reference prints for the code.
  * ptk_disto_tracked: the displacements after POWELL_ITER's re-anchoring.
  * ptk_disto_objective_timed (no reference counterpart): `reps` evaluations of
  *   the objective's kernels between two CUDA events, without read-back;
@@ -351,6 +372,7 @@ int ptk_disto_residuals(ptk_disto* d, const double* params14, double* value, dou
 int ptk_disto_fit(ptk_disto* d, double* params14, const double* perturb14, int algo, int num_iter,
                   double* index_ini, double* index_end, double* history);
 int ptk_disto_tracked(ptk_disto* d, double* dx, double* dy);
+int ptk_disto_levmar_info(ptk_disto* d, int* info, int* nfev, const char** text);
 int ptk_disto_objective_timed(ptk_disto* d, const double* params14, int reps, double* ms_per_eval);
 
 #ifdef __cplusplus

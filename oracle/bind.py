@@ -21,7 +21,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 PORT_SO = HERE / "_build" / "libptk_oracle.so"
 REF_SO = HERE / "_ref" / "libptk_ref.so"
-REF_SRC = Path(os.environ.get("PTK_REFERENCE_SRC", "/root/reference/src"))
+# the reference checkout sits beside this repository (sibling directory
+# reference/) unless PTK_REFERENCE_SRC names its src/ directory
+REF_SRC = Path(os.environ.get("PTK_REFERENCE_SRC", str(HERE.parent.parent / "reference" / "src")))
 
 
 def build(ref: bool = True) -> dict:

@@ -107,6 +107,7 @@ _SIGS = {
     "ptk_get_stream": (_P, [_P]),
     "ptk_synchronize": (C.c_int, [_P]),
     "ptk_kernel_launches": (C.c_int64, [_P]),
+    "ptk_test_bf16_wait_timeout": (C.c_int, [_P, C.c_int]),
     "ptk_abi_sizes": (C.c_int, [C.POINTER(C.c_size_t)] * 3),
     "ptk_search_pixel_noalloc": (C.c_int, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int] + [_P] * 8 +
                                  [C.c_int, C.c_int, C.POINTER(Zone), C.c_int] + [_P] * 5),
@@ -123,6 +124,7 @@ _SIGS = {
     "ptk_disto_residuals": (C.c_int, [_P, _P, C.POINTER(C.c_double), _P]),
     "ptk_disto_fit": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), _P]),
     "ptk_disto_tracked": (C.c_int, [_P, _P, _P]),
+    "ptk_disto_levmar_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_char_p)]),
     "ptk_disto_objective_timed": (C.c_int, [_P, _P, C.c_int, _P]),
 }
 
@@ -534,7 +536,15 @@ class DistoFit:
         hist = np.zeros((max(num_iter, 1), 15))
         self._check(self._L.ptk_disto_fit(self.h, _ptr(x), _ptr(dx), algo, num_iter, C.byref(ini), C.byref(end),
                                           _ptr(hist)))
-        return x, ini.value, end.value, hist[:num_iter] if algo == DISTO_POWELL_ITER else hist[:0]
+        keep = num_iter if algo == DISTO_POWELL_ITER else (1 if algo == DISTO_LEVMAR else 0)
+        return x, ini.value, end.value, hist[:keep]
+
+    def levmar_info(self) -> tuple[int, int, str]:
+        """Exit state of the last LEVMAR fit: lmdif's info code, residual
+        evaluations, and the text for the code."""
+        info, nfev, text = C.c_int(), C.c_int(), C.c_char_p()
+        self._check(self._L.ptk_disto_levmar_info(self.h, C.byref(info), C.byref(nfev), C.byref(text)))
+        return info.value, nfev.value, (text.value or b"").decode()
 
     def tracked(self) -> tuple[np.ndarray, np.ndarray]:
         dx = np.zeros((self.nimg1, self.n))

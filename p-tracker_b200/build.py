@@ -7,8 +7,9 @@
 Every .cu file is compiled by nvcc for sm_100a only
 (-gencode arch=compute_100a,code=sm_100a); the remap kernels are compiled with
 -fmad=false so their FP64 arithmetic repeats the CPU restatement's operations
-exactly (the remap is checked bit for bit), and so is the distortion fit's
-objective.  Objects go to _build/ next to
+exactly (the remap is checked bit for bit), and so are the distortion fit's
+objective and the plain form's subpixel objective and Powell minimiser (the
+reference is built without FMA contraction).  Objects go to _build/ next to
 this file; a source is recompiled only when it or a header is newer than its
 object.  Run `python p-tracker_b200/build.py` or call build().
 """
@@ -29,7 +30,7 @@ INCLUDE = ROOT / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-O3", "--expt-relaxed-constexpr"]
-NO_FMA = {"ptk_remap.cu", "ptk_disto.cu", "ptk_raw.cu"}
+NO_FMA = {"ptk_remap.cu", "ptk_disto.cu", "ptk_raw.cu", "ptk_subpix.cu"}
 CU_SOURCES = ["ptk_search.cu", "ptk_search_tiled.cu", "ptk_search_bf16.cu", "ptk_subpix_lm.cu", "ptk_subpix.cu", "ptk_remap.cu", "ptk_api.cu", "ptk_noalloc.cu", "ptk_disto.cu", "ptk_raw.cu"]
 CXX_SOURCES = ["grainfile.cpp", "imageio.cpp"]
 

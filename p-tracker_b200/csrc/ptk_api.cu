@@ -9,12 +9,29 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "ptk_internal.cuh"
 
 using namespace ptk;
+
+cudaError_t ptk::ensure_smem(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> set;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = set[{func, dev}];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
 
 namespace {
 
@@ -137,6 +154,7 @@ struct ptk_ctx {
 
   int iref{0};
   bool need_precompute{true};
+  int probe_wait{0};  // failure-path test hook (ptk_test_bf16_wait_timeout)
 };
 
 namespace {
@@ -543,6 +561,7 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
     b.ring = c->tune_ring > 0 && bf16_ring_ok(c->max_R, c->tune_ring) ? c->tune_ring : kBf16RingDefault;
     b.rescored = c->d_rescored;
     b.error = c->d_counts + 3;
+    b.probe_wait = c->probe_wait;
     launch_search_bf16(b, sg.grid, s, ev, frame_ready);
     frame_ready = nullptr;
     // The ranking finds the exact best wherever it is a match; a grain the
@@ -602,10 +621,11 @@ int enqueue_subpixel(ptk_ctx* c, int method, cudaStream_t s) {
     lp.tol = c->cfg.lm_tol > 0.0 ? c->cfg.lm_tol : 1e-4;
     lp.iters = nullptr;
     lp.order = c->d_order;
+    lp.max_r = c->max_R;
     launch_subpix_lm(c->g, frame(c, c->cur_slot), lp, s);
   } else if (method == PTK_SUBPIX_POWELL) {
     launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, c->max_R,
-                         s);
+                         c->d_order, s);
   } else {
     return fail(c, PTK_ERR_ARG, "unknown subpixel method");
   }
@@ -1460,6 +1480,14 @@ int ptk_synchronize(ptk_ctx* c) {
 }
 
 int64_t ptk_kernel_launches(ptk_ctx* c) { return c ? c->launches : 0; }
+
+int ptk_test_bf16_wait_timeout(ptk_ctx* c, int polls) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  if (polls < 0) return fail(c, PTK_ERR_ARG, "polls must be >= 0");
+  c->probe_wait = polls;
+  invalidate(c);  // captured frame graphs hold the old launch parameters
+  return PTK_OK;
+}
 
 int ptk_abi_sizes(size_t* config_bytes, size_t* grain_bytes, size_t* zone_bytes) {
   if (!config_bytes || !grain_bytes || !zone_bytes) return fail(nullptr, PTK_ERR_ARG, "null argument");

@@ -21,8 +21,12 @@
 // kernel for every objective value: POWELL (one minimisation, ftol 1e-12,
 // initial directions the perturbations) and POWELL_ITER (num_iter
 // minimisations, each followed by re-anchoring A1/B1 and the displacements on
-// the undistorted reference positions, :300-386).  The reference's LEVMAR
-// variant calls lmdif1 from the absent toofus library and is not provided.
+// the undistorted reference positions, :300-386), and LEVMAR (:400-479):
+// Levenberg-Marquardt over the residual vector of the GPU kernel, restated in
+// ptk_lmdif.hpp from the published MINPACK algorithm (the reference calls
+// lmdif1 from the absent toofus library with tol = DBL_EPSILON; pairs it
+// skips keep a zero residual there as here).
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -30,6 +34,7 @@
 
 #include "ptk.h"
 #include "ptk_internal.cuh"
+#include "ptk_lmdif.hpp"
 #include "ptk_undistor.cuh"
 
 struct ptk_disto {
@@ -46,6 +51,7 @@ struct ptk_disto {
   double2* d_pos{nullptr};  // undistorted points: slot 0 A1 (reference), slot 1 + im the tracked ones
   cudaStream_t stream{nullptr};
   std::string err;
+  int lm_info{-2}, lm_nfev{0};  // exit state and residual evaluations of the last LEVMAR fit
 };
 
 namespace ptk {
@@ -488,8 +494,8 @@ int ptk_disto_residuals(ptk_disto* d, const double* params14, double* value, dou
 int ptk_disto_fit(ptk_disto* d, double* params14, const double* perturb14, int algo, int num_iter,
                   double* index_ini, double* index_end, double* history) {
   if (!d || !params14 || !perturb14 || !index_ini || !index_end) return dfail(d, PTK_ERR_ARG, "null argument");
-  if (algo != PTK_DISTO_POWELL && algo != PTK_DISTO_POWELL_ITER)
-    return dfail(d, PTK_ERR_ARG, "optim_algo: POWELL and POWELL_ITER are provided (LEVMAR needs toofus lmdif1)");
+  if (algo != PTK_DISTO_POWELL && algo != PTK_DISTO_POWELL_ITER && algo != PTK_DISTO_LEVMAR)
+    return dfail(d, PTK_ERR_ARG, "optim_algo: POWELL, POWELL_ITER or LEVMAR");
   if (algo == PTK_DISTO_POWELL_ITER && num_iter < 0) return dfail(d, PTK_ERR_ARG, "powell_num_iter < 0");
   std::vector<double> X(params14, params14 + 14), DX(perturb14, perturb14 + 14);
   if (X[0] < 0.0) X[0] = 0.5 * (double)d->dimx;
@@ -521,12 +527,41 @@ int ptk_disto_fit(ptk_disto* d, double* params14, const double* perturb14, int a
       if (e == cudaSuccess) e = cudaGetLastError();
       if (e != cudaSuccess) return dfail(d, PTK_ERR_CUDA, std::string("re-anchoring: ") + cudaGetErrorString(e));
     }
+  } else if (algo == PTK_DISTO_LEVMAR) {
+    // all 14 parameters free, as the reference passes the whole vector to lmdif1
+    const long long m = (long long)d->nimg1 * d->npairs;
+    if (m < 14) return dfail(d, PTK_ERR_ARG, "LEVMAR needs at least 14 residuals (images x pairs)");
+    if (m > (1LL << 31) / 14) return dfail(d, PTK_ERR_LIMIT, "LEVMAR: residuals x 14 exceed the host Jacobian limit");
+    std::vector<double> fvec((size_t)m);
+    auto fcn = [&](const double* x, double* fv) {
+      double val = 0.0;
+      rc = disto_eval(d, x, 0, &val, fv);
+      return rc == PTK_OK;
+    };
+    int nfev = 0;
+    const int info = lmdif::lmdif1(fcn, (int)m, 14, X.data(), fvec.data(), DBL_EPSILON, &nfev);
+    if (info < 0) return rc;
+    d->lm_info = info;
+    d->lm_nfev = nfev;
+    if (history) {  // one row: final index, then the parameters (as one POWELL_ITER row)
+      if (!f(X, &v)) return rc;
+      history[0] = v / nb;
+      for (int k = 0; k < 14; ++k) history[1 + k] = X[k];
+    }
   } else if (!powell_minimize(f, X, DX, 1e-12)) {
     return rc;
   }
   if (!f(X, &v)) return rc;
   *index_end = v / nb;
   for (int k = 0; k < 14; ++k) params14[k] = X[k];
+  return PTK_OK;
+}
+
+int ptk_disto_levmar_info(ptk_disto* d, int* info, int* nfev, const char** text) {
+  if (!d || !info) return dfail(d, PTK_ERR_ARG, "null argument");
+  *info = d->lm_info;
+  if (nfev) *nfev = d->lm_nfev;
+  if (text) *text = d->lm_info >= 0 ? lmdif::info_text(d->lm_info) : "no LEVMAR fit has run";
   return PTK_OK;
 }
 

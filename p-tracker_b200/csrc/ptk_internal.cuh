@@ -119,6 +119,8 @@ struct Bf16Launch {
   float* tile_top;          // [list entry][tile] the tile's best ranking score (-inf: no candidate)
   SearchBest* rescored;     // [list entry][tile][kBf16KeepMax] exact best per kept candidate
   int* error;               // set when a bounded wait gave up
+  int probe_wait;           // failure-path test: > 0 makes the search kernel first wait this many polls on a
+                            // barrier nothing arrives on (before any copy or MMA), then report the timeout
 };
 
 struct SubpixParams {
@@ -134,7 +136,15 @@ struct LmParams {
   double tol;   // step tolerance in pixels (rotation scaled by the grain radius)
   int* iters;   // optional per-grain iteration count
   const int* order;  // grains by decreasing pattern size (one block each), or null for index order
+  int max_r;         // largest pattern radius (sizes the staged frame region)
 };
+
+// Raises `func`'s dynamic shared-memory limit to at least `bytes` on the
+// current device.  The attribute belongs to the device that is current when it
+// is set, so the largest value set is remembered per (kernel, device), behind a
+// mutex: contexts on several devices, or created from several host threads,
+// each get the limit their launches need (ptk_api.cu).
+cudaError_t ensure_smem(const void* func, size_t bytes);
 
 // ---- host-side launchers (defined in the kernel files) ------------------
 void launch_subpix_lm(const GrainsDev& g, const FrameDev& cur, const LmParams& lp, cudaStream_t s);
@@ -161,8 +171,9 @@ void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent
                         cudaEvent_t frame_ready = nullptr);
 void launch_end_frame(const GrainsDev& g, int swap_reference, cudaStream_t s);
 void prepare_subpix(int max_points, int max_r);
+// order: grains by decreasing pattern size (one block each), or null for index order
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& ref,
-                          const SubpixParams& sp, int max_points, int max_r, cudaStream_t s);
+                          const SubpixParams& sp, int max_points, int max_r, const int* order, cudaStream_t s);
 void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const double* X,
                       double* f, double* grad, int max_points, cudaStream_t s);
 void launch_widen_u8(const uint8_t* src, size_t src_pitch, uint16_t* dst, int dst_pitch, int dimx, int dimy,

@@ -127,13 +127,13 @@ __global__ void __launch_bounds__(kSearchThreads) k_search_noalloc(NoallocLaunch
       const short2 q0 = rot_round(pt, cr, sr);
       const int x0 = rx + q0.x, y0 = ry + q0.y;
       unsigned v0 = 0;
-      if (x0 < 0 || y0 < 0 || x0 >= p.dimx || y0 >= p.dimy) bad = 1;
+      if (x0 < 0 || y0 < 0 || x0 >= p.dimx || y0 >= p.dimy) bad |= 1;
       else v0 = p.ref[(size_t)y0 * p.pitch + x0];
       s_w[i] = (uint16_t)v0;
       S0 += v0;
       S00 += (long long)v0 * v0;
       const short2 q = rot_round(pt, c1, s1);
-      if (q.x < -half || q.x > half || q.y < -half || q.y > half) bad = 1;
+      if (q.x < -half || q.x > half || q.y < -half || q.y > half) bad |= 2;  // beyond max_radius: a caller limit
       s_off[i] = ((int)q.y << 16) | ((int)q.x & 0xffff);
       xmn = min(xmn, (int)q.x);
       xmx = max(xmx, (int)q.x);
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kSearchThreads) k_search_noalloc(NoallocLaunch
       ymn = min(ymn, __shfl_xor_sync(0xffffffffu, ymn, o));
       ymx = max(ymx, __shfl_xor_sync(0xffffffffu, ymx, o));
     }
-    if (bad) atomicOr(&s_bad, 1);
+    if (bad) atomicOr(&s_bad, bad);
     if (lane == 0) {
       s_red[0][warp] = S0;
       s_red[1][warp] = S00;
@@ -169,6 +169,11 @@ __global__ void __launch_bounds__(kSearchThreads) k_search_noalloc(NoallocLaunch
     const int v0 = -p.up + tv * kTileV, v1 = min(v0 + kTileV - 1, p.down);
     const int X0 = rx + gdx + bx0 + u0, Y0 = ry + gdy + by0 + v0;
     const int PW = (bx1 - bx0) + (u1 - u0) + 1, PH = (by1 - by0) + (v1 - v0) + 1;
+    if (s_bad & 2) {
+      if (tid == 0) best[item] = SearchBest{0.0, -2, 0};  // -2: a rotated offset exceeds max_radius
+      __syncthreads();
+      continue;
+    }
     const bool oob = s_bad || X0 < 0 || Y0 < 0 || X0 + PW > p.dimx || Y0 + PH > p.dimy;
     if (oob) {
       if (tid == 0) best[item] = SearchBest{0.0, -1, 0};  // -1: footprint leaves the frame
@@ -273,7 +278,7 @@ __global__ void k_finalize_noalloc(NoallocLaunch p, double* best_ncc, int32_t* b
   int err = 0;
   for (int k = 0; k < per_grain; ++k) {
     const SearchBest sb = best[(size_t)gi * per_grain + k];
-    if (sb.idx < 0) err = err ? err : sb.idx;
+    if (sb.idx < 0) err = (err == -2 || sb.idx == -2) ? -2 : -1;  // a caller-limit error outranks the frame edge
     else if (better_cand(sb.ncc, sb.idx, bn, bi)) {
       bn = sb.ncc;
       bi = sb.idx;
@@ -369,9 +374,17 @@ extern "C" int ptk_search_pixel_noalloc(const uint16_t* ref_pix, const uint16_t*
     scratch = g_addr[dev];
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // Every enqueue below reports its own status (cudaLaunchKernel, not the
+  // triple-chevron launch followed by cudaGetLastError), so an error left
+  // pending by the caller's earlier work is neither reported as this call's
+  // failure nor cleared.
   // the queue head must start at zero; the step list is rebuilt on the device
   if (cudaMemsetAsync(scratch, 0, sizeof(int), s) != cudaSuccess) return PTK_ERR_CUDA;
-  k_steps_noalloc<<<1, 1, 0, s>>>(inc, num, nrot, scratch);
+  {
+    void* args[] = {&inc, &num, &nrot, &scratch};
+    if (cudaLaunchKernel((const void*)k_steps_noalloc, dim3(1), dim3(1), args, 0, s) != cudaSuccess)
+      return PTK_ERR_CUDA;
+  }
   NoallocLaunch p;
   p.ref = ref_pix;
   p.cur = cur_pix;
@@ -400,7 +413,17 @@ extern "C" int ptk_search_pixel_noalloc(const uint16_t* ref_pix, const uint16_t*
   int sms = 148, occ = 1;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_search_noalloc, kSearchThreads, smem);
-  k_search_noalloc<<<sms * (occ > 0 ? occ : 1), kSearchThreads, smem, s>>>(p);
-  k_finalize_noalloc<<<(n_grains + 127) / 128, 128, 0, s>>>(p, best_ncc, best_u, best_v, best_drot);
-  return cudaGetLastError() == cudaSuccess ? PTK_OK : PTK_ERR_CUDA;
+  {
+    void* args[] = {&p};
+    if (cudaLaunchKernel((const void*)k_search_noalloc, dim3(sms * (occ > 0 ? occ : 1)), dim3(kSearchThreads), args,
+                         smem, s) != cudaSuccess)
+      return PTK_ERR_CUDA;
+  }
+  {
+    void* args[] = {&p, &best_ncc, &best_u, &best_v, &best_drot};
+    if (cudaLaunchKernel((const void*)k_finalize_noalloc, dim3((n_grains + 127) / 128), dim3(128), args, 0, s) !=
+        cudaSuccess)
+      return PTK_ERR_CUDA;
+  }
+  return PTK_OK;
 }

@@ -431,13 +431,7 @@ void launch_stage_begin(const GrainsDev& g, int* counts, cudaStream_t s) {
   k_stage_begin<<<(n + 255) / 256, 256, 0, s>>>(g, counts);
 }
 
-static void search_attr(size_t smem) {
-  static size_t attr_bytes = 0;
-  if (smem > attr_bytes) {
-    cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_bytes = smem;
-  }
-}
+static void search_attr(size_t smem) { ensure_smem((const void*)k_search, smem); }
 
 void launch_search(const SearchLaunch& p, int grid, size_t smem, cudaStream_t s) {
   search_attr(smem);

@@ -410,19 +410,12 @@ __global__ void __launch_bounds__(kTiledThreads, 2) k_search_tiled(SearchLaunch 
 size_t search_tiled_smem(int max_r) { return tiled_smem(max_r); }
 
 int search_tiled_occupancy(size_t smem, int max_r) {
-  static size_t attr128 = 0, attr256 = 0;
   int blocks = 0;
   if (tiled_pitch(max_r) == 128) {
-    if (smem > attr128) {
-      cudaFuncSetAttribute(k_search_tiled<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr128 = smem;
-    }
+    ensure_smem((const void*)k_search_tiled<128>, smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_search_tiled<128>, kTiledThreads, smem);
   } else {
-    if (smem > attr256) {
-      cudaFuncSetAttribute(k_search_tiled<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr256 = smem;
-    }
+    ensure_smem((const void*)k_search_tiled<256>, smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_search_tiled<256>, kTiledThreads, smem);
   }
   return blocks;

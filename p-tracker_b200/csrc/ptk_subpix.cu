@@ -18,6 +18,7 @@
 // and tests match the CPU oracle's restatement exactly.
 #include <climits>
 
+#include "ptk_crtrig.cuh"
 #include "ptk_internal.cuh"
 
 namespace ptk {
@@ -159,43 +160,147 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 // Per-grain constants of the objective.
 struct ObjGrain {
   int b, P;
-  double xref, yref;  // refcoord + d (FP64)
+  double xref, yref;  // (double)refcoord + d, in the reference's order
   double drot;
   double mean0, c0c0;
   int refx, refy;
 };
 
-// NCC_to_minimize_xyR, src/p-tracker.cpp:1018-1088.  Called by every thread
-// of the block with the same X; returns the same value on every thread.
+// Current-frame region around a grain, staged once in shared memory for the
+// objective evaluations of its Powell run (uint16, row-major).  w == 0: none.
+struct Patch {
+  const uint16_t* pix;
+  int x0, y0, w, h;
+};
+
+__device__ __forceinline__ double patch_px(const Patch& pt, int x, int y) {
+  return (double)pt.pix[(y - pt.y0) * pt.w + (x - pt.x0)];
+}
+
+// Per-grain state of the exact objective, in shared memory: the samples of
+// the last evaluation, the reference values under pattern0_rotated, and the
+// cosine and sine of the last rotation angle.
+struct ExactObj {
+  double* vals;          // P samples
+  const uint16_t* w0;    // P reference values (staged)
+  double* bcast;         // 8 doubles: [0] mean1, [1] C0C1, [2] C1C1, [3] cos, [4] sin
+  double inv_num_pix;    // 1 / P
+  double last_rot, c1, s1;
+};
+
+// Sum of d0_i^2 over the grain's points in point order, each step rounded:
+// C0C0 of do_precomputations (src/p-tracker.cpp:646-651).  One thread.
+__device__ double c0c0_in_order(const uint16_t* w0, int P, double mean0) {
+  double c = 0.0;
+  for (int i = 0; i < P; ++i) {
+    const double d0 = (double)w0[i] - mean0;
+    c += d0 * d0;
+  }
+  return c;
+}
+
+// NCC_to_minimize_xyR (src/p-tracker.cpp:1018-1088) with the reference's
+// operations in the reference's order, so that its value is the reference's
+// bit for bit whenever cos and sin of the angle are (the host C library's
+// cosine and sine are not always correctly rounded; ptk_crtrig.cuh's are):
+//   * sample positions xpix1 + c1 x + s1 y and ypix1 - s1 x + c1 y, the
+//     interpolators and the NCC expression with every product and sum rounded
+//     separately (this file is compiled without FMA contraction);
+//   * mean1 = sum of the samples in point order, times 1/P; C0C1 and C1C1
+//     summed in point order.  The samples are produced by the whole block;
+//     the three sums are sequential dependency chains run by one thread each
+//     (C0C1 and C1C1 on two warps at once).
+// Called by every thread of the block with the same X; returns the same value
+// on every thread.
 template <int NT>
-__device__ double objective(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const ObjGrain& o,
-                            const double X[3], double* vals, double* red, bool* clamped) {
+__device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp,
+                                  const ObjGrain& o, const Patch& pt, ExactObj& ex, const double X[3],
+                                  bool* clamped) {
+  const int tid = threadIdx.x;
   const double xpix1 = o.xref + X[0];
   const double ypix1 = o.yref + X[1];
   const double rot = o.drot + X[2];
-  double s1, c1;
-  sincos(rot, &s1, &c1);
-  double sum = 0.0;
-  for (int i = threadIdx.x; i < o.P; i += NT) {
+  if (!(rot == ex.last_rot)) {  // block-uniform: the line searches along x and y keep the angle
+    if (tid == 0) ex.bcast[3] = crtrig::cr_cos(rot);
+    if (tid == 32) ex.bcast[4] = crtrig::cr_sin(rot);
+    __syncthreads();
+    ex.c1 = ex.bcast[3];
+    ex.s1 = ex.bcast[4];
+    ex.last_rot = rot;
+  }
+  const double c1 = ex.c1, s1 = ex.s1;
+  for (int i = tid; i < o.P; i += NT) {
     const short2 q = g.pat0[o.b + i];
     const double x = (double)q.x, y = (double)q.y;
     const double xs = xpix1 + c1 * x + s1 * y;
     const double ys = ypix1 - s1 * x + c1 * y;
-    const double v = interp(cur, sp.interp, xs, ys, clamped);
-    vals[i] = v;
-    sum += v;
+    double v;
+    const int ix = (int)floor(xs), iy = (int)floor(ys);
+    if (sp.interp == PTK_INTERP_CUBIC && pt.w > 0 && ix - 1 >= pt.x0 && iy - 1 >= pt.y0 && ix + 2 < pt.x0 + pt.w &&
+        iy + 2 < pt.y0 + pt.h) {
+      const double x01 = xs - (double)ix, y01 = ys - (double)iy;
+      double arr[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int xx = ix - 1 + k;
+        arr[k] = cubic1(patch_px(pt, xx, iy - 1), patch_px(pt, xx, iy), patch_px(pt, xx, iy + 1),
+                        patch_px(pt, xx, iy + 2), y01);
+      }
+      v = cubic1(arr[0], arr[1], arr[2], arr[3], x01);
+    } else {
+      v = interp(cur, sp.interp, xs, ys, clamped);
+    }
+    ex.vals[i] = v;
   }
-  const double mean1 = block_sum<NT>(sum, red) * (1.0 / (double)o.P);
-  double c01 = 0.0, c11 = 0.0;
-  for (int i = threadIdx.x; i < o.P; i += NT) {
-    const double d1 = vals[i] - mean1;
-    const double d0 = (double)g.w0[o.b + i] - o.mean0;
-    c01 += d0 * d1;
-    c11 += d1 * d1;
+  __syncthreads();
+  if (tid == 0) {
+    const double* v = ex.vals;
+    double m = 0.0;
+    int i = 0;
+    for (; i + 4 <= o.P; i += 4) {
+      const double a = v[i], b = v[i + 1], c = v[i + 2], d = v[i + 3];
+      m += a;
+      m += b;
+      m += c;
+      m += d;
+    }
+    for (; i < o.P; ++i) m += v[i];
+    ex.bcast[0] = m * ex.inv_num_pix;
   }
-  c01 = block_sum<NT>(c01, red);
-  c11 = block_sum<NT>(c11, red);
-  const double ncc = c01 / sqrt(o.c0c0 * c11);
+  __syncthreads();
+  const double mean1 = ex.bcast[0];
+  if (tid == 0) {
+    const double* v = ex.vals;
+    const uint16_t* w = ex.w0;
+    double c01 = 0.0;
+    int i = 0;
+    for (; i + 2 <= o.P; i += 2) {
+      const double d1a = v[i] - mean1, d1b = v[i + 1] - mean1;
+      const double d0a = (double)w[i] - o.mean0, d0b = (double)w[i + 1] - o.mean0;
+      c01 += d0a * d1a;
+      c01 += d0b * d1b;
+    }
+    for (; i < o.P; ++i) c01 += ((double)w[i] - o.mean0) * (v[i] - mean1);
+    ex.bcast[1] = c01;
+  } else if (tid == 32) {
+    const double* v = ex.vals;
+    double c11 = 0.0;
+    int i = 0;
+    for (; i + 4 <= o.P; i += 4) {
+      const double a = v[i] - mean1, b = v[i + 1] - mean1, c = v[i + 2] - mean1, d = v[i + 3] - mean1;
+      c11 += a * a;
+      c11 += b * b;
+      c11 += c * c;
+      c11 += d * d;
+    }
+    for (; i < o.P; ++i) {
+      const double a = v[i] - mean1;
+      c11 += a * a;
+    }
+    ex.bcast[2] = c11;
+  }
+  __syncthreads();
+  const double ncc = ex.bcast[1] / sqrt(o.c0c0 * ex.bcast[2]);
   double W = 1.0;
   const double disp = sqrt(X[0] * X[0] + X[1] * X[1]);
   if (disp > sp.disp_max) W = sp.stiffness * (disp - sp.disp_max) + 1.0;
@@ -284,88 +389,6 @@ __device__ ObjGrain load_grain(const GrainsDev& g, int gi) {
   return o;
 }
 
-// Current-frame region around a grain, staged once in shared memory for the
-// objective evaluations of its Powell run (uint16, row-major).
-struct Patch {
-  const uint16_t* pix;
-  int x0, y0, w, h;
-};
-
-__device__ __forceinline__ double patch_or_frame(const Patch& pt, const FrameDev& f, int x, int y) {
-  return (double)pt.pix[(y - pt.y0) * pt.w + (x - pt.x0)];
-}
-
-// Same objective as `objective` in one pass: the samples are centred on mean0,
-// so C11 = sum (v - m0)^2 - P mean(v - m0)^2 and C01 = sum a (v - m0) - mean(v - m0) sum a
-// (sum a = S0 - P mean0) carry no harmful cancellation; one block reduction of
-// three values per evaluation.  Cubic samples whose 4x4 support lies in the
-// staged patch read shared memory.
-template <int NT>
-__device__ double objective_fast(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const ObjGrain& o,
-                                 const Patch& pt, double suma, const double X[3], double* red3, bool* clamped) {
-  const double xpix1 = o.xref + X[0];
-  const double ypix1 = o.yref + X[1];
-  double s1, c1;
-  sincos(o.drot + X[2], &s1, &c1);
-  double S1 = 0.0, S2 = 0.0, S3 = 0.0;
-  for (int i = threadIdx.x; i < o.P; i += NT) {
-    const short2 q = g.pat0[o.b + i];
-    const double x = (double)q.x, y = (double)q.y;
-    const double xs = xpix1 + c1 * x + s1 * y;
-    const double ys = ypix1 - s1 * x + c1 * y;
-    double v;
-    const int ix = (int)floor(xs), iy = (int)floor(ys);
-    if (sp.interp == PTK_INTERP_CUBIC && ix - 1 >= pt.x0 && iy - 1 >= pt.y0 && ix + 2 < pt.x0 + pt.w &&
-        iy + 2 < pt.y0 + pt.h) {
-      const double x01 = xs - (double)ix, y01 = ys - (double)iy;
-      double arr[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int xx = ix - 1 + k;
-        arr[k] = cubic1(patch_or_frame(pt, cur, xx, iy - 1), patch_or_frame(pt, cur, xx, iy),
-                        patch_or_frame(pt, cur, xx, iy + 1), patch_or_frame(pt, cur, xx, iy + 2), y01);
-      }
-      v = cubic1(arr[0], arr[1], arr[2], arr[3], x01);
-    } else {
-      v = interp(cur, sp.interp, xs, ys, clamped);
-    }
-    const double vc = v - o.mean0;
-    const double a = (double)g.w0[o.b + i] - o.mean0;
-    S1 += vc;
-    S2 += vc * vc;
-    S3 += a * vc;
-  }
-  for (int off = 16; off > 0; off >>= 1) {
-    S1 += __shfl_xor_sync(0xffffffffu, S1, off);
-    S2 += __shfl_xor_sync(0xffffffffu, S2, off);
-    S3 += __shfl_xor_sync(0xffffffffu, S3, off);
-  }
-  const int w = threadIdx.x >> 5;
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) {
-    red3[3 * w] = S1;
-    red3[3 * w + 1] = S2;
-    red3[3 * w + 2] = S3;
-  }
-  __syncthreads();
-  S1 = S2 = S3 = 0.0;
-#pragma unroll
-  for (int k = 0; k < NT / 32; ++k) {
-    S1 += red3[3 * k];
-    S2 += red3[3 * k + 1];
-    S3 += red3[3 * k + 2];
-  }
-  const double P = (double)o.P;
-  const double mvc = S1 / P;
-  const double c11 = S2 - P * mvc * mvc;
-  const double c01 = S3 - mvc * suma;
-  const double ncc = c01 / sqrt(o.c0c0 * c11);
-  double W = 1.0;
-  const double disp = sqrt(X[0] * X[0] + X[1] * X[1]);
-  if (disp > sp.disp_max) W = sp.stiffness * (disp - sp.disp_max) + 1.0;
-  return (1.0 - ncc) * W;
-}
-
 // --- Powell on the device, block-uniform ----------------------------------
 template <int NT>
 struct PowellEval {
@@ -374,13 +397,12 @@ struct PowellEval {
   const SubpixParams* sp;
   const ObjGrain* o;
   const Patch* pt;
-  double suma;
-  double* red;
+  ExactObj* ex;
   bool* clamped;
   int nfev;
   __device__ double operator()(const double X[3]) {
     ++nfev;
-    return objective_fast<NT>(*g, *cur, *sp, *o, *pt, suma, X, red, clamped);
+    return objective_exact<NT>(*g, *cur, *sp, *o, *pt, *ex, X, clamped);
   }
 };
 
@@ -536,16 +558,32 @@ __device__ void powell_minimize(F& f, double p[3], const double step[3], double 
 
 }  // namespace
 
-// follow_pattern_subpixel_xyR (src/p-tracker.cpp:1090-1128) for every grain.
+// Dynamic shared memory of the Powell kernel: the staged frame region (its
+// cap in uint16 elements first), then per pattern point a double sample and
+// the uint16 reference value.
+struct PowellSmem {
+  int patch_cap;   // elements of the staged frame region
+  int max_points;  // largest pattern of the grains
+  size_t bytes;
+};
+
+__host__ __device__ inline size_t powell_vals_offset(int patch_cap) {
+  return ((size_t)patch_cap * sizeof(uint16_t) + 15) & ~(size_t)15;
+}
+
+// follow_pattern_subpixel_xyR (src/p-tracker.cpp:1090-1128) for every grain,
+// one block per grain, grains taken in `order` (decreasing pattern size) when
+// given.
 __global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, FrameDev cur, SubpixParams sp,
-                                                                    int patch_cap) {
+                                                                    int patch_cap, int max_points,
+                                                                    const int* order) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ double red[3 * (kSubpixThreads / 32)];
+  __shared__ double bcast[8];
   __shared__ int s_clamped, s_bb[4];
-  const int gi = blockIdx.x;
+  const int gi = order ? order[blockIdx.x] : (int)blockIdx.x;
   if (g.masked[gi] || (g.flags[gi] & 3)) return;
-  const ObjGrain o = load_grain(g, gi);
-  if (o.P <= 0 || o.P > kMaxPatternPoints) return;
+  ObjGrain o = load_grain(g, gi);
+  if (o.P <= 0 || o.P > max_points) return;
   // stage the frame region under the pattern, with a margin for the Powell steps
   if (threadIdx.x == 0) {
     s_clamped = 0;
@@ -553,6 +591,9 @@ __global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, F
     s_bb[1] = s_bb[3] = -(1 << 30);
   }
   __syncthreads();
+  uint16_t* s_patch = reinterpret_cast<uint16_t*>(smem);
+  double* s_vals = reinterpret_cast<double*>(smem + powell_vals_offset(patch_cap));
+  uint16_t* s_w0 = reinterpret_cast<uint16_t*>(s_vals + max_points);
   int xmn = 1 << 30, xmx = -(1 << 30), ymn = 1 << 30, ymx = -(1 << 30);
   for (int i = threadIdx.x; i < o.P; i += kSubpixThreads) {
     const short2 q = g.pat0[o.b + i];
@@ -560,6 +601,7 @@ __global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, F
     xmx = max(xmx, (int)q.x);
     ymn = min(ymn, (int)q.y);
     ymx = max(ymx, (int)q.y);
+    s_w0[i] = g.w0[o.b + i];
   }
   atomicMin(&s_bb[0], xmn);
   atomicMax(&s_bb[1], xmx);
@@ -571,17 +613,19 @@ __global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, F
   int px0 = max(cx + s_bb[0] - kMargin, 0), py0 = max(cy + s_bb[2] - kMargin, 0);
   int px1 = min(cx + s_bb[1] + kMargin + 2, cur.dimx), py1 = min(cy + s_bb[3] + kMargin + 2, cur.dimy);
   int pw = max(px1 - px0, 0), ph = max(py1 - py0, 0);
-  if (pw * ph > patch_cap) ph = pw > 0 ? min(ph, patch_cap / pw) : 0;  // never expected: host sizes the cap
-  uint16_t* s_patch = reinterpret_cast<uint16_t*>(smem);
+  if (pw * ph > patch_cap) ph = pw > 0 ? min(ph, patch_cap / pw) : 0;  // samples outside read the frame
   for (int e = threadIdx.x; e < pw * ph; e += kSubpixThreads) {
     const int yy = e / pw, xx = e - yy * pw;
     s_patch[e] = cur.pix[(size_t)(py0 + yy) * cur.pitch + (px0 + xx)];
   }
+  // C0C0 as do_precomputations sums it (point order, each step rounded)
+  if (threadIdx.x == 0) bcast[5] = c0c0_in_order(s_w0, o.P, o.mean0);
   __syncthreads();
+  o.c0c0 = bcast[5];
   const Patch pt{s_patch, px0, py0, pw, ph};
-  const double suma = (double)g.s0[gi] - (double)o.P * o.mean0;
+  ExactObj ex{s_vals, s_w0, bcast, 1.0 / (double)o.P, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0};
   bool clamped = false;
-  PowellEval<kSubpixThreads> f{&g, &cur, &sp, &o, &pt, suma, red, &clamped, 0};
+  PowellEval<kSubpixThreads> f{&g, &cur, &sp, &o, &pt, &ex, &clamped, 0};
   double X[3] = {0.0, 0.0, 0.0};
   double fret;
   powell_minimize(f, X, sp.init_dir, sp.tol, &fret);
@@ -599,14 +643,17 @@ __global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, F
   }
 }
 
-// Objective (and optionally its gradient) at caller-given X for every grain.
+// Objective (the exact one, as Powell evaluates it) or its FP64 gradient at
+// caller-given X for every grain.
 __global__ void __launch_bounds__(kSubpixThreads) k_objective(GrainsDev g, FrameDev cur, SubpixParams sp,
-                                                                const double* Xall, double* f, double* grad) {
+                                                                const double* Xall, double* f, double* grad,
+                                                                int max_points) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[kSubpixThreads / 32];
+  __shared__ double bcast[8];
   const int gi = blockIdx.x;
-  const ObjGrain o = load_grain(g, gi);
-  if (o.P <= 0 || o.P > kMaxPatternPoints) {
+  ObjGrain o = load_grain(g, gi);
+  if (o.P <= 0 || o.P > max_points) {
     if (threadIdx.x == 0) {
       f[gi] = __longlong_as_double(0x7ff8000000000000ll);
       if (grad) grad[3 * gi] = grad[3 * gi + 1] = grad[3 * gi + 2] = f[gi];
@@ -626,45 +673,54 @@ __global__ void __launch_bounds__(kSubpixThreads) k_objective(GrainsDev g, Frame
       grad[3 * gi + 2] = G[2];
     }
   } else {
-    val = objective<kSubpixThreads>(g, cur, sp, o, X, vals, red, &clamped);
+    uint16_t* s_w0 = reinterpret_cast<uint16_t*>(vals + max_points);
+    for (int i = threadIdx.x; i < o.P; i += kSubpixThreads) s_w0[i] = g.w0[o.b + i];
+    __syncthreads();
+    if (threadIdx.x == 0) bcast[5] = c0c0_in_order(s_w0, o.P, o.mean0);
+    __syncthreads();
+    o.c0c0 = bcast[5];
+    const Patch none{nullptr, 0, 0, 0, 0};
+    ExactObj ex{vals, s_w0, bcast, 1.0 / (double)o.P, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0};
+    val = objective_exact<kSubpixThreads>(g, cur, sp, o, none, ex, X, &clamped);
   }
   if (threadIdx.x == 0) f[gi] = val;
 }
 
-static size_t powell_patch_bytes(int max_r) {
+static PowellSmem powell_smem(int max_points, int max_r) {
+  PowellSmem m;
   const size_t side = (size_t)(2 * max_r + 1 + 2 * 6 + 2);
-  return side * side * sizeof(uint16_t);
+  size_t patch = side * side;
+  const size_t rest = (size_t)max_points * (sizeof(double) + sizeof(uint16_t));
+  constexpr size_t kCap = 227 * 1024 - 1024;  // the kernel's static shared memory included
+  if (powell_vals_offset((int)patch) + rest > kCap)
+    patch = rest < kCap ? (kCap - rest) / sizeof(uint16_t) - 8 : 0;  // samples outside the region read the frame
+  m.patch_cap = (int)patch;
+  m.max_points = max_points;
+  m.bytes = powell_vals_offset(m.patch_cap) + rest;
+  return m;
 }
 
 void prepare_subpix(int max_points, int max_r) {
-  static size_t powell_bytes = 0, objective_bytes = 0;
-  const size_t a = powell_patch_bytes(max_r);
-  if (a > powell_bytes && a <= 227 * 1024) {
-    cudaFuncSetAttribute(k_subpix_powell, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a);
-    powell_bytes = a;
-  }
+  const PowellSmem m = powell_smem(max_points, max_r);
+  ensure_smem((const void*)k_subpix_powell, m.bytes);
   const size_t b = (size_t)max_points * sizeof(double) * 3;
-  if (b > objective_bytes && b <= 227 * 1024) {
-    cudaFuncSetAttribute(k_objective, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
-    objective_bytes = b;
-  }
+  if (b <= 227 * 1024) ensure_smem((const void*)k_objective, b);
 }
 
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& /*ref*/, const SubpixParams& sp,
-                          int max_points, int max_r, cudaStream_t s) {
+                          int max_points, int max_r, const int* order, cudaStream_t s) {
   if (g.n <= 0) return;
   prepare_subpix(max_points, max_r);
-  size_t smem = powell_patch_bytes(max_r);
-  if (smem > 227 * 1024) smem = 227 * 1024;  // samples outside the staged region read the frame
-  k_subpix_powell<<<g.n, kSubpixThreads, smem, s>>>(g, cur, sp, (int)(smem / sizeof(uint16_t)));
+  const PowellSmem m = powell_smem(max_points, max_r);
+  k_subpix_powell<<<g.n, kSubpixThreads, m.bytes, s>>>(g, cur, sp, m.patch_cap, max_points, order);
 }
 
 void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const double* X, double* f,
                       double* grad, int max_points, cudaStream_t s) {
   if (g.n <= 0) return;
   prepare_subpix(max_points, 0);
-  const size_t smem = (size_t)max_points * sizeof(double) * (grad ? 3 : 1);
-  k_objective<<<g.n, kSubpixThreads, smem, s>>>(g, cur, sp, X, f, grad);
+  const size_t smem = (size_t)max_points * sizeof(double) * (grad ? 3 : 1) + (grad ? 0 : (size_t)max_points * 2);
+  k_objective<<<g.n, kSubpixThreads, smem, s>>>(g, cur, sp, X, f, grad, max_points);
 }
 
 }  // namespace ptk

@@ -57,6 +57,17 @@ struct LmGrain {
   double norm_a;      // |a| = sqrt(C0C0)
 };
 
+// Current-frame region around a grain, staged once in shared memory as FP32
+// (exact for 16-bit pixels) for the evaluations of its LM run.  w == 0: none.
+struct LmPatch {
+  const float* pix;
+  int x0, y0, w, h;
+};
+
+// Margin of the staged region around the pattern's bounding box: the LM's
+// moves (pixels) plus the cubic support.
+constexpr int kLmMargin = 4;
+
 struct LmEval {
   double F, ncc;
   double H[6];  // xx, xy, xr, yy, yr, rr
@@ -67,8 +78,8 @@ struct LmEval {
 // Sums over the grain's points at X, reduced over the block in a fixed order
 // (every thread returns the same values).
 template <int NT>
-__device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain& o, const double X[3],
-                          double (*part)[kNSums]) {
+__device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmPatch& pt, const LmGrain& o,
+                          const double X[3], double (*part)[kNSums]) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double sr, cr;
   sincos(o.drot + X[2], &sr, &cr);
@@ -89,25 +100,41 @@ __device__ LmEval lm_eval(const GrainsDev& g, const FrameDev& cur, const LmGrain
     const float fpx = floorf(px), fpy = floorf(py);
     const float tx = px - fpx, ty = py - fpy;
     int ix = o.ix0 + (int)fpx, iy = o.iy0 + (int)fpy;
-    if (ix < 1 || iy < 1 || ix + 2 >= cur.dimx || iy + 2 >= cur.dimy) {
-      clamped = true;
-      ix = min(max(ix, 1), cur.dimx - 3);
-      iy = min(max(iy, 1), cur.dimy - 3);
-    }
     float wx[4], dwx[4], wy[4], dwy[4];
     cr_weights(tx, wx, dwx);
     cr_weights(ty, wy, dwy);
     float v = 0.f, gx = 0.f, gy = 0.f;
-    const uint16_t* row = cur.pix + (size_t)(iy - 1) * cur.pitch + (ix - 1);
+    if (ix - 1 >= pt.x0 && iy - 1 >= pt.y0 && ix + 2 < pt.x0 + pt.w && iy + 2 < pt.y0 + pt.h) {
+      // the 4x4 support lies in the staged region (which lies in the frame)
+      const float* row = pt.pix + (iy - 1 - pt.y0) * pt.w + (ix - 1 - pt.x0);
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      const uint16_t* rp = row + (size_t)jj * cur.pitch;
-      const float p0 = u16f(__ldg(rp)), p1 = u16f(__ldg(rp + 1)), p2 = u16f(__ldg(rp + 2)), p3 = u16f(__ldg(rp + 3));
-      const float hx = wx[0] * p0 + wx[1] * p1 + wx[2] * p2 + wx[3] * p3;
-      const float dhx = dwx[0] * p0 + dwx[1] * p1 + dwx[2] * p2 + dwx[3] * p3;
-      v += wy[jj] * hx;
-      gx += wy[jj] * dhx;
-      gy += dwy[jj] * hx;
+      for (int jj = 0; jj < 4; ++jj) {
+        const float* rp = row + jj * pt.w;
+        const float p0 = rp[0], p1 = rp[1], p2 = rp[2], p3 = rp[3];
+        const float hx = wx[0] * p0 + wx[1] * p1 + wx[2] * p2 + wx[3] * p3;
+        const float dhx = dwx[0] * p0 + dwx[1] * p1 + dwx[2] * p2 + dwx[3] * p3;
+        v += wy[jj] * hx;
+        gx += wy[jj] * dhx;
+        gy += dwy[jj] * hx;
+      }
+    } else {
+      if (ix < 1 || iy < 1 || ix + 2 >= cur.dimx || iy + 2 >= cur.dimy) {
+        clamped = true;
+        ix = min(max(ix, 1), cur.dimx - 3);
+        iy = min(max(iy, 1), cur.dimy - 3);
+      }
+      const uint16_t* row = cur.pix + (size_t)(iy - 1) * cur.pitch + (ix - 1);
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const uint16_t* rp = row + (size_t)jj * cur.pitch;
+        const float p0 = u16f(__ldg(rp)), p1 = u16f(__ldg(rp + 1)), p2 = u16f(__ldg(rp + 2)),
+                    p3 = u16f(__ldg(rp + 3));
+        const float hx = wx[0] * p0 + wx[1] * p1 + wx[2] * p2 + wx[3] * p3;
+        const float dhx = dwx[0] * p0 + dwx[1] * p1 + dwx[2] * p2 + dwx[3] * p3;
+        v += wy[jj] * hx;
+        gx += wy[jj] * dhx;
+        gy += dwy[jj] * hx;
+      }
     }
     const float gr = gx * (-s * x + c * y) + gy * (-c * x - s * y);
     const float vc = v - o.mean0;
@@ -186,8 +213,45 @@ __device__ bool lm_solve(const double H[6], const double gv[3], double lambda, d
 
 }  // namespace
 
-__global__ void __launch_bounds__(kLmThreads) k_subpix_lm(GrainsDev g, FrameDev cur, LmParams lp) {
+// Stages the frame region under the grain's pattern0_rotated points (their
+// bounding box at the start position, widened by kLmMargin plus the cubic
+// support, clipped to the frame) as FP32 in shared memory of `cap` floats.
+__device__ LmPatch lm_stage(const GrainsDev& g, const FrameDev& cur, const LmGrain& o, float* s_patch, int cap,
+                            int* s_bb) {
+  if (threadIdx.x == 0) {
+    s_bb[0] = s_bb[2] = 1 << 30;
+    s_bb[1] = s_bb[3] = -(1 << 30);
+  }
+  __syncthreads();
+  int xmn = 1 << 30, xmx = -(1 << 30), ymn = 1 << 30, ymx = -(1 << 30);
+  for (int i = threadIdx.x; i < o.P; i += kLmThreads) {
+    const short2 q = g.pat0[o.b + i];
+    xmn = min(xmn, (int)q.x);
+    xmx = max(xmx, (int)q.x);
+    ymn = min(ymn, (int)q.y);
+    ymx = max(ymx, (int)q.y);
+  }
+  atomicMin(&s_bb[0], xmn);
+  atomicMax(&s_bb[1], xmx);
+  atomicMin(&s_bb[2], ymn);
+  atomicMax(&s_bb[3], ymx);
+  __syncthreads();
+  const int x0 = max(o.ix0 + s_bb[0] - kLmMargin - 1, 0), y0 = max(o.iy0 + s_bb[2] - kLmMargin - 1, 0);
+  const int x1 = min(o.ix0 + s_bb[1] + kLmMargin + 3, cur.dimx), y1 = min(o.iy0 + s_bb[3] + kLmMargin + 3, cur.dimy);
+  int w = max(x1 - x0, 0), h = max(y1 - y0, 0);
+  if (w * h > cap) h = w > 0 ? min(h, cap / w) : 0;  // never expected: the host sizes the cap
+  for (int e = threadIdx.x; e < w * h; e += kLmThreads) {
+    const int yy = e / w, xx = e - yy * w;
+    s_patch[e] = u16f(__ldg(cur.pix + (size_t)(y0 + yy) * cur.pitch + (x0 + xx)));
+  }
+  __syncthreads();
+  return LmPatch{s_patch, x0, y0, w, h};
+}
+
+__global__ void __launch_bounds__(kLmThreads) k_subpix_lm(GrainsDev g, FrameDev cur, LmParams lp, int patch_cap) {
+  extern __shared__ __align__(16) float s_lm_patch[];
   __shared__ double part[kLmThreads / 32][kNSums];
+  __shared__ int s_bb[4];
   const int gi = lp.order ? lp.order[blockIdx.x] : (int)blockIdx.x;
   if (g.masked[gi] || (g.flags[gi] & 3)) return;
   LmGrain o;
@@ -205,9 +269,10 @@ __global__ void __launch_bounds__(kLmThreads) k_subpix_lm(GrainsDev g, FrameDev 
   o.mean0 = (float)g.mean0[gi];
   o.norm_a = sqrt(g.c0c0[gi]);
   const double rscale = g.radius[gi] > 1.0 ? g.radius[gi] : 1.0;  // rotation step in pixels at the rim
+  const LmPatch pt = lm_stage(g, cur, o, s_lm_patch, patch_cap, s_bb);
 
   double X[3] = {0.0, 0.0, 0.0};
-  LmEval cur_e = lm_eval<kLmThreads>(g, cur, o, X, part);
+  LmEval cur_e = lm_eval<kLmThreads>(g, cur, pt, o, X, part);
   bool clamped = cur_e.clamped;
   double lambda = 1e-3;
   int it = 0, accepted = 0, rejected_run = 0;
@@ -222,7 +287,7 @@ __global__ void __launch_bounds__(kLmThreads) k_subpix_lm(GrainsDev g, FrameDev 
       const double step = fmax(fmax(fabs(d[0]), fabs(d[1])), fabs(d[2]) * rscale);
       if (step < lp.tol) break;
       const double Xn[3] = {X[0] + d[0], X[1] + d[1], X[2] + d[2]};
-      const LmEval ne = lm_eval<kLmThreads>(g, cur, o, Xn, part);
+      const LmEval ne = lm_eval<kLmThreads>(g, cur, pt, o, Xn, part);
       if (isfinite(ne.F) && ne.F < cur_e.F) {
         X[0] = Xn[0];
         X[1] = Xn[1];
@@ -272,7 +337,8 @@ __global__ void __launch_bounds__(kLmThreads) k_grad_f32(GrainsDev g, FrameDev c
   o.mean0 = (float)g.mean0[gi];
   o.norm_a = sqrt(g.c0c0[gi]);
   const double X[3] = {Xall[3 * gi], Xall[3 * gi + 1], Xall[3 * gi + 2]};
-  const LmEval e = lm_eval<kLmThreads>(g, cur, o, X, part);
+  const LmPatch none{nullptr, 0, 0, 0, 0};
+  const LmEval e = lm_eval<kLmThreads>(g, cur, none, o, X, part);
   if (threadIdx.x == 0) {
     f[gi] = 1.0 - e.ncc;
     // d(1 - NCC)/dX = (1/2) dF/dX = J^T r
@@ -284,7 +350,12 @@ __global__ void __launch_bounds__(kLmThreads) k_grad_f32(GrainsDev g, FrameDev c
 
 void launch_subpix_lm(const GrainsDev& g, const FrameDev& cur, const LmParams& lp, cudaStream_t s) {
   if (g.n <= 0) return;
-  k_subpix_lm<<<g.n, kLmThreads, 0, s>>>(g, cur, lp);
+  // staged region: pattern0_rotated extent (|q| <= max_r + 1) plus the margins
+  const int side = 2 * (lp.max_r + 1) + 1 + 2 * (kLmMargin + 2);
+  int cap = side * side;
+  if ((size_t)cap * sizeof(float) > 200 * 1024) cap = 200 * 1024 / (int)sizeof(float);  // larger regions read the frame
+  ensure_smem((const void*)k_subpix_lm, (size_t)cap * sizeof(float));
+  k_subpix_lm<<<g.n, kLmThreads, (size_t)cap * sizeof(float), s>>>(g, cur, lp, cap);
 }
 
 void launch_grad_f32(const GrainsDev& g, const FrameDev& cur, const double* X, double* f, double* grad,

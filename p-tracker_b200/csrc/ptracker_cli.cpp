@@ -30,8 +30,8 @@
 // `procedure correction_distortion` tracks image_numbers_corrDisto[1..]
 // against image_numbers_corrDisto[0] (pixel search from the imposed
 // approximate displacements, no rescue, then subpixel; dic_out_<num>.txt per
-// image), then fits the 14 undistor parameters with ptk_disto_fit (POWELL or
-// POWELL_ITER; LEVMAR needs toofus's lmdif1 and is refused) and writes
+// image), then fits the 14 undistor parameters with ptk_disto_fit (POWELL,
+// POWELL_ITER or LEVMAR) and writes
 // corrDisto_log.txt, errors.txt, distobox.txt and, for POWELL_ITER,
 // convergence.txt as the reference does.
 //
@@ -659,9 +659,6 @@ int main(int argc, char** argv) {
   if (s.grains.empty()) die("no grains (grains_to_follow / start_file / restart_file)");
   if (corr) {
     if (s.corr_images.size() < 2) die("image_numbers_corrDisto needs the reference image and at least one more");
-    if (s.optim_algo == PTK_DISTO_LEVMAR)
-      die("optim_algo LEVMAR calls lmdif1 from the toofus library, which is not part of this build: use POWELL or "
-          "POWELL_ITER");
     if (s.imposed_x.size() != s.corr_images.size()) {
       s.imposed_x.assign(s.corr_images.size(), 0.0);
       s.imposed_y.assign(s.corr_images.size(), 0.0);
@@ -779,11 +776,19 @@ int main(int argc, char** argv) {
     const int iters = s.optim_algo == PTK_DISTO_POWELL_ITER ? s.powell_num_iter : 0;
     std::vector<double> hist((size_t)(iters > 0 ? iters : 1) * 15);
     double ini = 0.0, end = 0.0;
-    std::printf("START minimizing equiprojectivity criterion (with %s)\n",
-                s.optim_algo == PTK_DISTO_POWELL ? "POWELL" : "POWELL_ITER");
+    const char* algo_name = s.optim_algo == PTK_DISTO_POWELL        ? "POWELL"
+                            : s.optim_algo == PTK_DISTO_POWELL_ITER ? "POWELL_ITER"
+                                                                    : "LEVMAR";
+    std::printf("START minimizing equiprojectivity criterion (with %s)\n", algo_name);
     if (ptk_disto_fit(dfit, X, s.disto_perturb, s.optim_algo, iters, &ini, &end, hist.data()))
       die(std::string("ptk_disto_fit: ") + ptk_disto_last_error(dfit));
-    std::printf("END minimizing equiprojectivity criterion\n\n");
+    std::printf("END minimizing equiprojectivity criterion (with %s)\n\n", algo_name);
+    if (s.optim_algo == PTK_DISTO_LEVMAR) {  // src/distortion_correction.cpp:474
+      int info = 0, nfev = 0;
+      const char* text = "";
+      ptk_disto_levmar_info(dfit, &info, &nfev, &text);
+      std::printf("exit state: %s\n", text);
+    }
     ptk_disto_destroy(dfit);
     if (s.optim_algo == PTK_DISTO_POWELL_ITER) {
       std::ofstream cf("convergence.txt");

@@ -193,12 +193,6 @@ optim_algo NEWTON
     assert any("unknown for optim_algo" in line for line in out)
 
 
-def test_levmar_is_refused(ptk, tmp_path):
-    (tmp_path / "start.txt").write_text("1\n10 20 0 12\n")
-    (tmp_path / "commands.txt").write_text("procedure correction_distortion\nstart_file start.txt\n"
-                                           "image_numbers_corrDisto 2 0 1\noptim_algo LEVMAR\n")
-    r = subprocess.run([str(ptk.cli_path()), "commands.txt"], capture_output=True, text=True, cwd=tmp_path, timeout=60)
-    assert r.returncode != 0 and "LEVMAR" in r.stderr
 
 
 @pytest.mark.parametrize("compression", ["tiff_lzw", "tiff_adobe_deflate", "tiff_deflate", "packbits"])

@@ -160,3 +160,50 @@ def test_bf16_full_frame_with_lm(ptk, wl, oracle, cuda_device, pair_cache):
     np.testing.assert_array_equal(gr[:, :2], cr[:, :2])
     assert np.abs(gr[:, 4:6] - cr[:, 4:6]).max() <= 0.01
     assert np.abs(gr[:, 6] - cr[:, 6]).max() <= 1e-4
+
+
+def test_bf16_wait_timeout_is_reported(ptk, wl, oracle, cuda_device, pair_cache):
+    """A bounded wait of the tensor-core search that runs out is reported by
+    ptk_synchronize as PTK_ERR_TIMEOUT, without a fault: the test hook makes the
+    kernel wait on a barrier nothing arrives on, before any copy or MMA is
+    issued, with a limit of 1000 polls.  Afterwards the same context (hook off)
+    and a fresh one track the pair as an untouched context does."""
+    pair = pair_cache("small16", 3)
+    p = pair["params"]
+    o = wl.tracker_options(p)
+
+    def make():
+        t = ptk.Tracker(p["dimx"], p["dimy"], rescue_level=o["rescue_level"], NCC_min=0.7, iraz=1 << 30,
+                        search_method=ptk.SEARCH_BF16, subpix_method=ptk.SUBPIX_ADJOINT_LM)
+        for lvl, z in enumerate(o["zones"]):
+            if z is not None:
+                t.set_zone(lvl, *z)
+        t.set_grains(pair["rec"])
+        t.make_patterns("grain_diameter", 1.0, 1.0)
+        t.load_frame(0, pair["ref"])
+        t.load_frame(1, pair["cur"])
+        return t
+
+    want = make()
+    want.track_frame(1)
+    expect = want.get_grains()
+    want.close()
+    L = ptk.lib()
+    t = make()
+    t.snapshot_grains()
+    assert L.ptk_test_bf16_wait_timeout(t.h, 1000) == ptk.PTK_OK
+    t.precompute()
+    t.search(0)
+    assert L.ptk_synchronize(t.h) == ptk.PTK_ERR_TIMEOUT
+    assert b"gave up" in L.ptk_last_error(t.h)
+    assert L.ptk_synchronize(t.h) == ptk.PTK_OK  # the flag is cleared once reported
+    assert L.ptk_test_bf16_wait_timeout(t.h, 0) == ptk.PTK_OK
+    t.restore_grains()
+    t.track_frame(1)
+    assert L.ptk_synchronize(t.h) == ptk.PTK_OK
+    np.testing.assert_array_equal(t.get_grains(), expect)
+    t.close()
+    fresh = make()
+    fresh.track_frame(1)
+    np.testing.assert_array_equal(fresh.get_grains(), expect)
+    fresh.close()

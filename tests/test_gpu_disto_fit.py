@@ -1,9 +1,9 @@
 """The distortion-parameter fit on the GPU (ptk_disto_*) against the CPU
 oracle: every residual of the equiprojectivity criterion bit for bit (the
 kernel is compiled without FMA contraction, as the CPU restatement), the
-criterion to 1e-12 (a different summation order), and the POWELL and
-POWELL_ITER minimisations on synthetic rigid motions seen through radial
-distortion."""
+criterion to 1e-12 (a different summation order), and the POWELL,
+POWELL_ITER and LEVMAR minimisations on synthetic rigid motions seen through
+radial distortion."""
 from __future__ import annotations
 
 import numpy as np
@@ -86,8 +86,33 @@ def test_fit_powell_iter_matches_oracle(ptk, oracle, cuda_device, data):
     f.close()
 
 
-def test_levmar_is_rejected(ptk, cuda_device, data):
-    f = _fit(ptk, data)
-    with pytest.raises(ptk.PtkError, match="LEVMAR"):
-        f.fit(np.zeros(14), np.full(14, 1e-6), ptk.DISTO_LEVMAR)
+def test_fit_levmar_matches_minpack(ptk, oracle, cuda_device, data):
+    """LEVMAR: all 14 parameters by Levenberg-Marquardt over the GPU residual
+    vector, against MINPACK's lmdif (scipy) over the oracle's residuals, which
+    the GPU's equal bit for bit, with lmdif1's settings and tol = DBL_EPSILON
+    as the reference passes: same exit state and evaluation count, same
+    parameters, and a criterion driven to zero (translations seen through the
+    lens are equiprojective at a perfect fit; with all 14 parameters free the
+    lens terms trade off against each other, as in the reference)."""
+    from scipy.optimize import leastsq
+
+    c = data
+    X0 = c["X"].copy()
+    X0[2] = 0.0
+    f = _fit(ptk, c)
+    x, ini, end, hist = f.fit(X0, np.zeros(14), ptk.DISTO_LEVMAR)
+    info, nfev, text = f.levmar_info()
     f.close()
+
+    def res(v):
+        return oracle.disto_objective(np.asarray(v), c["refx"], c["refy"], c["dx"], c["dy"], c["ncc"], 0.7,
+                                      c["pairs"], with_residuals=True)[1]
+
+    eps = float(np.finfo(float).eps)
+    xs, _, infod, msg, ier = leastsq(res, X0, full_output=True, ftol=eps, xtol=eps, gtol=0.0, maxfev=200 * 15,
+                                     epsfcn=0.0, factor=100.0)
+    assert info == ier and nfev == infod["nfev"], (info, ier, msg, nfev, infod["nfev"])
+    assert text
+    np.testing.assert_allclose(x, xs, rtol=1e-10, atol=1e-30)
+    assert hist.shape == (1, 15) and hist[0, 0] == end
+    assert end < 1e-18 * ini

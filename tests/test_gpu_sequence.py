@@ -27,6 +27,13 @@ def seq(wl):
     return s
 
 
+@pytest.fixture(scope="module")
+def long_seq(wl):
+    """24 frames (23 reference changes) of the same kind."""
+    p = dict(wl.PRESETS["cfg5"], dimx=1536, dimy=1024, n=80, shear=30.0, jump_frac=0.05)
+    return wl.make_sequence(p, seed=11, frames=24)
+
+
 def _track(ptk, wl, oracle, s, tol_px, **form):
     p = s["params"]
     o = wl.tracker_options(p)
@@ -70,3 +77,10 @@ def test_sequence_headline_form(ptk, wl, oracle, cuda_device, seq):
 
 def test_sequence_plain_form(ptk, wl, oracle, cuda_device, seq):
     _track(ptk, wl, oracle, seq, 1e-3)
+
+
+def test_long_sequence_plain_form(ptk, wl, oracle, cuda_device, long_seq):
+    """The plain form along 23 reference changes: every grain-frame within
+    1e-3 px and 1e-4 rad of the oracle (the device objective and Powell repeat
+    the reference's operations, so the two trajectories do not drift apart)."""
+    _track(ptk, wl, oracle, long_seq, 1e-3)
