@@ -126,6 +126,10 @@ struct ptk_ctx {
   unsigned char* d_bf_wslots{nullptr};  // BF16 weights of every rotation step, per grain
   size_t bf_wslots_bytes{0};
   bool bf_geom_dirty{true};            // patterns changed since the slots were laid out
+  std::vector<int> h_bf_half;          // host copies of the slot layout (tensor-map encoding)
+  std::vector<size_t> h_bf_wofs;
+  CUtensorMap* d_bf_tmaps[3]{nullptr, nullptr, nullptr};  // per level: each grain's operand-row tensor map
+  int bf_tmaps_nrot[3]{0, 0, 0};                           // rotation steps they were encoded for (0: stale)
   int2* d_topk{nullptr};
   unsigned* d_topk_rot{nullptr};  // rotation steps of each kept candidate to rescore
   float* d_tile_top{nullptr};     // best ranking score of each (grain, tile)
@@ -456,6 +460,13 @@ int ensure_bf16(ptk_ctx* c, size_t items) {
     CK(cudaMalloc(&c->d_bf_wofs, sizeof(size_t) * wofs.size()));
     CK(cudaMemcpy(c->d_bf_half, half.data(), sizeof(int) * half.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c->d_bf_wofs, wofs.data(), sizeof(size_t) * wofs.size(), cudaMemcpyHostToDevice));
+    c->h_bf_half = half;
+    c->h_bf_wofs = wofs;
+    for (int l = 0; l < 3; ++l) {  // the slots move (and the grain count may change): encode the maps again
+      cudaFree(c->d_bf_tmaps[l]);
+      c->d_bf_tmaps[l] = nullptr;
+      c->bf_tmaps_nrot[l] = 0;
+    }
     const size_t bytes = std::max<size_t>(total, 1) * 16;
     if (bytes > c->bf_wslots_bytes) {
       cudaFree(c->d_bf_wslots);
@@ -489,6 +500,23 @@ int ensure_bf16(ptk_ctx* c, size_t items) {
   return PTK_OK;
 }
 
+// Tensor maps of the grains' operand slots for a BF16 level (its rotation
+// step count decides the slots' layout), encoded on the host when the slots
+// were laid out anew or the level's step count changed.
+int ensure_bf16_tmaps(ptk_ctx* c, int level, int nrot) {
+  if (c->bf_tmaps_nrot[level] == nrot && c->d_bf_tmaps[level]) return PTK_OK;
+  const int n = c->n > 0 ? c->n : 1;
+  std::vector<CUtensorMap> maps((size_t)n);
+  std::memset(static_cast<void*>(maps.data()), 0, sizeof(CUtensorMap) * maps.size());
+  if (c->n > 0 && !bf16_encode_tmaps(c->h_bf_half.data(), c->h_bf_wofs.data(), c->n, c->d_bf_wslots, nrot,
+                                     maps.data()))
+    return fail(c, PTK_ERR_CUDA, "cuTensorMapEncodeTiled refused the BF16 operand maps");
+  if (!c->d_bf_tmaps[level]) CK(cudaMalloc(&c->d_bf_tmaps[level], sizeof(CUtensorMap) * (size_t)n));
+  CK(cudaMemcpy(c->d_bf_tmaps[level], maps.data(), sizeof(CUtensorMap) * (size_t)n, cudaMemcpyHostToDevice));
+  c->bf_tmaps_nrot[level] = nrot;
+  return PTK_OK;
+}
+
 // A BF16 level also needs the exact kernels' scratch: the grains it rejects
 // are searched again exactly.
 int ensure_search_scratch(ptk_ctx* c, int level, const SearchGeom& sg) {
@@ -497,7 +525,8 @@ int ensure_search_scratch(ptk_ctx* c, int level, const SearchGeom& sg) {
   int rc = search_geometry(c, level, &sx, false);
   if (rc) return rc;
   if ((rc = ensure_best(c, sx.items))) return rc;
-  return ensure_bf16(c, sg.items);
+  if ((rc = ensure_bf16(c, sg.items))) return rc;
+  return ensure_bf16_tmaps(c, level, sg.nrot);
 }
 
 // Kernels one search level launches (finalizes included): BF16 weights,
@@ -555,6 +584,7 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
     b.half = c->d_bf_half;
     b.wofs = c->d_bf_wofs;
     b.wslots = c->d_bf_wslots;
+    b.tmaps = c->d_bf_tmaps[level];
     b.topk = c->d_topk;
     b.topk_rot = c->d_topk_rot;
     b.tile_top = c->d_tile_top;
@@ -776,6 +806,7 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_bf_half);
   cudaFree(c->d_bf_wofs);
   cudaFree(c->d_bf_wslots);
+  for (int l = 0; l < 3; ++l) cudaFree(c->d_bf_tmaps[l]);
   cudaFree(c->d_topk);
   cudaFree(c->d_topk_rot);
   cudaFree(c->d_tile_top);

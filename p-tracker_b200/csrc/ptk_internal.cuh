@@ -2,6 +2,7 @@
 // sm_100a tracking path.  Not part of the public ABI (include/ptk.h).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -112,7 +113,8 @@ struct Bf16Launch {
   int max_items;            // list capacity x tiles: grid of the per-tile kernels
   const int* half;          // per grain: footprint half-extent ceil(max |offset|) + 1
   const size_t* wofs;       // per grain: offset of its weight slot in wslots (16-byte units)
-  unsigned char* wslots;    // BF16 weights of every rotation step, per grain
+  unsigned char* wslots;    // BF16 weights of the level's rotation steps, per grain
+  const CUtensorMap* tmaps; // per grain: tensor map of its operand rows (bf16_encode_tmaps)
   int2* topk;               // [list entry][tile][kBf16KeepMax] kept (u, v), INT_MIN when none
   unsigned* topk_rot;       // same layout: bit r = rotation step r is rescored at that candidate
   int ring;                 // operand-row buffers of the search kernel's ring (2..8; the strips take the rest)
@@ -163,6 +165,8 @@ bool bf16_supported(int max_r, int nrot, int max_dup);
 bool bf16_ring_ok(int max_half, int ring);
 constexpr int kBf16RingDefault = 4;
 size_t bf16_weight_entries(int half);
+bool bf16_encode_tmaps(const int* half, const size_t* wofs, int n, unsigned char* wslots, int nrot,
+                       CUtensorMap* out);
 void prepare_search_bf16();
 // ev (optional, 5 events): recorded before the first kernel and after each of the four
 // frame_ready (may be null): an event the search waits for after the weights

@@ -70,9 +70,12 @@
 // (footprint side <= 95), at most 32 rotation steps, no offset repeated more
 // than 63 times within a pattern.
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <climits>
+#include <mutex>
 
 #include "ptk_internal.cuh"
 
@@ -192,6 +195,18 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
       : "memory");
 }
 
+// One box of a 5-D tensor map global -> shared (TMA, tiled, no multicast):
+// coordinates innermost first; elements outside the tensor are filled with
+// zeros and count toward the transaction bytes.
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* tmap, int c0, int c1, int c2, int c3,
+                                            int c4, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+      "%6}], [%7];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(mbar)
+      : "memory");
+}
+
 // 16-byte asynchronous copy global -> shared through L2 (per thread).
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
@@ -284,8 +299,11 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
   if (G.fw >= kMaxFoot) return;  // excluded by the host's geometry check
   const int tid = threadIdx.x;
   const int rows = G.fw * G.nbf;
+  // [W / M][footprint row][8-column block][live rotation step][8 values]:
+  // only the level's nrot steps are stored; the search kernel's tensor map
+  // zero-fills the other rotation slots of its A operands
   uint4* slotW = reinterpret_cast<uint4*>(p.wslots) + p.wofs[gi];
-  uint4* slotM = slotW + (size_t)rows * kNRot;
+  uint4* slotM = slotW + (size_t)rows * p.nrot;
   __shared__ int s_rlo[kMaxFoot], s_rhi[kMaxFoot];
   if (tid < G.fw) {
     s_rlo[tid] = INT_MAX;
@@ -366,7 +384,7 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
           atomicMax(&s_rhi[y], hi);
         }
       }
-      const size_t at = (size_t)rem * kNRot + r0 + k;
+      const size_t at = (size_t)rem * p.nrot + r0 + k;
       slotW[at] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
                              pack_bf16x2(v[6], v[7]));
       slotM[at] = make_uint4(pack_bf16x2(m[0], m[1]), pack_bf16x2(m[2], m[3]), pack_bf16x2(m[4], m[5]),
@@ -376,7 +394,7 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
   }
   // per footprint row: the first and last 8-column block holding a point of
   // any rotation step (an empty row: first > last)
-  unsigned char* rng = reinterpret_cast<unsigned char*>(slotM + (size_t)rows * kNRot);
+  unsigned char* rng = reinterpret_cast<unsigned char*>(slotM + (size_t)rows * p.nrot);
   if (tid < G.fw) {
     rng[2 * tid] = (unsigned char)min(s_rlo[tid], 255);
     rng[2 * tid + 1] = (unsigned char)max(s_rhi[tid], 0);
@@ -432,6 +450,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = s_tmem;
   uint32_t parity = 0;  // thread 0: parity of the next MMA-completion phase of s_mbar
+  if (tid == 0 && (smem_u32(smem_bf) & 127u)) {
+    // the operand rows' TMA boxes land on 512-byte multiples from here: the
+    // dynamic shared memory must start 128-byte aligned (never seen otherwise)
+    s_err = 1;
+    atomicOr(p.error, 1);
+  }
   if (p.probe_wait > 0 && tid == 0) {
     // Failure-path test: a bounded wait that runs out (no copy or MMA has been
     // issued yet), reported exactly as a real one.
@@ -481,10 +505,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     const float mean0 = (float)g.mean0[gi];
     const float c00_rsqrt = g.c0c0[gi] > 0.0 ? (float)(1.0 / sqrt(g.c0c0[gi])) : 0.0f;
     const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
-    const size_t wrows = (size_t)G.fw * G.nbf * kNRot;
+    const size_t wrows = (size_t)G.fw * G.nbf * p.nrot;
     const uint4* slotW = reinterpret_cast<const uint4*>(p.wslots) + p.wofs[gi];
     const uint4* slotM = slotW + wrows;
     if (tid < 2 * G.fw) s_rng[tid] = reinterpret_cast<const unsigned char*>(slotM + wrows)[tid];
+    const CUtensorMap* tmap = p.tmaps + gi;  // this grain's operand rows, rotation slots zero-filled to 32
+    if (tid == 0) asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
     // ring buffer k: W row at k * 2 wb * 512, M row wb * 512 after it
     const size_t hbytes = (size_t)(G.rs + 31) * G.hb * 128;
     unsigned char* sA = smem;
@@ -597,9 +623,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
         const uint32_t full = smem_u32(&s_full[k]);
         mbar_expect_tx(full, (uint32_t)(2 * G.nbf * 512));
         const uint32_t dst = abase + (uint32_t)(k * 2 * G.wb * 512 + 3 * 512);
-        const size_t src = (size_t)y * G.nbf * kNRot;
-        bulk_g2s(dst, slotW + src, (uint32_t)(G.nbf * 512), full);
-        bulk_g2s(dst + (uint32_t)(G.wb * 512), slotM + src, (uint32_t)(G.nbf * 512), full);
+        // footprint row y of W (coordinate 4 = 0) and of M (1): nbf blocks of
+        // 32 rotation slots x 8 values, 512 bytes per block
+        tma_load_5d(dst, tmap, 0, 0, 0, y, 0, full);
+        tma_load_5d(dst + (uint32_t)(G.wb * 512), tmap, 0, 0, 0, y, 1, full);
         s_iss[k] = use + 1;
         return true;
       };
@@ -1095,6 +1122,48 @@ void prepare_search_bf16() {
   ensure_smem((const void*)k_search_bf16<6>, kSmemBudget);
   ensure_smem((const void*)k_weights_bf16, kWSmem);
   ensure_smem((const void*)k_rescore_bf16, kRescoreSmem);
+}
+
+// Tensor maps of the grains' operand slots for a level with `nrot` rotation
+// steps (host): per grain a 5-D BF16 tensor {8 values, nrot steps, nbf blocks,
+// fw rows, W/M} at its slot, read one footprint row at a time as a box
+// {8, 32, nbf, 1, 1} - the 32 - nrot slots beyond the tensor come back as
+// zeros, in the shared-memory layout of the A operands.  Returns false when
+// the driver's encoder is unavailable or refuses a map.
+bool bf16_encode_tmaps(const int* half, const size_t* wofs, int n, unsigned char* wslots, int nrot,
+                       CUtensorMap* out) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  if (!encode || nrot < 1 || nrot > kNRot) return false;
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  for (int i = 0; i < n; ++i) {
+    const Geom G = geom_of(half[i]);
+    if (G.fw >= kMaxFoot) {  // never searched by the BF16 kernels (bf16_supported): a small valid map
+      const cuuint64_t d1[5] = {8, 1, 1, 1, 1};
+      const cuuint64_t s1[4] = {16, 16, 16, 16};
+      const cuuint32_t b1[5] = {8, 1, 1, 1, 1};
+      if (encode(&out[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, wslots + wofs[i] * 16, d1, s1, b1, estr,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+      continue;
+    }
+    const cuuint64_t dims[5] = {8, (cuuint64_t)nrot, (cuuint64_t)G.nbf, (cuuint64_t)G.fw, 2};
+    const cuuint64_t strides[4] = {16, 16ull * nrot, 16ull * nrot * G.nbf, 16ull * nrot * G.nbf * G.fw};
+    const cuuint32_t box[5] = {8, (cuuint32_t)kNRot, (cuuint32_t)G.nbf, 1, 1};
+    if (encode(&out[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, wslots + wofs[i] * 16, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  return true;
 }
 
 void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent_t* ev, cudaEvent_t frame_ready) {
