@@ -115,7 +115,7 @@ struct ptk_ctx {
 
   // lists: counts[0] = n (level-0 list), counts[1] rescue, counts[2] super-rescue
   int* d_counts{nullptr};
-  int* d_lists{nullptr};  // [rescue n][super n][exact re-search n]
+  int* d_lists{nullptr};  // [rescue n][super n][exact re-search n][LM refinements that left their cell n]
   int* d_work{nullptr};
   SearchBest* d_best{nullptr};
   size_t best_cap{0};
@@ -652,7 +652,18 @@ int enqueue_subpixel(ptk_ctx* c, int method, cudaStream_t s) {
     lp.iters = nullptr;
     lp.order = c->d_order;
     lp.max_r = c->max_R;
+    // the cell of the integer optimum: half a pixel, half a level-0 rotation step
+    lp.redo_list = c->d_lists + 3 * (size_t)c->n;
+    lp.redo_count = c->d_counts + 7;
+    lp.cell_px = 0.5;
+    const ptk_zone& z0 = c->cfg.zone[0];
+    lp.cell_rot = (c->cfg.rotations != 0 && z0.num_rot != 0 && z0.inc_rot > 0.0) ? 0.5 * z0.inc_rot : HUGE_VAL;
+    CK(cudaMemsetAsync(lp.redo_count, 0, sizeof(int), s));
     launch_subpix_lm(c->g, frame(c, c->cur_slot), lp, s);
+    // those grains: the reference's Powell from their pixel-stage state
+    launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, c->max_R,
+                         lp.redo_list, s, lp.redo_count);
+    c->launches += 1;
   } else if (method == PTK_SUBPIX_POWELL) {
     launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, c->max_R,
                          c->d_order, s);
@@ -866,7 +877,7 @@ int ptk_set_grains(ptk_ctx* c, const ptk_grain* grains, int n) {
     c->n = n;
     BlockLayout L(n);
     CK(cudaMalloc(&c->d_block, L.total));
-    CK(cudaMalloc(&c->d_lists, sizeof(int) * 3 * (n > 0 ? n : 1)));
+    CK(cudaMalloc(&c->d_lists, sizeof(int) * 4 * (n > 0 ? n : 1)));
     c->h_pat.assign(n, std::vector<short2>());
     c->patterns_ok = false;
     cudaFree(c->d_best);

@@ -139,6 +139,10 @@ struct LmParams {
   int* iters;   // optional per-grain iteration count
   const int* order;  // grains by decreasing pattern size (one block each), or null for index order
   int max_r;         // largest pattern radius (sizes the staged frame region)
+  int* redo_list;    // grains whose refinement left the cell (for Powell), or null to keep every result
+  int* redo_count;   // their number (zeroed before the launch)
+  double cell_px;    // cell of the integer optimum: |dx|, |dy| <= cell_px
+  double cell_rot;   // and |drot| <= cell_rot
 };
 
 // Raises `func`'s dynamic shared-memory limit to at least `bytes` on the
@@ -175,9 +179,12 @@ void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent
                         cudaEvent_t frame_ready = nullptr);
 void launch_end_frame(const GrainsDev& g, int swap_reference, cudaStream_t s);
 void prepare_subpix(int max_points, int max_r);
-// order: grains by decreasing pattern size (one block each), or null for index order
+// order: grains by decreasing pattern size (one block each), or null for index
+// order; with list_count, only the first *list_count entries of `order` (a
+// device-built list) are refined
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& ref,
-                          const SubpixParams& sp, int max_points, int max_r, const int* order, cudaStream_t s);
+                          const SubpixParams& sp, int max_points, int max_r, const int* order, cudaStream_t s,
+                          const int* list_count = nullptr);
 void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const double* X,
                       double* f, double* grad, int max_points, cudaStream_t s);
 void launch_widen_u8(const uint8_t* src, size_t src_pitch, uint16_t* dst, int dst_pitch, int dimx, int dimy,

@@ -909,28 +909,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
 //    the search marked for each (those within the keep margin of the
 //    candidate's best step), with the exact search's integer sums and NCC
 //    expression; tiles of a multi-tile zone whose best score is more than the
-//    weak keep margin below the grain's best tile are not rescored.  One block
-//    per (grain, tile).  The frame region under every kept candidate's
-//    rotated footprints is staged in shared memory first; a work unit is one
-//    rotation step for all the candidates that need it, taken by one warp
-//    whose lanes share the pattern points (the rotation of a point is computed
-//    once per step); per candidate the best record over its rotation steps in
-//    the reference's order.
-constexpr int kRescoreThreads = 256;
-constexpr int kRescoreWarps = kRescoreThreads / 32;
-// region side: a 32-candidate spread plus the rotated footprint (|q| <= 47)
-constexpr int kRescoreSide = 32 + 2 * 47;
-constexpr int kRescoreSmem = kRescoreSide * kRescoreSide * 2;
-
-__global__ void __launch_bounds__(kRescoreThreads, 2) k_rescore_bf16(Bf16Launch p) {
-  extern __shared__ __align__(16) unsigned char smem_rs[];
-  uint16_t* s_reg = reinterpret_cast<uint16_t*>(smem_rs);
-  __shared__ double s_bn[kBf16KeepMax][kRescoreWarps];
-  __shared__ int s_bi[kBf16KeepMax][kRescoreWarps];
+//    weak keep margin below the grain's best tile are not rescored.  One block per (grain, tile); a work unit is one rotation
+//    step for two candidates that both need it (or one), taken by one warp
+//    whose lanes share the pattern points; per candidate the best record over
+//    its rotation steps in the reference's order.
+__global__ void __launch_bounds__(256, 4) k_rescore_bf16(Bf16Launch p) {
+  constexpr int kW = 8;
+  __shared__ double s_bn[kBf16KeepMax][kW];
+  __shared__ int s_bi[kBf16KeepMax][kW];
   __shared__ int s_base[kBf16KeepMax], s_uv[kBf16KeepMax];
-  __shared__ unsigned s_rm[kBf16KeepMax];
-  __shared__ int s_nk, s_nu, s_rx0, s_ry0, s_rw, s_rh;
-  __shared__ int s_unit[kNRot];  // rotation step | candidates needing it << 8
+  __shared__ int s_nk, s_nu;
+  __shared__ int s_unit[kNRot * kBf16KeepMax / 2];  // rotation | first candidate << 8 | second << 16 (255: none)
   const int item = blockIdx.x;
   const int tiles = p.tiles_u * p.tiles_v;
   const int li = item / tiles;
@@ -949,7 +938,7 @@ __global__ void __launch_bounds__(kRescoreThreads, 2) k_rescore_bf16(Bf16Launch 
   const int b = g.pstart[gi], P = g.pstart[gi + 1] - b;
   const bool skip = g.masked[gi] || (g.flags[gi] & 7) || P <= 0 || P > kMaxPatternPoints;
   const int NU = p.left + p.right + 1, NV = p.up + p.down + 1;
-  if (tid == 0) {  // the kept candidates, compacted, the staged region and the work units
+  if (tid == 0) {  // the kept candidates, compacted: anchor pixel index and order index without the rotation
     int nk = 0, nu = 0;
     // a tile whose best score lies further below the grain's best tile than
     // the weak keep margin cannot hold the exact best (the keep rule's bound)
@@ -964,46 +953,36 @@ __global__ void __launch_bounds__(kRescoreThreads, 2) k_rescore_bf16(Bf16Launch 
       const int2* cand = p.topk + (size_t)item * kBf16KeepMax;
       const unsigned* rots = p.topk_rot + (size_t)item * kBf16KeepMax;
       const int gdx = (int)round(g.dx[gi]), gdy = (int)round(g.dy[gi]);
-      const int X = g.refx[gi] + gdx, Y = g.refy[gi] + gdy;
-      int2 cu[kBf16KeepMax];
-      int umn = INT_MAX, umx = INT_MIN, vmn = INT_MAX, vmx = INT_MIN;
+      unsigned rm[kBf16KeepMax];
       for (int k = 0; k < p.keep && k < kBf16KeepMax; ++k) {
         const int2 c = cand[k];
         if (c.x == INT_MIN) continue;
-        cu[nk] = c;
+        s_base[nk] = (g.refy[gi] + gdy + c.y) * p.cur.pitch + (g.refx[gi] + gdx + c.x);
         s_uv[nk] = (c.x + p.left) * NV + (c.y + p.up);
-        s_rm[nk] = rots[k];
-        umn = min(umn, c.x);
-        umx = max(umx, c.x);
-        vmn = min(vmn, c.y);
-        vmx = max(vmx, c.y);
+        rm[nk] = rots[k];
         ++nk;
       }
-      if (nk > 0) {
-        // every rotated point lies within half - 1 of the anchor; the tile's
-        // footprints were checked to stay in the frame by the search
-        const int e = p.half[gi] - 1;
-        const int x0 = max(X + umn - e, 0), y0 = max(Y + vmn - e, 0);
-        const int x1 = min(X + umx + e, p.cur.dimx - 1), y1 = min(Y + vmx + e, p.cur.dimy - 1);
-        s_rx0 = x0;
-        s_ry0 = y0;
-        s_rw = x1 - x0 + 1;
-        s_rh = y1 - y0 + 1;
-        for (int k = 0; k < nk; ++k) s_base[k] = (Y + cu[k].y - y0) * s_rw + (X + cu[k].x - x0);
-        // units: per rotation step, the candidates that need it
-        for (int r = 0; r < p.nrot; ++r) {
-          unsigned who = 0u;
-          for (int k = 0; k < nk; ++k) who |= ((s_rm[k] >> r) & 1u) << k;
-          if (who) s_unit[nu++] = r | (int)(who << 8);
+      // units: per rotation step, the candidates that need it, two at a time
+      for (int r = 0; r < p.nrot; ++r) {
+        int first = -1;
+        for (int k = 0; k < nk; ++k) {
+          if (!((rm[k] >> r) & 1u)) continue;
+          if (first < 0) {
+            first = k;
+          } else {
+            s_unit[nu++] = r | (first << 8) | (k << 16);
+            first = -1;
+          }
         }
+        if (first >= 0) s_unit[nu++] = r | (first << 8) | (255 << 16);
       }
     }
     s_nk = nk;
     s_nu = nu;
   }
-  if (tid < kBf16KeepMax * kRescoreWarps) {
-    s_bn[tid / kRescoreWarps][tid % kRescoreWarps] = 0.0;
-    s_bi[tid / kRescoreWarps][tid % kRescoreWarps] = INT_MAX;
+  if (tid < kBf16KeepMax * kW) {
+    s_bn[tid / kW][tid % kW] = 0.0;
+    s_bi[tid / kW][tid % kW] = INT_MAX;
   }
   __syncthreads();
   const int nk = s_nk;
@@ -1011,71 +990,58 @@ __global__ void __launch_bounds__(kRescoreThreads, 2) k_rescore_bf16(Bf16Launch 
     if (tid < kBf16KeepMax) rec[tid] = SearchBest{0.0, INT_MAX, 0};
     return;
   }
-  {  // stage the region: one row per warp pass, lanes along the row
-    const int rw = s_rw, rh = s_rh, x0 = s_rx0, y0 = s_ry0;
-    for (int row = warp; row < rh; row += kRescoreWarps) {
-      const uint16_t* src = p.cur.pix + (size_t)(y0 + row) * p.cur.pitch + x0;
-      uint16_t* dst = s_reg + row * rw;
-      for (int x = lane; x < rw; x += 32) dst[x] = __ldg(src + x);
-    }
-  }
-  __syncthreads();
   const long long Pl = P, S0 = g.s0[gi];
   const double den1 = (double)(Pl * g.s00[gi] - S0 * S0);
-  const int rw = s_rw;
+  const int pitch = p.cur.pitch;
   const double base_rot = g.refrot[gi] + g.drot[gi];
   const int nu = s_nu;
-  for (int u = warp; u < nu; u += kRescoreWarps) {
+  for (int u = warp; u < nu; u += kW) {
     const int unit = s_unit[u];
-    const int r = unit & 0xff;
-    const unsigned who = (unsigned)unit >> 8;
+    const int r = unit & 0xff, k0 = (unit >> 8) & 0xff, k1 = (unit >> 16) & 0xff;
     double sr, cr;
     sincos(base_rot + p.steps[r], &sr, &cr);
     const float cf = (float)cr, sf = (float)sr;
-    int base[kBf16KeepMax];
-#pragma unroll
-    for (int k = 0; k < kBf16KeepMax; ++k) base[k] = s_base[k < nk ? k : 0];
-    unsigned s1[kBf16KeepMax];
-    unsigned long long s11[kBf16KeepMax], s01[kBf16KeepMax];
-#pragma unroll
-    for (int k = 0; k < kBf16KeepMax; ++k) {
-      s1[k] = 0u;
-      s11[k] = 0ull;
-      s01[k] = 0ull;
-    }
-#pragma unroll 2
+    const bool two = k1 != 255;
+    const uint16_t* pa = p.cur.pix + s_base[k0];
+    const uint16_t* pb = p.cur.pix + s_base[two ? k1 : k0];
+    unsigned s1a = 0, s1b = 0;
+    unsigned long long s11a = 0, s11b = 0, s01a = 0, s01b = 0;
+#pragma unroll 4
     for (int i = lane; i < P; i += 32) {
       const short2 q = rotate_round_fast(g.pat[b + i], cf, sf, cr, sr);
-      const int o = (int)q.y * rw + (int)q.x;
+      const int o = (int)q.y * pitch + (int)q.x;
       const unsigned w = g.w0[b + i];
-#pragma unroll
-      for (int k = 0; k < kBf16KeepMax; ++k) {
-        if (!((who >> k) & 1u)) continue;
-        const unsigned v = s_reg[base[k] + o];
-        s1[k] += v;
-        s11[k] += (unsigned long long)(v * v);
-        s01[k] += (unsigned long long)(w * v);
+      const unsigned va = __ldg(pa + o);
+      s1a += va;
+      s11a += (unsigned long long)(va * va);
+      s01a += (unsigned long long)(w * va);
+      if (two) {
+        const unsigned vb = __ldg(pb + o);
+        s1b += vb;
+        s11b += (unsigned long long)(vb * vb);
+        s01b += (unsigned long long)(w * vb);
       }
     }
-#pragma unroll
-    for (int k = 0; k < kBf16KeepMax; ++k) {
-      if (!((who >> k) & 1u)) continue;
-      unsigned long long a = s1[k], c = s11[k], d = s01[k];
-      for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_xor_sync(0xffffffffu, a, o);
-        c += __shfl_xor_sync(0xffffffffu, c, o);
-        d += __shfl_xor_sync(0xffffffffu, d, o);
-      }
-      if (lane == 0) {
-        const long long S1 = (long long)a, S11 = (long long)c, S01 = (long long)d;
-        const long long num = Pl * S01 - S0 * S1;
-        const long long d2 = Pl * S11 - S1 * S1;
-        const double ncc = (double)num / sqrt(den1 * (double)d2);
-        const int idx = r * NU * NV + s_uv[k];
-        if (better_b(ncc, idx, s_bn[k][warp], s_bi[k][warp])) {
-          s_bn[k][warp] = ncc;
-          s_bi[k][warp] = idx;
-        }
+    unsigned long long a0 = s1a, c0 = s11a, d0 = s01a, a1 = s1b, c1 = s11b, d1 = s01b;
+    for (int o = 16; o > 0; o >>= 1) {
+      a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+      c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+      d0 += __shfl_xor_sync(0xffffffffu, d0, o);
+      a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+      c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+      d1 += __shfl_xor_sync(0xffffffffu, d1, o);
+    }
+    if (lane < 2 && (lane == 0 || two)) {
+      const int k = lane == 0 ? k0 : k1;
+      const long long S1 = (long long)(lane == 0 ? a0 : a1), S11 = (long long)(lane == 0 ? c0 : c1);
+      const long long S01 = (long long)(lane == 0 ? d0 : d1);
+      const long long num = Pl * S01 - S0 * S1;
+      const long long d2 = Pl * S11 - S1 * S1;
+      const double ncc = (double)num / sqrt(den1 * (double)d2);
+      const int idx = r * NU * NV + s_uv[k];
+      if (better_b(ncc, idx, s_bn[k][warp], s_bi[k][warp])) {
+        s_bn[k][warp] = ncc;
+        s_bi[k][warp] = idx;
       }
     }
   }
@@ -1083,7 +1049,7 @@ __global__ void __launch_bounds__(kRescoreThreads, 2) k_rescore_bf16(Bf16Launch 
   if (tid < kBf16KeepMax) {
     double fn = 0.0;
     int fi = INT_MAX;
-    for (int w = 0; w < kRescoreWarps; ++w)
+    for (int w = 0; w < kW; ++w)
       if (better_b(s_bn[tid][w], s_bi[tid][w], fn, fi)) {
         fn = s_bn[tid][w];
         fi = s_bi[tid][w];
@@ -1121,7 +1087,6 @@ void prepare_search_bf16() {
   ensure_smem((const void*)k_search_bf16<4>, kSmemBudget);
   ensure_smem((const void*)k_search_bf16<6>, kSmemBudget);
   ensure_smem((const void*)k_weights_bf16, kWSmem);
-  ensure_smem((const void*)k_rescore_bf16, kRescoreSmem);
 }
 
 // Tensor maps of the grains' operand slots for a level with `nrot` rotation
@@ -1180,7 +1145,7 @@ void launch_search_bf16(const Bf16Launch& p, int grid, cudaStream_t s, cudaEvent
     default: k_search_bf16<4><<<grid, kThreads, kSmemBudget, s>>>(p); break;
   }
   if (ev) cudaEventRecord(ev[2], s);
-  k_rescore_bf16<<<items, kRescoreThreads, kRescoreSmem, s>>>(p);
+  k_rescore_bf16<<<items, 256, 0, s>>>(p);
   if (ev) cudaEventRecord(ev[3], s);
 }
 

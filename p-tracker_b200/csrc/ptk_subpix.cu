@@ -1,12 +1,13 @@
 // Subpixel refinement on sm_100a: the NCC objective through image
 // interpolation, its adjoint gradient, and a per-grain Powell minimiser.
 //
-// The objective follows the reference's FP64 operations (src/p-tracker.cpp:
-// 1018-1088, src/interpol.cpp:19-144); the order of the sums over pattern
-// points (a block reduction here) and fused multiply-adds change values only
-// in the last bits.  Inside Powell, the objective is evaluated in one pass
-// with the samples centred on mean0 and the frame region under the grain
-// staged in shared memory.
+// The objective (objective_exact) follows the reference's FP64 operations
+// (src/p-tracker.cpp:1018-1088, src/interpol.cpp:19-144) in their order and
+// without FMA contraction (this file is compiled with -fmad=false); only its
+// three sums over the pattern points are taken in parallel and rounded once
+// (correctly rounded, where the reference rounds after every point), and
+// cos / sin come from ptk_crtrig.cuh.  Inside Powell the frame region under
+// the grain is staged in shared memory.
 //
 // One CTA of kSubpixThreads refines one grain.  The Powell driver
 // (follow_pattern_subpixel_xyR, src/p-tracker.cpp:1090-1128; the minimiser
@@ -183,7 +184,8 @@ __device__ __forceinline__ double patch_px(const Patch& pt, int x, int y) {
 struct ExactObj {
   double* vals;          // P samples
   const uint16_t* w0;    // P reference values (staged)
-  double* bcast;         // 8 doubles: [0] mean1, [1] C0C1, [2] C1C1, [3] cos, [4] sin
+  double* bcast;         // 8 doubles: [3] cos, [4] sin, [5] C0C0
+  double* red2;          // 2 doubles per warp: the block sums' partials
   double inv_num_pix;    // 1 / P
   double last_rot, c1, s1;
 };
@@ -199,19 +201,69 @@ __device__ double c0c0_in_order(const uint16_t* w0, int P, double mean0) {
   return c;
 }
 
-// NCC_to_minimize_xyR (src/p-tracker.cpp:1018-1088) with the reference's
-// operations in the reference's order, so that its value is the reference's
-// bit for bit whenever cos and sin of the angle are (the host C library's
-// cosine and sine are not always correctly rounded; ptk_crtrig.cuh's are):
-//   * sample positions xpix1 + c1 x + s1 y and ypix1 - s1 x + c1 y, the
-//     interpolators and the NCC expression with every product and sum rounded
-//     separately (this file is compiled without FMA contraction);
-//   * mean1 = sum of the samples in point order, times 1/P; C0C1 and C1C1
-//     summed in point order.  The samples are produced by the whole block;
-//     the three sums are sequential dependency chains run by one thread each
-//     (C0C1 and C1C1 on two warps at once).
-// Called by every thread of the block with the same X; returns the same value
-// on every thread.
+// Compensated summation (Ogita, Rump and Oishi, "Accurate sum and dot
+// product", SIAM J. Sci. Comput. 26 (2005), algorithm Sum2): s + c carries the
+// running sum to about twice the working precision, so the final s + c is the
+// exact sum rounded once (up to an error far below half an ulp), whatever the
+// order the terms come in.  Each step is Knuth's error-free two-sum; this file
+// is compiled without FMA contraction, which none of it uses anyway.
+struct Sum2 {
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add(double x) {
+    const double t = s + x;
+    const double bp = t - s;
+    c += (s - (t - bp)) + (x - bp);
+    s = t;
+  }
+  __device__ __forceinline__ void add(const Sum2& o) {
+    add(o.s);
+    c += o.c;
+  }
+};
+
+// The block's Sum2 partials combined in a fixed order (lanes by a butterfly,
+// then the warps in index order): every thread returns the same rounded sum.
+template <int NT>
+__device__ __forceinline__ double block_sum2(Sum2 v, double* red2) {
+  for (int o = 16; o > 0; o >>= 1) {
+    Sum2 w;
+    w.s = __shfl_xor_sync(0xffffffffu, v.s, o);
+    w.c = __shfl_xor_sync(0xffffffffu, v.c, o);
+    // both lanes of a pair combine the same two values in the same order
+    const bool lo = (threadIdx.x & o) == 0;
+    Sum2 a = lo ? v : w, b = lo ? w : v;
+    a.add(b);
+    v = a;
+  }
+  const int wp = threadIdx.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    red2[2 * wp] = v.s;
+    red2[2 * wp + 1] = v.c;
+  }
+  __syncthreads();
+  Sum2 t;
+#pragma unroll
+  for (int k = 0; k < NT / 32; ++k) {
+    Sum2 w;
+    w.s = red2[2 * k];
+    w.c = red2[2 * k + 1];
+    t.add(w);
+  }
+  return t.s + t.c;
+}
+
+// NCC_to_minimize_xyR (src/p-tracker.cpp:1018-1088): the reference's two-pass
+// arithmetic - sample positions xpix1 + c1 x + s1 y and ypix1 - s1 x + c1 y,
+// the interpolators, mean1 = (sum of the samples) / P, then C0C1 and C1C1 over
+// the centred values, every product and difference rounded separately (this
+// file is compiled without FMA contraction) - with each of the three sums
+// correctly rounded (Sum2 over the block) where the reference rounds after
+// every term in point order, and cos / sin of the angle correctly rounded
+// (ptk_crtrig.cuh) where the host C library is within an ulp.  The value
+// therefore differs from the reference's only by the reference's own rounding
+// of its sequential sums.  Called by every thread of the block with the same
+// X; returns the same value on every thread.
 template <int NT>
 __device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp,
                                   const ObjGrain& o, const Patch& pt, ExactObj& ex, const double X[3],
@@ -229,6 +281,7 @@ __device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const
     ex.last_rot = rot;
   }
   const double c1 = ex.c1, s1 = ex.s1;
+  Sum2 sv;
   for (int i = tid; i < o.P; i += NT) {
     const short2 q = g.pat0[o.b + i];
     const double x = (double)q.x, y = (double)q.y;
@@ -250,57 +303,20 @@ __device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const
     } else {
       v = interp(cur, sp.interp, xs, ys, clamped);
     }
-    ex.vals[i] = v;
+    ex.vals[i] = v;  // each thread reads back only its own samples
+    sv.add(v);
   }
-  __syncthreads();
-  if (tid == 0) {
-    const double* v = ex.vals;
-    double m = 0.0;
-    int i = 0;
-    for (; i + 4 <= o.P; i += 4) {
-      const double a = v[i], b = v[i + 1], c = v[i + 2], d = v[i + 3];
-      m += a;
-      m += b;
-      m += c;
-      m += d;
-    }
-    for (; i < o.P; ++i) m += v[i];
-    ex.bcast[0] = m * ex.inv_num_pix;
+  const double mean1 = block_sum2<NT>(sv, ex.red2) * ex.inv_num_pix;
+  Sum2 s01, s11;
+  for (int i = tid; i < o.P; i += NT) {
+    const double d1 = ex.vals[i] - mean1;
+    const double d0 = (double)ex.w0[i] - o.mean0;
+    s01.add(d0 * d1);
+    s11.add(d1 * d1);
   }
-  __syncthreads();
-  const double mean1 = ex.bcast[0];
-  if (tid == 0) {
-    const double* v = ex.vals;
-    const uint16_t* w = ex.w0;
-    double c01 = 0.0;
-    int i = 0;
-    for (; i + 2 <= o.P; i += 2) {
-      const double d1a = v[i] - mean1, d1b = v[i + 1] - mean1;
-      const double d0a = (double)w[i] - o.mean0, d0b = (double)w[i + 1] - o.mean0;
-      c01 += d0a * d1a;
-      c01 += d0b * d1b;
-    }
-    for (; i < o.P; ++i) c01 += ((double)w[i] - o.mean0) * (v[i] - mean1);
-    ex.bcast[1] = c01;
-  } else if (tid == 32) {
-    const double* v = ex.vals;
-    double c11 = 0.0;
-    int i = 0;
-    for (; i + 4 <= o.P; i += 4) {
-      const double a = v[i] - mean1, b = v[i + 1] - mean1, c = v[i + 2] - mean1, d = v[i + 3] - mean1;
-      c11 += a * a;
-      c11 += b * b;
-      c11 += c * c;
-      c11 += d * d;
-    }
-    for (; i < o.P; ++i) {
-      const double a = v[i] - mean1;
-      c11 += a * a;
-    }
-    ex.bcast[2] = c11;
-  }
-  __syncthreads();
-  const double ncc = ex.bcast[1] / sqrt(o.c0c0 * ex.bcast[2]);
+  const double c01 = block_sum2<NT>(s01, ex.red2);
+  const double c11 = block_sum2<NT>(s11, ex.red2);
+  const double ncc = c01 / sqrt(o.c0c0 * c11);
   double W = 1.0;
   const double disp = sqrt(X[0] * X[0] + X[1] * X[1]);
   if (disp > sp.disp_max) W = sp.stiffness * (disp - sp.disp_max) + 1.0;
@@ -576,10 +592,12 @@ __host__ __device__ inline size_t powell_vals_offset(int patch_cap) {
 // given.
 __global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, FrameDev cur, SubpixParams sp,
                                                                     int patch_cap, int max_points,
-                                                                    const int* order) {
+                                                                    const int* order, const int* list_count) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double bcast[8];
+  __shared__ double red2[2 * (kSubpixThreads / 32)];
   __shared__ int s_clamped, s_bb[4];
+  if (list_count && (int)blockIdx.x >= *list_count) return;
   const int gi = order ? order[blockIdx.x] : (int)blockIdx.x;
   if (g.masked[gi] || (g.flags[gi] & 3)) return;
   ObjGrain o = load_grain(g, gi);
@@ -623,7 +641,7 @@ __global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, F
   __syncthreads();
   o.c0c0 = bcast[5];
   const Patch pt{s_patch, px0, py0, pw, ph};
-  ExactObj ex{s_vals, s_w0, bcast, 1.0 / (double)o.P, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0};
+  ExactObj ex{s_vals, s_w0, bcast, red2, 1.0 / (double)o.P, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0};
   bool clamped = false;
   PowellEval<kSubpixThreads> f{&g, &cur, &sp, &o, &pt, &ex, &clamped, 0};
   double X[3] = {0.0, 0.0, 0.0};
@@ -651,6 +669,7 @@ __global__ void __launch_bounds__(kSubpixThreads) k_objective(GrainsDev g, Frame
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[kSubpixThreads / 32];
   __shared__ double bcast[8];
+  __shared__ double red2[2 * (kSubpixThreads / 32)];
   const int gi = blockIdx.x;
   ObjGrain o = load_grain(g, gi);
   if (o.P <= 0 || o.P > max_points) {
@@ -680,7 +699,7 @@ __global__ void __launch_bounds__(kSubpixThreads) k_objective(GrainsDev g, Frame
     __syncthreads();
     o.c0c0 = bcast[5];
     const Patch none{nullptr, 0, 0, 0, 0};
-    ExactObj ex{vals, s_w0, bcast, 1.0 / (double)o.P, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0};
+    ExactObj ex{vals, s_w0, bcast, red2, 1.0 / (double)o.P, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0};
     val = objective_exact<kSubpixThreads>(g, cur, sp, o, none, ex, X, &clamped);
   }
   if (threadIdx.x == 0) f[gi] = val;
@@ -708,11 +727,11 @@ void prepare_subpix(int max_points, int max_r) {
 }
 
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& /*ref*/, const SubpixParams& sp,
-                          int max_points, int max_r, const int* order, cudaStream_t s) {
+                          int max_points, int max_r, const int* order, cudaStream_t s, const int* list_count) {
   if (g.n <= 0) return;
   prepare_subpix(max_points, max_r);
   const PowellSmem m = powell_smem(max_points, max_r);
-  k_subpix_powell<<<g.n, kSubpixThreads, m.bytes, s>>>(g, cur, sp, m.patch_cap, max_points, order);
+  k_subpix_powell<<<g.n, kSubpixThreads, m.bytes, s>>>(g, cur, sp, m.patch_cap, max_points, order, list_count);
 }
 
 void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp, const double* X, double* f,

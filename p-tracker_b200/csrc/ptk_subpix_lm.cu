@@ -21,7 +21,11 @@
 // level-0 order) so that the large ones start first; the iteration stops when
 // the step is below the tolerance, or after two rejected steps in a row once
 // a step was accepted (the FP32 sums' noise floor: further steps only
-// re-sample it).
+// re-sample it).  A grain whose refinement ends outside the cell of its
+// integer optimum (more than half a pixel, or half a rotation step, away) is
+// left untouched and listed for the Powell kernel, which then refines it as
+// the reference does: there the objective has several maxima within reach and
+// the result depends on the minimiser's path.
 #include "ptk_internal.cuh"
 
 namespace ptk {
@@ -303,6 +307,13 @@ __global__ void __launch_bounds__(kLmThreads) k_subpix_lm(GrainsDev g, FrameDev 
         if (++rejected_run >= 2 && accepted > 0) break;
       }
     }
+  }
+  // Outside the cell of the integer optimum (the local quadratic model of the
+  // objective did not hold: another maximum attracted the steps), the grain
+  // keeps its pixel-stage state and goes to the reference's Powell.
+  if (lp.redo_list && (fabs(X[0]) > lp.cell_px || fabs(X[1]) > lp.cell_px || fabs(X[2]) > lp.cell_rot)) {
+    if (threadIdx.x == 0) lp.redo_list[atomicAdd(lp.redo_count, 1)] = gi;
+    return;
   }
   if (threadIdx.x == 0) {
     g.ncc_subpix[gi] = 1.0 - 0.5 * cur_e.F;

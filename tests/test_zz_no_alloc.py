@@ -101,38 +101,49 @@ def test_noalloc_matches_context_path(ptk, wl, cuda_device, pair_cache):
         np.testing.assert_array_equal(got_r, expect_rot, err_msg=f"call {call}: rotation steps differ")
 
 
-def _call(ptk, pair, rec, xy, starts, maxp, maxr, z, stream_ptr=None):
-    """One call through the C ABI on torch-owned device buffers; returns the
-    status and the four outputs on the host."""
+def _buffers(pair, rec, xy, starts):
+    """The entry point's inputs and outputs as torch-owned device buffers."""
     import torch
 
     dev = torch.device("cuda", 0)
     n = rec.shape[0]
-    ref = torch.from_numpy(np.ascontiguousarray(pair["ref"]).view(np.int16)).to(dev)
-    cur = torch.from_numpy(np.ascontiguousarray(pair["cur"]).view(np.int16)).to(dev)
-    ints = [torch.tensor(rec[:, k].astype(np.int32), device=dev) for k in (0, 1)]
-    dbl = [torch.tensor(rec[:, k], dtype=torch.float64, device=dev) for k in (2, 6, 4, 5)]
-    pxy, pst = torch.from_numpy(xy).to(dev), torch.from_numpy(starts).to(dev)
-    ncc = torch.full((n,), -7.0, dtype=torch.float64, device=dev)
-    bu = torch.full((n,), 12345, dtype=torch.int32, device=dev)
-    bv = torch.full((n,), 12345, dtype=torch.int32, device=dev)
-    br = torch.full((n,), 9.0, dtype=torch.float64, device=dev)
+    b = dict(
+        ref=torch.from_numpy(np.ascontiguousarray(pair["ref"]).view(np.int16)).to(dev),
+        cur=torch.from_numpy(np.ascontiguousarray(pair["cur"]).view(np.int16)).to(dev),
+        ints=[torch.tensor(rec[:, k].astype(np.int32), device=dev) for k in (0, 1)],
+        dbl=[torch.tensor(rec[:, k], dtype=torch.float64, device=dev) for k in (2, 6, 4, 5)],
+        pxy=torch.from_numpy(xy).to(dev), pst=torch.from_numpy(starts).to(dev),
+        ncc=torch.full((n,), -7.0, dtype=torch.float64, device=dev),
+        bu=torch.full((n,), 12345, dtype=torch.int32, device=dev),
+        bv=torch.full((n,), 12345, dtype=torch.int32, device=dev),
+        br=torch.full((n,), 9.0, dtype=torch.float64, device=dev))
+    torch.cuda.synchronize()
+    return b
+
+
+def _enqueue(ptk, pair, b, maxp, maxr, z):
+    """One call through the C ABI on the default stream; returns its status."""
     zone = ptk.Zone(*z)
     vp = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
-    rc = ptk.lib().ptk_search_pixel_noalloc(
-        vp(ref), vp(cur), ref.stride(0) * 2, pair["ref"].shape[1], pair["ref"].shape[0], n, vp(ints[0]),
-        vp(ints[1]), *[vp(t) for t in dbl], vp(pst), vp(pxy), maxp, maxr, C.byref(zone), 1, vp(ncc), vp(bu), vp(bv),
-        vp(br), C.c_void_p(stream_ptr if stream_ptr is not None else torch.cuda.current_stream().cuda_stream))
+    return ptk.lib().ptk_search_pixel_noalloc(
+        vp(b["ref"]), vp(b["cur"]), b["ref"].stride(0) * 2, pair["ref"].shape[1], pair["ref"].shape[0],
+        b["ncc"].shape[0], vp(b["ints"][0]), vp(b["ints"][1]), *[vp(t) for t in b["dbl"]], vp(b["pst"]),
+        vp(b["pxy"]), maxp, maxr, C.byref(zone), 1, vp(b["ncc"]), vp(b["bu"]), vp(b["bv"]), vp(b["br"]), None)
+
+
+def _results(b):
+    import torch
+
     torch.cuda.synchronize()
-    return rc, ncc.cpu().numpy(), bu.cpu().numpy(), bv.cpu().numpy(), br.cpu().numpy()
+    return b["ncc"].cpu().numpy(), b["bu"].cpu().numpy(), b["bv"].cpu().numpy(), b["br"].cpu().numpy()
 
 
 def test_noalloc_rect_pattern_limits(ptk, wl, cuda_device, pair_cache):
-    """A 25 x 13 rectangle at refrot 0.3 rad: its corners rotate to |x| = 13,
-    beyond its unrotated half-width 12.  With max_radius 15 (the Euclidean
-    radius 13.4, rounded up, plus one) the results equal the context path's;
-    with max_radius 12 every grain reports the caller-limit code
-    (NaN, INT_MIN + 1), not the frame-edge code."""
+    """A 25 x 17 rectangle at refrot 0.3 rad: its corners (Euclidean radius
+    14.4) rotate to |x| = 14 at every searched angle.  With max_radius 16 (the
+    radius rounded up, plus one) the results equal the context path's; with
+    max_radius 12 every grain reports the caller-limit code (NaN,
+    INT_MIN + 1), not the frame-edge code."""
     pair = dict(pair_cache("small16", 7))
     rec = pair["rec"].copy()
     rec[:, 2] = 0.3
@@ -142,7 +153,7 @@ def test_noalloc_rect_pattern_limits(ptk, wl, cuda_device, pair_cache):
     t = ptk.Tracker(p["dimx"], p["dimy"], rescue_level=0, NCC_min=-1.0)
     t.set_zone(0, *z)
     t.set_grains(rec)
-    t.make_patterns("rect", 12, 6)
+    t.make_patterns("rect", 12, 8)
     t.load_frame(0, pair["ref"])
     t.load_frame(1, pair["cur"])
     t.precompute()
@@ -150,13 +161,14 @@ def test_noalloc_rect_pattern_limits(ptk, wl, cuda_device, pair_cache):
     ctx = t.get_grains()
     st = t.status()
     t.close()
-    yy, xx = np.mgrid[-6:7, -12:13]
+    yy, xx = np.mgrid[-8:9, -12:13]
     one = np.stack([xx.ravel(), yy.ravel()], 1).astype(np.int16)  # rows of dy, then dx (make_rect_pattern)
     n = rec.shape[0]
     xy = np.concatenate([one] * n)
     starts = (np.arange(n + 1) * one.shape[0]).astype(np.int32)
-    rc, ncc, bu, bv, br = _call(ptk, pair, rec, xy, starts, one.shape[0], 15, z)
-    assert rc == 0
+    b = _buffers(pair, rec, xy, starts)
+    assert _enqueue(ptk, pair, b, one.shape[0], 16, z) == 0
+    ncc, bu, bv, br = _results(b)
     # grains both paths searched (a footprint at the frame edge is skipped by both)
     ok = (st == 0) & (bu > np.iinfo(np.int32).min + 1)
     assert ok.sum() > n // 2
@@ -164,8 +176,8 @@ def test_noalloc_rect_pattern_limits(ptk, wl, cuda_device, pair_cache):
     np.testing.assert_array_equal(bu[ok], (ctx[ok, 4] - gdx[ok]).round().astype(np.int64))
     np.testing.assert_array_equal(bv[ok], (ctx[ok, 5] - gdy[ok]).round().astype(np.int64))
     assert np.abs(ncc[ok] - ctx[ok, 10]).max() <= NCC_TOL
-    rc, ncc, bu, bv, br = _call(ptk, pair, rec, xy, starts, one.shape[0], 12, z)
-    assert rc == 0
+    assert _enqueue(ptk, pair, b, one.shape[0], 12, z) == 0
+    ncc, bu, bv, br = _results(b)
     assert np.isnan(ncc).all()
     assert (bu == np.iinfo(np.int32).min + 1).all() and (bv == np.iinfo(np.int32).min + 1).all()
 
@@ -173,26 +185,28 @@ def test_noalloc_rect_pattern_limits(ptk, wl, cuda_device, pair_cache):
 def test_noalloc_leaves_pending_error_alone(ptk, wl, cuda_device, pair_cache):
     """An error left pending in the calling thread by earlier, unrelated CUDA
     runtime work (here a cudaSetDevice to a device that does not exist, which
-    touches no GPU) is neither returned as this call's failure nor cleared."""
-    import torch
-
+    touches no GPU) is neither returned as this call's failure nor cleared.
+    The buffers are made before the error is planted and read after it is
+    cleared, so that no other library sees it."""
     rt = C.CDLL("libcudart.so.12")
     rt.cudaSetDevice.argtypes = [C.c_int]
-    torch.cuda.synchronize()
+    pair = pair_cache("small16", 7)
+    z = wl.tracker_options(pair["params"])["zones"][0]
+    xy, starts, maxp, maxr = _patterns(pair["rec"])
+    b = _buffers(pair, pair["rec"], xy, starts)
     rt.cudaGetLastError()
     assert rt.cudaSetDevice(1 << 20) != 0
     pending = rt.cudaPeekAtLastError()
     assert pending != 0
     try:
-        pair = pair_cache("small16", 7)
-        z = wl.tracker_options(pair["params"])["zones"][0]
-        xy, starts, maxp, maxr = _patterns(pair["rec"])
-        rc, ncc, *_ = _call(ptk, pair, pair["rec"], xy, starts, maxp, maxr, z)
-        assert rc == 0
-        assert np.isfinite(ncc).all()
-        assert rt.cudaPeekAtLastError() == pending
+        rc = _enqueue(ptk, pair, b, maxp, maxr, z)
+        still = rt.cudaPeekAtLastError()
     finally:
         rt.cudaGetLastError()
+    assert rc == 0
+    assert still == pending
+    ncc, *_ = _results(b)
+    assert np.isfinite(ncc).all()
 
 
 def test_noalloc_rejects_oversized_work(ptk, cuda_device):
