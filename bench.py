@@ -215,6 +215,18 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
+def recorded_traffic(summary: str):
+    """DRAM bytes (read + write) per launch of a kernel on the default
+    workload, as its committed ncu summary records them
+    (`traffic_bytes_per_launch: N`); None when there is none."""
+    import re
+    p = ROOT / "profiles" / summary
+    if not p.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
 def search_ppc(tracker, rec: np.ndarray, zone, nsteps: int) -> int:
     """Pattern-pixel-candidate evaluations of one pixel-stage search."""
     P = sum(tracker.pattern_size(g) for g in range(rec.shape[0]))
@@ -961,7 +973,10 @@ def main() -> int:
             "gpu_launches": int(launches),
             "roofline": {"kernel": "k_search_bf16 (tcgen05 candidate ranking)", "bound": "tensor",
                          "achieved": alg, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-                         "frac": alg / peaks["bf16_tflops"], "traffic": None,
+                         "frac": alg / peaks["bf16_tflops"],
+                         "traffic": recorded_traffic("k_search_bf16_cfg2.md") if args.workload == "cfg2" else None,
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of this "
+                                           "kernel on this workload (profiles/k_search_bf16_cfg2.md)",
                          "algorithmic_flop_per_launch": 6.0 * ppc, "ppc_per_launch": int(ppc),
                          "tensor_flop_per_launch": gemm_flops(pair["rec"]), "tensor_tflops": gemm,
                          "tensor_frac": gemm / peaks["bf16_tflops"], "launch_ms": k_search_ms,

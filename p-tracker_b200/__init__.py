@@ -52,7 +52,7 @@ class Config(C.Structure):
                 ("subpix_displacement_max", C.c_double), ("rotations", C.c_int32), ("zone", Zone * 3),
                 ("iraz", C.c_int32), ("subpix_method", C.c_int32), ("search_method", C.c_int32),
                 ("topk", C.c_int32), ("lm_max_iter", C.c_int32), ("lm_tol", C.c_double),
-                ("autotune", C.c_int32)]
+                ("autotune", C.c_int32), ("lm_cell_px", C.c_double), ("lm_cell_rot", C.c_double)]
 
 
 class TuneReport(C.Structure):

@@ -585,6 +585,8 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
     b.wofs = c->d_bf_wofs;
     b.wslots = c->d_bf_wslots;
     b.tmaps = c->d_bf_tmaps[level];
+    if (!b.tmaps || c->bf_tmaps_nrot[level] != sg.nrot)  // every caller prepares them first
+      return fail(c, PTK_ERR_STATE, "BF16 operand tensor maps missing for this level");
     b.topk = c->d_topk;
     b.topk_rot = c->d_topk_rot;
     b.tile_top = c->d_tile_top;
@@ -655,15 +657,19 @@ int enqueue_subpixel(ptk_ctx* c, int method, cudaStream_t s) {
     // the cell of the integer optimum: half a pixel, half a level-0 rotation step
     lp.redo_list = c->d_lists + 3 * (size_t)c->n;
     lp.redo_count = c->d_counts + 7;
-    lp.cell_px = 0.5;
+    lp.cell_px = c->cfg.lm_cell_px;
     const ptk_zone& z0 = c->cfg.zone[0];
-    lp.cell_rot = (c->cfg.rotations != 0 && z0.num_rot != 0 && z0.inc_rot > 0.0) ? 0.5 * z0.inc_rot : HUGE_VAL;
+    lp.cell_rot = (c->cfg.rotations != 0 && z0.num_rot != 0 && z0.inc_rot > 0.0 && c->cfg.lm_cell_rot > 0.0)
+                      ? c->cfg.lm_cell_rot * z0.inc_rot
+                      : HUGE_VAL;
+    if (!(lp.cell_px > 0.0)) lp.redo_list = nullptr;  // hand-off disabled: every LM result is kept
     CK(cudaMemsetAsync(lp.redo_count, 0, sizeof(int), s));
     launch_subpix_lm(c->g, frame(c, c->cur_slot), lp, s);
-    // those grains: the reference's Powell from their pixel-stage state
-    launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, c->max_R,
-                         lp.redo_list, s, lp.redo_count);
-    c->launches += 1;
+    if (lp.redo_list) {  // those grains: the reference's Powell from their pixel-stage state
+      launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, c->max_R,
+                           lp.redo_list, s, lp.redo_count);
+      c->launches += 1;
+    }
   } else if (method == PTK_SUBPIX_POWELL) {
     launch_subpix_powell(c->g, frame(c, c->cur_slot), frame(c, c->ref_slot), subpix_params(c), c->max_P, c->max_R,
                          c->d_order, s);
@@ -693,6 +699,11 @@ int prepare_searches(ptk_ctx* c) {
   if (need_bf) {
     int rc = ensure_bf16(c, need_bf);
     if (rc) return rc;
+    for (int level = 0; level < 3 && level <= c->cfg.rescue_level; ++level) {
+      SearchGeom sg;
+      if ((rc = search_geometry(c, level, &sg))) return rc;
+      if (sg.bf16 && (rc = ensure_bf16_tmaps(c, level, sg.nrot))) return rc;
+    }
   }
   return ensure_best(c, need ? need : 1);
 }
@@ -740,6 +751,8 @@ int ptk_config_default(ptk_config* cfg) {
   cfg->lm_max_iter = 30;
   cfg->lm_tol = 1e-4;
   cfg->autotune = 0;
+  cfg->lm_cell_px = 0.5;
+  cfg->lm_cell_rot = 2.0;
   return PTK_OK;
 }
 

@@ -13,6 +13,7 @@
 //     search_method  exact | bf16          integer search (default exact)
 //     subpix_method  powell | adjoint_lm   subpixel refinement (default powell)
 //     topk K, lm_max_iter N, lm_tol T      their parameters
+//     lm_cell PX STEPS                    LM results beyond this cell go to Powell (0 0: none)
 //     autotune 0 | 1                       time the level-0 search shapes
 //                                          before the first frame (ptk_autotune)
 //     undistort_images 0 | 1               resample every frame with the
@@ -407,6 +408,8 @@ Settings read_commands(const char* path) {
       in >> s.cfg.lm_max_iter;
     } else if (tok == "lm_tol") {
       in >> s.cfg.lm_tol;
+    } else if (tok == "lm_cell") {  // pixels, rotation steps (0 0: keep every LM result)
+      in >> s.cfg.lm_cell_px >> s.cfg.lm_cell_rot;
     } else if (tok == "autotune") {
       in >> s.cfg.autotune;
     } else if (tok == "undistort_images") {
