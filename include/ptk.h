@@ -102,9 +102,9 @@ typedef struct ptk_config {
   int32_t autotune;              /* 1: ptk_track_frame runs ptk_autotune once, before its first frame;
                                     if tuning fails the built-in shapes are kept (default 0) */
   double lm_cell_px;             /* adjoint LM: a refinement ending more than this many pixels (x or y)
-                                    from its integer optimum ... (default 0.5; <= 0: every LM result kept) */
-  double lm_cell_rot;            /* ... or more than this many level-0 rotation steps from it leaves the
-                                    grain, untouched, to the reference's Powell (default 2) */
+                                    from its integer optimum ... (default 0: every LM result kept) */
+  double lm_cell_rot;            /* ... or more than this many level-0 rotation steps from it (<= 0: no
+                                    rotation bound) leaves the grain, untouched, to the reference's Powell */
 } ptk_config;
 
 typedef struct ptk_ctx ptk_ctx;

@@ -751,8 +751,8 @@ int ptk_config_default(ptk_config* cfg) {
   cfg->lm_max_iter = 30;
   cfg->lm_tol = 1e-4;
   cfg->autotune = 0;
-  cfg->lm_cell_px = 0.5;
-  cfg->lm_cell_rot = 2.0;
+  cfg->lm_cell_px = 0.0;
+  cfg->lm_cell_rot = 0.0;
   return PTK_OK;
 }
 
