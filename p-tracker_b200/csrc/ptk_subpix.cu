@@ -182,11 +182,11 @@ __device__ __forceinline__ double patch_px(const Patch& pt, int x, int y) {
 // the last evaluation, the reference values under pattern0_rotated, and the
 // cosine and sine of the last rotation angle.
 struct ExactObj {
-  double* vals;          // P samples
   const uint16_t* w0;    // P reference values (staged)
-  double* bcast;         // 8 doubles: [3] cos, [4] sin, [5] C0C0
-  double* red2;          // 2 doubles per warp: the block sums' partials
+  double* bcast;         // 8 doubles: [3] cos, [4] sin, [5] C0C0, [6] [7] sum of d0 (double-double)
+  double* red2;          // 6 doubles per warp: the block sums' partials
   double inv_num_pix;    // 1 / P
+  double sd0_hi, sd0_lo; // sum over the points of d0_i = (double)I0_i - mean0, double-double
   double last_rot, c1, s1;
 };
 
@@ -221,49 +221,75 @@ struct Sum2 {
   }
 };
 
-// The block's Sum2 partials combined in a fixed order (lanes by a butterfly,
-// then the warps in index order): every thread returns the same rounded sum.
+// The block's three Sum2 partials combined in a fixed order (lanes by a
+// butterfly, then the warps in index order): every thread returns the same
+// three double-double sums, normalised (hi + lo with |lo| <= ulp(hi) / 2).
 template <int NT>
-__device__ __forceinline__ double block_sum2(Sum2 v, double* red2) {
+__device__ __forceinline__ void block_sum2x3(Sum2 v[3], double* red2, crtrig::dd out[3]) {
   for (int o = 16; o > 0; o >>= 1) {
-    Sum2 w;
-    w.s = __shfl_xor_sync(0xffffffffu, v.s, o);
-    w.c = __shfl_xor_sync(0xffffffffu, v.c, o);
     // both lanes of a pair combine the same two values in the same order
     const bool lo = (threadIdx.x & o) == 0;
-    Sum2 a = lo ? v : w, b = lo ? w : v;
-    a.add(b);
-    v = a;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      Sum2 w;
+      w.s = __shfl_xor_sync(0xffffffffu, v[k].s, o);
+      w.c = __shfl_xor_sync(0xffffffffu, v[k].c, o);
+      Sum2 a = lo ? v[k] : w, b = lo ? w : v[k];
+      a.add(b);
+      v[k] = a;
+    }
   }
   const int wp = threadIdx.x >> 5;
   __syncthreads();
   if ((threadIdx.x & 31) == 0) {
-    red2[2 * wp] = v.s;
-    red2[2 * wp + 1] = v.c;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      red2[6 * wp + 2 * k] = v[k].s;
+      red2[6 * wp + 2 * k + 1] = v[k].c;
+    }
   }
   __syncthreads();
-  Sum2 t;
 #pragma unroll
-  for (int k = 0; k < NT / 32; ++k) {
-    Sum2 w;
-    w.s = red2[2 * k];
-    w.c = red2[2 * k + 1];
-    t.add(w);
+  for (int k = 0; k < 3; ++k) {
+    Sum2 t;
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) {
+      Sum2 x;
+      x.s = red2[6 * w + 2 * k];
+      x.c = red2[6 * w + 2 * k + 1];
+      t.add(x);
+    }
+    out[k] = crtrig::fast_two_sum(t.s, t.c);
   }
-  return t.s + t.c;
 }
 
-// NCC_to_minimize_xyR (src/p-tracker.cpp:1018-1088): the reference's two-pass
-// arithmetic - sample positions xpix1 + c1 x + s1 y and ypix1 - s1 x + c1 y,
-// the interpolators, mean1 = (sum of the samples) / P, then C0C1 and C1C1 over
-// the centred values, every product and difference rounded separately (this
-// file is compiled without FMA contraction) - with each of the three sums
-// correctly rounded (Sum2 over the block) where the reference rounds after
-// every term in point order, and cos / sin of the angle correctly rounded
-// (ptk_crtrig.cuh) where the host C library is within an ulp.  The value
-// therefore differs from the reference's only by the reference's own rounding
-// of its sequential sums.  Called by every thread of the block with the same
-// X; returns the same value on every thread.
+// a / d for a double-double a and a double d (one correction step).
+__device__ __forceinline__ crtrig::dd dd_div_d(crtrig::dd a, double d) {
+  const double q1 = a.hi / d;
+  const crtrig::dd p = crtrig::two_prod(q1, d);
+  const double r = ((a.hi - p.hi) - p.lo) + a.lo;
+  return crtrig::fast_two_sum(q1, r / d);
+}
+
+// NCC_to_minimize_xyR (src/p-tracker.cpp:1018-1088) in one pass over the
+// points: the sample positions xpix1 + c1 x + s1 y and ypix1 - s1 x + c1 y and
+// the interpolators in the reference's operations and order, every product and
+// sum rounded separately (this file is compiled without FMA contraction), cos /
+// sin correctly rounded (ptk_crtrig.cuh) where the host C library is within an
+// ulp; and the reference's two-pass sums
+//     mean1 = (sum v) / P,  C1C1 = sum (v - mean1)^2,  C0C1 = sum d0 (v - mean1)
+// (d0 = I0 - mean0, rounded as the reference rounds it) from the exact sums
+// sum v, sum v^2 and sum d0 v - each product split exactly by a fused
+// multiply-add, the terms added with compensation (Sum2), the block's
+// partials combined in a fixed order - as
+//     C1C1 = sum v^2 - (sum v)^2 / P,  C0C1 = sum d0 v - (sum v)(sum d0) / P
+// evaluated in double-double and rounded once.  Each is the exact value of
+// the reference's expression with the exact mean (the reference rounds after
+// every point instead, and centres on the rounded mean1, a difference of
+// P (mean1 - sum v / P)^2, far below its own rounding), so the objective
+// differs from the reference's only by the reference's own rounding.  Called
+// by every thread of the block with the same X; returns the same value on
+// every thread.
 template <int NT>
 __device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp,
                                   const ObjGrain& o, const Patch& pt, ExactObj& ex, const double X[3],
@@ -281,7 +307,7 @@ __device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const
     ex.last_rot = rot;
   }
   const double c1 = ex.c1, s1 = ex.s1;
-  Sum2 sv;
+  Sum2 acc[3];  // sum v, sum v^2, sum d0 v
   for (int i = tid; i < o.P; i += NT) {
     const short2 q = g.pat0[o.b + i];
     const double x = (double)q.x, y = (double)q.y;
@@ -303,24 +329,42 @@ __device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const
     } else {
       v = interp(cur, sp.interp, xs, ys, clamped);
     }
-    ex.vals[i] = v;  // each thread reads back only its own samples
-    sv.add(v);
-  }
-  const double mean1 = block_sum2<NT>(sv, ex.red2) * ex.inv_num_pix;
-  Sum2 s01, s11;
-  for (int i = tid; i < o.P; i += NT) {
-    const double d1 = ex.vals[i] - mean1;
     const double d0 = (double)ex.w0[i] - o.mean0;
-    s01.add(d0 * d1);
-    s11.add(d1 * d1);
+    acc[0].add(v);
+    const double vv = v * v, d0v = d0 * v;
+    acc[1].add(vv);
+    acc[1].c += fma(v, v, -vv);  // the products' rounding errors, exact by the fused multiply-add
+    acc[2].add(d0v);
+    acc[2].c += fma(d0, v, -d0v);
   }
-  const double c01 = block_sum2<NT>(s01, ex.red2);
-  const double c11 = block_sum2<NT>(s11, ex.red2);
-  const double ncc = c01 / sqrt(o.c0c0 * c11);
+  crtrig::dd S[3];
+  block_sum2x3<NT>(acc, ex.red2, S);
+  const double P = (double)o.P;
+  const crtrig::dd sumd0{ex.sd0_hi, ex.sd0_lo};
+  const crtrig::dd c11 = crtrig::dd_add(S[1], crtrig::dd_neg(dd_div_d(crtrig::dd_mul(S[0], S[0]), P)));
+  const crtrig::dd c01 = crtrig::dd_add(S[2], crtrig::dd_neg(dd_div_d(crtrig::dd_mul(S[0], sumd0), P)));
+  const double ncc = (c01.hi + c01.lo) / sqrt(o.c0c0 * (c11.hi + c11.lo));
   double W = 1.0;
   const double disp = sqrt(X[0] * X[0] + X[1] * X[1]);
   if (disp > sp.disp_max) W = sp.stiffness * (disp - sp.disp_max) + 1.0;
   return (1.0 - ncc) * W;
+}
+
+// Once per grain: C0C0 as do_precomputations sums it (point order, each step
+// rounded; src/p-tracker.cpp:646-651) in bcast[5], and the double-double sum
+// of the points' d0 in bcast[6..7].  Every thread must call it.
+template <int NT>
+__device__ void grain_sums(const uint16_t* w0, int P, double mean0, double* bcast, double* red2) {
+  if (threadIdx.x == 0) bcast[5] = c0c0_in_order(w0, P, mean0);
+  Sum2 acc[3];
+  for (int i = threadIdx.x; i < P; i += NT) acc[0].add((double)w0[i] - mean0);
+  crtrig::dd S[3];
+  block_sum2x3<NT>(acc, red2, S);
+  if (threadIdx.x == 0) {
+    bcast[6] = S[0].hi;
+    bcast[7] = S[0].lo;
+  }
+  __syncthreads();
 }
 
 // Objective and its gradient (adjoint through the cubic interpolant and the
@@ -575,8 +619,8 @@ __device__ void powell_minimize(F& f, double p[3], const double step[3], double 
 }  // namespace
 
 // Dynamic shared memory of the Powell kernel: the staged frame region (its
-// cap in uint16 elements first), then per pattern point a double sample and
-// the uint16 reference value.
+// cap in uint16 elements first), then per pattern point its uint16 reference
+// value.
 struct PowellSmem {
   int patch_cap;   // elements of the staged frame region
   int max_points;  // largest pattern of the grains
@@ -590,12 +634,12 @@ __host__ __device__ inline size_t powell_vals_offset(int patch_cap) {
 // follow_pattern_subpixel_xyR (src/p-tracker.cpp:1090-1128) for every grain,
 // one block per grain, grains taken in `order` (decreasing pattern size) when
 // given.
-__global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, FrameDev cur, SubpixParams sp,
-                                                                    int patch_cap, int max_points,
-                                                                    const int* order, const int* list_count) {
+__global__ void __launch_bounds__(kSubpixThreads, 5) k_subpix_powell(GrainsDev g, FrameDev cur, SubpixParams sp,
+                                                                       int patch_cap, int max_points,
+                                                                       const int* order, const int* list_count) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double bcast[8];
-  __shared__ double red2[2 * (kSubpixThreads / 32)];
+  __shared__ double red2[6 * (kSubpixThreads / 32)];
   __shared__ int s_clamped, s_bb[4];
   if (list_count && (int)blockIdx.x >= *list_count) return;
   const int gi = order ? order[blockIdx.x] : (int)blockIdx.x;
@@ -610,8 +654,7 @@ __global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, F
   }
   __syncthreads();
   uint16_t* s_patch = reinterpret_cast<uint16_t*>(smem);
-  double* s_vals = reinterpret_cast<double*>(smem + powell_vals_offset(patch_cap));
-  uint16_t* s_w0 = reinterpret_cast<uint16_t*>(s_vals + max_points);
+  uint16_t* s_w0 = reinterpret_cast<uint16_t*>(smem + powell_vals_offset(patch_cap));
   int xmn = 1 << 30, xmx = -(1 << 30), ymn = 1 << 30, ymx = -(1 << 30);
   for (int i = threadIdx.x; i < o.P; i += kSubpixThreads) {
     const short2 q = g.pat0[o.b + i];
@@ -636,12 +679,12 @@ __global__ void __launch_bounds__(kSubpixThreads) k_subpix_powell(GrainsDev g, F
     const int yy = e / pw, xx = e - yy * pw;
     s_patch[e] = cur.pix[(size_t)(py0 + yy) * cur.pitch + (px0 + xx)];
   }
-  // C0C0 as do_precomputations sums it (point order, each step rounded)
-  if (threadIdx.x == 0) bcast[5] = c0c0_in_order(s_w0, o.P, o.mean0);
   __syncthreads();
+  grain_sums<kSubpixThreads>(s_w0, o.P, o.mean0, bcast, red2);
   o.c0c0 = bcast[5];
   const Patch pt{s_patch, px0, py0, pw, ph};
-  ExactObj ex{s_vals, s_w0, bcast, red2, 1.0 / (double)o.P, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0};
+  ExactObj ex{s_w0, bcast, red2, 1.0 / (double)o.P, bcast[6], bcast[7], __longlong_as_double(0x7ff8000000000000ll),
+              0.0, 0.0};
   bool clamped = false;
   PowellEval<kSubpixThreads> f{&g, &cur, &sp, &o, &pt, &ex, &clamped, 0};
   double X[3] = {0.0, 0.0, 0.0};
@@ -669,7 +712,7 @@ __global__ void __launch_bounds__(kSubpixThreads) k_objective(GrainsDev g, Frame
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[kSubpixThreads / 32];
   __shared__ double bcast[8];
-  __shared__ double red2[2 * (kSubpixThreads / 32)];
+  __shared__ double red2[6 * (kSubpixThreads / 32)];
   const int gi = blockIdx.x;
   ObjGrain o = load_grain(g, gi);
   if (o.P <= 0 || o.P > max_points) {
@@ -692,14 +735,14 @@ __global__ void __launch_bounds__(kSubpixThreads) k_objective(GrainsDev g, Frame
       grad[3 * gi + 2] = G[2];
     }
   } else {
-    uint16_t* s_w0 = reinterpret_cast<uint16_t*>(vals + max_points);
+    uint16_t* s_w0 = reinterpret_cast<uint16_t*>(smem);
     for (int i = threadIdx.x; i < o.P; i += kSubpixThreads) s_w0[i] = g.w0[o.b + i];
     __syncthreads();
-    if (threadIdx.x == 0) bcast[5] = c0c0_in_order(s_w0, o.P, o.mean0);
-    __syncthreads();
+    grain_sums<kSubpixThreads>(s_w0, o.P, o.mean0, bcast, red2);
     o.c0c0 = bcast[5];
     const Patch none{nullptr, 0, 0, 0, 0};
-    ExactObj ex{vals, s_w0, bcast, red2, 1.0 / (double)o.P, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0};
+    ExactObj ex{s_w0, bcast, red2, 1.0 / (double)o.P, bcast[6], bcast[7], __longlong_as_double(0x7ff8000000000000ll),
+                0.0, 0.0};
     val = objective_exact<kSubpixThreads>(g, cur, sp, o, none, ex, X, &clamped);
   }
   if (threadIdx.x == 0) f[gi] = val;
@@ -709,7 +752,7 @@ static PowellSmem powell_smem(int max_points, int max_r) {
   PowellSmem m;
   const size_t side = (size_t)(2 * max_r + 1 + 2 * 6 + 2);
   size_t patch = side * side;
-  const size_t rest = (size_t)max_points * (sizeof(double) + sizeof(uint16_t));
+  const size_t rest = (size_t)max_points * sizeof(uint16_t);
   constexpr size_t kCap = 227 * 1024 - 1024;  // the kernel's static shared memory included
   if (powell_vals_offset((int)patch) + rest > kCap)
     patch = rest < kCap ? (kCap - rest) / sizeof(uint16_t) - 8 : 0;  // samples outside the region read the frame
@@ -738,7 +781,7 @@ void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParam
                       double* grad, int max_points, cudaStream_t s) {
   if (g.n <= 0) return;
   prepare_subpix(max_points, 0);
-  const size_t smem = (size_t)max_points * sizeof(double) * (grad ? 3 : 1) + (grad ? 0 : (size_t)max_points * 2);
+  const size_t smem = grad ? (size_t)max_points * sizeof(double) * 3 : (size_t)max_points * sizeof(uint16_t);
   k_objective<<<g.n, kSubpixThreads, smem, s>>>(g, cur, sp, X, f, grad, max_points);
 }
 
