@@ -129,6 +129,7 @@ struct ptk_ctx {
   std::vector<int> h_bf_half;          // host copies of the slot layout (tensor-map encoding)
   std::vector<size_t> h_bf_wofs;
   CUtensorMap* d_bf_tmaps[3]{nullptr, nullptr, nullptr};  // per level: each grain's operand-row tensor map
+  double2* d_bf_rot_cs{nullptr};                           // per grain: cos / sin of the level's rotation steps
   int bf_tmaps_nrot[3]{0, 0, 0};                           // rotation steps they were encoded for (0: stale)
   int2* d_topk{nullptr};
   unsigned* d_topk_rot{nullptr};  // rotation steps of each kept candidate to rescore
@@ -462,6 +463,9 @@ int ensure_bf16(ptk_ctx* c, size_t items) {
     CK(cudaMemcpy(c->d_bf_wofs, wofs.data(), sizeof(size_t) * wofs.size(), cudaMemcpyHostToDevice));
     c->h_bf_half = half;
     c->h_bf_wofs = wofs;
+    cudaFree(c->d_bf_rot_cs);
+    c->d_bf_rot_cs = nullptr;
+    CK(cudaMalloc(&c->d_bf_rot_cs, sizeof(double2) * 32 * half.size()));
     for (int l = 0; l < 3; ++l) {  // the slots move (and the grain count may change): encode the maps again
       cudaFree(c->d_bf_tmaps[l]);
       c->d_bf_tmaps[l] = nullptr;
@@ -585,6 +589,7 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
     b.wofs = c->d_bf_wofs;
     b.wslots = c->d_bf_wslots;
     b.tmaps = c->d_bf_tmaps[level];
+    b.rot_cs = c->d_bf_rot_cs;
     if (!b.tmaps || c->bf_tmaps_nrot[level] != sg.nrot)  // every caller prepares them first
       return fail(c, PTK_ERR_STATE, "BF16 operand tensor maps missing for this level");
     b.topk = c->d_topk;
@@ -831,6 +836,7 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_bf_wofs);
   cudaFree(c->d_bf_wslots);
   for (int l = 0; l < 3; ++l) cudaFree(c->d_bf_tmaps[l]);
+  cudaFree(c->d_bf_rot_cs);
   cudaFree(c->d_topk);
   cudaFree(c->d_topk_rot);
   cudaFree(c->d_tile_top);

@@ -115,6 +115,7 @@ struct Bf16Launch {
   const size_t* wofs;       // per grain: offset of its weight slot in wslots (16-byte units)
   unsigned char* wslots;    // BF16 weights of the level's rotation steps, per grain
   const CUtensorMap* tmaps; // per grain: tensor map of its operand rows (bf16_encode_tmaps)
+  double2* rot_cs;          // [grain][32]: cos, sin of each rotation step's total angle (weights kernel)
   int2* topk;               // [list entry][tile][kBf16KeepMax] kept (u, v), INT_MIN when none
   unsigned* topk_rot;       // same layout: bit r = rotation step r is rescored at that candidate
   int ring;                 // operand-row buffers of the search kernel's ring (2..8; the strips take the rest)

@@ -315,6 +315,8 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
     sincos(base_rot + p.steps[tid], &sr, &cr);
     s_cs[tid] = make_double2(cr, sr);
     s_csf[tid] = make_float2((float)cr, (float)sr);
+    // kept for this level's search and rescore kernels, which rotate by the same steps
+    p.rot_cs[(size_t)gi * kNRot + tid] = make_double2(cr, sr);
   }
   const float mean0 = (float)g.mean0[gi];
   const int fw2 = G.fw * G.fw;
@@ -494,12 +496,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     }
     // rotation cos/sin (total_rot = base_rot + step, as the exact search) and
     // the grain's footprint geometry
-    const double base_rot = g.refrot[gi] + g.drot[gi];
-    if (tid < p.nrot) {
-      double sr, cr;
-      sincos(base_rot + p.steps[tid], &sr, &cr);
-      s_cs[tid] = make_double2(cr, sr);
-      s_csf[tid] = make_float2((float)cr, (float)sr);
+    if (tid < p.nrot) {  // the weights kernel's cos / sin of this grain's steps
+      const double2 cs = p.rot_cs[(size_t)gi * kNRot + tid];
+      s_cs[tid] = cs;
+      s_csf[tid] = make_float2((float)cs.x, (float)cs.y);
     }
     const Geom G = geom_of(p.half[gi], RING);
     const float mean0 = (float)g.mean0[gi];
@@ -993,13 +993,12 @@ __global__ void __launch_bounds__(256, 4) k_rescore_bf16(Bf16Launch p) {
   const long long Pl = P, S0 = g.s0[gi];
   const double den1 = (double)(Pl * g.s00[gi] - S0 * S0);
   const int pitch = p.cur.pitch;
-  const double base_rot = g.refrot[gi] + g.drot[gi];
   const int nu = s_nu;
   for (int u = warp; u < nu; u += kW) {
     const int unit = s_unit[u];
     const int r = unit & 0xff, k0 = (unit >> 8) & 0xff, k1 = (unit >> 16) & 0xff;
-    double sr, cr;
-    sincos(base_rot + p.steps[r], &sr, &cr);
+    const double2 cs = p.rot_cs[(size_t)gi * kNRot + r];  // the weights kernel's cos / sin of the step
+    const double sr = cs.y, cr = cs.x;
     const float cf = (float)cr, sf = (float)sr;
     const bool two = k1 != 255;
     const uint16_t* pa = p.cur.pix + s_base[k0];
