@@ -129,6 +129,7 @@ struct ptk_ctx {
   std::vector<int> h_bf_half;          // host copies of the slot layout (tensor-map encoding)
   std::vector<size_t> h_bf_wofs;
   CUtensorMap* d_bf_tmaps[3]{nullptr, nullptr, nullptr};  // per level: each grain's operand-row tensor map
+  CUtensorMap* d_frame_tmaps{nullptr};  // [frame buffer][kBf16FrameMaps] the BF16 search's image-strip maps
   double2* d_bf_rot_cs{nullptr};                           // per grain: cos / sin of the level's rotation steps
   int bf_tmaps_nrot[3]{0, 0, 0};                           // rotation steps they were encoded for (0: stale)
   int2* d_topk{nullptr};
@@ -592,6 +593,8 @@ int enqueue_search(ptk_ctx* c, int level, cudaStream_t s, cudaEvent_t* ev = null
     b.rot_cs = c->d_bf_rot_cs;
     if (!b.tmaps || c->bf_tmaps_nrot[level] != sg.nrot)  // every caller prepares them first
       return fail(c, PTK_ERR_STATE, "BF16 operand tensor maps missing for this level");
+    if (!c->d_frame_tmaps) return fail(c, PTK_ERR_STATE, "BF16 search: the driver's tensor-map encoder is unavailable");
+    b.frame_tmaps = c->d_frame_tmaps + c->cur_slot * kBf16FrameMaps;
     b.topk = c->d_topk;
     b.topk_rot = c->d_topk_rot;
     b.tile_top = c->d_tile_top;
@@ -793,6 +796,16 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
     if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(frame)"));
     cudaMemset(c->d_img[k], 0, bytes);
   }
+  {  // the BF16 search's tensor maps of both frame buffers (left unset without the driver's encoder)
+    CUtensorMap h[2 * kBf16FrameMaps];
+    if (bf16_encode_frame_tmaps(c->d_img[0], cfg->dimx, cfg->dimy, c->pitch, h) &&
+        bf16_encode_frame_tmaps(c->d_img[1], cfg->dimx, cfg->dimy, c->pitch, h + kBf16FrameMaps)) {
+      e = cudaMalloc(&c->d_frame_tmaps, sizeof(h));
+      if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(frame maps)"));
+      e = cudaMemcpy(c->d_frame_tmaps, h, sizeof(h), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMemcpy(frame maps)"));
+    }
+  }
   // counts: [0] grains, [1] rescue list, [2] super-rescue list, [3] error flag,
   // [4 + level] exact re-search list of a BF16 level
   e = cudaMalloc(&c->d_counts, 8 * sizeof(int));
@@ -837,6 +850,7 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_bf_wslots);
   for (int l = 0; l < 3; ++l) cudaFree(c->d_bf_tmaps[l]);
   cudaFree(c->d_bf_rot_cs);
+  cudaFree(c->d_frame_tmaps);
   cudaFree(c->d_topk);
   cudaFree(c->d_topk_rot);
   cudaFree(c->d_tile_top);

@@ -98,6 +98,7 @@ struct FinalizeLaunch {
 
 // BF16 tensor-core search: kept candidates per tile (upper bound of `keep`).
 constexpr int kBf16KeepMax = 8;
+constexpr int kBf16FrameMaps = 9;  // frame tensor maps per frame buffer, one per Hankel width
 
 struct Bf16Launch {
   GrainsDev g;
@@ -115,6 +116,7 @@ struct Bf16Launch {
   const size_t* wofs;       // per grain: offset of its weight slot in wslots (16-byte units)
   unsigned char* wslots;    // BF16 weights of the level's rotation steps, per grain
   const CUtensorMap* tmaps; // per grain: tensor map of its operand rows (bf16_encode_tmaps)
+  const CUtensorMap* frame_tmaps;  // the current frame's maps per Hankel width (bf16_encode_frame_tmaps)
   double2* rot_cs;          // [grain][32]: cos, sin of each rotation step's total angle (weights kernel)
   int2* topk;               // [list entry][tile][kBf16KeepMax] kept (u, v), INT_MIN when none
   unsigned* topk_rot;       // same layout: bit r = rotation step r is rescored at that candidate
@@ -172,6 +174,7 @@ constexpr int kBf16RingDefault = 4;
 size_t bf16_weight_entries(int half);
 bool bf16_encode_tmaps(const int* half, const size_t* wofs, int n, unsigned char* wslots, int nrot,
                        CUtensorMap* out);
+bool bf16_encode_frame_tmaps(const uint16_t* pix, int dimx, int dimy, int pitch, CUtensorMap* out);
 void prepare_search_bf16();
 // ev (optional, 5 events): recorded before the first kernel and after each of the four
 // frame_ready (may be null): an event the search waits for after the weights

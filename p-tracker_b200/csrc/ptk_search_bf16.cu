@@ -100,6 +100,7 @@ constexpr float kKeepRel = 0.03f;
 constexpr float kKeepRelWeak = 0.10f;
 constexpr float kGoodMatch = 0.9f;
 constexpr long kWaitLimit = 1L << 22;
+constexpr int kStageBoxRows = 8;  // image rows per TMA box of the strip staging
 // after an error: the waits for the CTA's own copies and MMAs still in flight
 // (they complete unless the device is broken) get a longer bound
 constexpr long kDrainLimit = 1L << 26;
@@ -122,7 +123,7 @@ struct Geom {
   int nch;   // 16-column MMA chunks (footprint + 24 columns of shift)
   int wb;    // weight blocks per row in shared memory (3 leading zero blocks)
   int hb;    // Hankel blocks per image row
-  int rp;    // bytes per staged image row (the Hankel's 8 hb + 7 pixels from a 16-byte boundary)
+  int rp;    // bytes per staged image row (8 hb + 16 pixels from a 16-byte boundary: one TMA box row)
   int rs;    // footprint rows per strip (Hankel rows filled at once, plus 31)
   int nb;    // operand-row ring buffers
 };
@@ -137,9 +138,9 @@ __host__ __device__ inline Geom geom_of(int half, int nb = kRingUsed) {
   g.hb = 2 * g.nch;
   g.rp = 16 * g.hb + 32;
   // the operand-row ring, then two Hankel buffers and the staged image rows
-  // with 31 rows of halo
+  // with 31 rows of halo (staged in boxes of 8 rows: up to 7 more)
   const int halo_row = 2 * g.hb * 128 + g.rp;
-  int rs = (kSmemBudget - nb * 2 * g.wb * 512) / halo_row - 31;
+  int rs = (kSmemBudget - nb * 2 * g.wb * 512 - (kStageBoxRows - 1) * g.rp) / halo_row - 31;
   if (rs > g.fw) rs = g.fw;
   g.rs = rs < 1 ? 1 : rs;
   g.nb = nb;
@@ -207,11 +208,16 @@ __device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* tma
       : "memory");
 }
 
-// 16-byte asynchronous copy global -> shared through L2 (per thread).
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+// One box of a 2-D tensor map global -> shared (TMA, tiled, no multicast);
+// x must be a multiple of 8 pixels (16 bytes); rows or columns outside the
+// frame come back as zeros.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* tmap, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
@@ -416,6 +422,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   __shared__ __align__(8) unsigned long long s_full[kRing];  // operand row copied into a ring buffer
   __shared__ __align__(8) unsigned long long s_free[kRing];  // the MMAs reading a ring buffer completed
   __shared__ __align__(8) unsigned long long s_probe;  // failure-path test: nothing ever arrives on it
+  __shared__ __align__(8) unsigned long long s_stage;  // a strip's image rows staged (TMA)
+  __shared__ int s_stage_out;                          // stagings issued and not yet waited for (0 or 1)
   // operand rows through the ring (thread 0): uses of each buffer copied and
   // consumed so far (a buffer's barriers complete one phase per use)
   __shared__ unsigned s_iss[kRing], s_con[kRing];
@@ -443,6 +451,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_free[k])));
     }
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_probe)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_stage)));
+    s_stage_out = 0;
     asm volatile("fence.mbarrier_init.release.cluster;");
     s_err = 0;
     for (int k = 0; k < kRing; ++k) s_iss[k] = s_con[k] = 0u;
@@ -452,6 +462,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = s_tmem;
   uint32_t parity = 0;  // thread 0: parity of the next MMA-completion phase of s_mbar
+  uint32_t sparity = 0;  // thread 0: parity of the next staging phase of s_stage
   if (tid == 0 && (smem_u32(smem_bf) & 127u)) {
     // the operand rows' TMA boxes land on 512-byte multiples from here: the
     // dynamic shared memory must start 128-byte aligned (never seen otherwise)
@@ -510,7 +521,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     const uint4* slotM = slotW + wrows;
     if (tid < 2 * G.fw) s_rng[tid] = reinterpret_cast<const unsigned char*>(slotM + wrows)[tid];
     const CUtensorMap* tmap = p.tmaps + gi;  // this grain's operand rows, rotation slots zero-filled to 32
-    if (tid == 0) asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
+    const CUtensorMap* fmap = p.frame_tmaps + (G.hb >> 1);  // the frame's map for this Hankel width
+    if (tid == 0) {
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(fmap) : "memory");
+    }
     // ring buffer k: W row at k * 2 wb * 512, M row wb * 512 after it
     const size_t hbytes = (size_t)(G.rs + 31) * G.hb * 128;
     unsigned char* sA = smem;
@@ -591,24 +606,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
       }
       // image origin of footprint column 0 at candidate (u0, v0)
       const int Xi = g.refx[gi] + gdx - G.half + u0, Yi = g.refy[gi] + gdy - G.half + v0;
-      // A strip whose image rows lie inside the frame stages them in shared
-      // memory with 16-byte asynchronous copies (columns Xa .. Xa + ncols - 1),
-      // issued by every thread during the previous strip's MMAs where there
-      // is one.
+      // A strip's image rows (columns Xa .. Xa + 8 hb + 15, rows from Yi + ys)
+      // are staged in shared memory by TMA boxes of 8 rows from the frame's
+      // tensor map for this Hankel width, issued by thread 0 - for the next
+      // strip during the current strip's MMAs.  Rows and columns outside the
+      // frame come back as zeros: they only meet candidates outside the zone
+      // or footprint pixels whose weights are zero in every rotation step.
       const int nwin = 8 * G.hb;
       const int Xa = Xi & ~7, xoff = Xi - Xa;
-      const int ncols = (xoff + nwin + 7 + 7) & ~7;
-      auto staged = [&](int ys_) {
-        const int y0 = Yi + ys_, n_ = min(G.rs, G.fw - ys_);
-        return y0 >= 0 && y0 + n_ + 30 < p.cur.dimy && Xi >= 0 && Xi + nwin + 6 < p.cur.dimx &&
-               Xa + ncols <= p.cur.pitch;
+      auto stage_rows = [&](int ys_) {  // thread 0
+        const int boxes = (min(G.rs, G.fw - ys_) + 31 + kStageBoxRows - 1) / kStageBoxRows;
+        const uint32_t sb = smem_u32(&s_stage);
+        mbar_expect_tx(sb, (uint32_t)(boxes * kStageBoxRows * G.rp));
+        for (int j = 0; j < boxes; ++j)
+          tma_load_2d(rbase + (uint32_t)(j * kStageBoxRows * G.rp), fmap, Xa, Yi + ys_ + j * kStageBoxRows, sb);
+        s_stage_out = 1;
       };
-      auto stage_rows = [&](int ys_) {
-        const int n_ = min(G.rs, G.fw - ys_) + 31, cpr = ncols >> 3;
-        for (int e = tid; e < n_ * cpr; e += kThreads) {
-          const int rho = e / cpr, c = e - rho * cpr;
-          cp_async16(rbase + (uint32_t)(rho * G.rp + 16 * c),
-                     p.cur.pix + (size_t)(Yi + ys_ + rho) * p.cur.pitch + Xa + 8 * c);
+      auto wait_rows = [&]() {  // thread 0 (a wait that gives up leaves the staging to the drain)
+        if (mbar_wait(smem_u32(&s_stage), sparity)) {
+          s_stage_out = 0;
+          sparity ^= 1u;
+        } else {
+          s_err = 1;
+          atomicOr(p.error, 1);
         }
       };
       // Operand rows stream through the ring (thread 0): row y of the tile goes
@@ -637,38 +657,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
             atomicOr(p.error, 1);
             break;
           }
-      bool prefetched = false;
+      if (tid == 0 && !s_err) stage_rows(0);
       uint32_t acc = 0u;  // the tile's first MMA into each accumulator overwrites it
       for (int ys = 0; ys < G.fw; ys += G.rs) {
         const int nr = min(G.rs, G.fw - ys);
-        const bool inside = staged(ys);
-        if (inside && !prefetched) stage_rows(ys);
-        if (inside && !prefetched) {  // (a prefetch completed before the previous strip's last barrier)
-          cp_async_wait_all();
-          __syncthreads();
-        }
+        if (tid == 0 && s_stage_out) wait_rows();  // this strip's rows (staged during the previous MMAs)
+        __syncthreads();
+        if (s_err) break;
         // Hankel image rows ys .. ys + nr + 30 of I - m and of (I - m)^2.
         // Entry (block a, shift s) of a row is the 8-pixel window starting at
         // column x = 8 a + s, stored at byte 16 x: a warp fills one row, 25
         // windows per pass, lane x reading pixel x and taking pixels
         // x + 1 .. x + 7 from the next lanes, so the 16-byte stores of a pass
-        // are contiguous.  Staged strips read the pixels from shared memory,
-        // strips at the frame's edges from global memory with bounds checks.
-        const int Y0 = Yi + ys;
+        // are contiguous.  The pixels come from the staged rows.
         for (int rho = warp; rho < nr + 31; rho += kWarps) {
-          const int Y = Y0 + rho;
-          const bool rowin = Y >= 0 && Y < p.cur.dimy;
-          const uint16_t* src = p.cur.pix + (size_t)(rowin ? Y : 0) * p.cur.pitch;
           const uint16_t* srow = reinterpret_cast<const uint16_t*>(sR + (size_t)rho * G.rp) + xoff;
           unsigned char* drow = sHa + (size_t)rho * G.hb * 128;
           unsigned char* qrow = sHs + (size_t)rho * G.hb * 128;
           for (int x0 = 0; x0 < nwin; x0 += 25) {
-            const int x = x0 + lane, X = Xi + x;
-            float f = 0.0f;
-            if (x < nwin + 7) {
-              if (inside) f = __int_as_float(0x4B000000 | (int)srow[x]) - sub;
-              else if (rowin && X >= 0 && X < p.cur.dimx) f = __int_as_float(0x4B000000 | (int)__ldg(src + X)) - sub;
-            }
+            const int x = x0 + lane;
+            const float f = x < nwin + 7 ? __int_as_float(0x4B000000 | (int)srow[x]) - sub : 0.0f;
             const float f1 = __shfl_down_sync(0xffffffffu, f, 1);
             const uint32_t p0 = pack_bf16x2(f, f1);
             const uint32_t q0 = pack_bf16x2(f * f, f1 * f1);
@@ -687,8 +695,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         // the staged rows are consumed: bring in the next strip's during these MMAs
-        prefetched = ys + G.rs < G.fw && staged(ys + G.rs);
-        if (prefetched) stage_rows(ys + G.rs);
+        if (tid == 0 && !s_err && ys + G.rs < G.fw) stage_rows(ys + G.rs);
         bool committed = false;  // thread 0: MMAs of this strip committed to s_mbar
         if (tid == 0 && !s_err) {
           for (int yl = 0; yl < nr; ++yl) {
@@ -736,7 +743,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
           parity ^= 1u;
           asm volatile("tcgen05.fence::before_thread_sync;");
         }
-        if (prefetched) cp_async_wait_all();
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;");
         if (s_err) break;
@@ -888,7 +894,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     }
     if (s_err) break;
   }
-  cp_async_wait_all();
   __syncthreads();
   if (s_err && tid == 0) {
     // Before the tensor memory is freed and the CTA exits: the bulk copies still
@@ -898,6 +903,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     // drain bound.
     for (int k = 0; k < kRing; ++k)
       for (unsigned u = s_con[k]; u < s_iss[k]; ++u) mbar_wait(smem_u32(&s_full[k]), u & 1u, kDrainLimit);
+    if (s_stage_out) mbar_wait(smem_u32(&s_stage), sparity, kDrainLimit);  // the image rows still in flight
     mbar_wait(mbar, parity ^ 1u, kDrainLimit);
   }
   asm volatile("tcgen05.fence::after_thread_sync;");
@@ -1077,7 +1083,7 @@ bool bf16_ring_ok(int max_half, int ring) {
   if (ring != 2 && ring != 3 && ring != 4 && ring != 6) return false;  // the instantiated kernels
   const Geom G = geom_of(max_half, ring);
   const int halo_row = 2 * G.hb * 128 + G.rp;
-  return (kSmemBudget - ring * 2 * G.wb * 512) / halo_row - 31 >= 1;
+  return (kSmemBudget - ring * 2 * G.wb * 512 - (kStageBoxRows - 1) * G.rp) / halo_row - 31 >= 1;
 }
 
 void prepare_search_bf16() {
@@ -1094,8 +1100,7 @@ void prepare_search_bf16() {
 // {8, 32, nbf, 1, 1} - the 32 - nrot slots beyond the tensor come back as
 // zeros, in the shared-memory layout of the A operands.  Returns false when
 // the driver's encoder is unavailable or refuses a map.
-bool bf16_encode_tmaps(const int* half, const size_t* wofs, int n, unsigned char* wslots, int nrot,
-                       CUtensorMap* out) {
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   static std::once_flag once;
   std::call_once(once, [] {
@@ -1105,6 +1110,12 @@ bool bf16_encode_tmaps(const int* half, const size_t* wofs, int n, unsigned char
         q == cudaDriverEntryPointSuccess)
       encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   });
+  return encode;
+}
+
+bool bf16_encode_tmaps(const int* half, const size_t* wofs, int n, unsigned char* wslots, int nrot,
+                       CUtensorMap* out) {
+  const PFN_cuTensorMapEncodeTiled_v12000 encode = tmap_encoder();
   if (!encode || nrot < 1 || nrot > kNRot) return false;
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   for (int i = 0; i < n; ++i) {
@@ -1123,6 +1134,29 @@ bool bf16_encode_tmaps(const int* half, const size_t* wofs, int n, unsigned char
     const cuuint64_t strides[4] = {16, 16ull * nrot, 16ull * nrot * G.nbf, 16ull * nrot * G.nbf * G.fw};
     const cuuint32_t box[5] = {8, (cuuint32_t)kNRot, (cuuint32_t)G.nbf, 1, 1};
     if (encode(&out[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, wslots + wofs[i] * 16, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  return true;
+}
+
+// Tensor maps of one frame buffer (host): the u16 image {dimx, dimy} at its
+// row pitch, read as boxes of 8 rows x (8 hb + 16) pixels, one map per Hankel
+// width hb = 2 nch at out[nch] (nch = 2 .. kBf16FrameMaps - 1, which covers
+// every footprint below kMaxFoot; out[0] and out[1] repeat nch = 2).  Pixels
+// outside the frame read as zeros.
+bool bf16_encode_frame_tmaps(const uint16_t* pix, int dimx, int dimy, int pitch, CUtensorMap* out) {
+  const PFN_cuTensorMapEncodeTiled_v12000 encode = tmap_encoder();
+  if (!encode || dimx < 1 || dimy < 1 || pitch < dimx) return false;
+  static_assert((kMaxFoot - 1 + 7) / 8 / 2 + 2 < kBf16FrameMaps, "one frame map per Hankel width");
+  const cuuint64_t dims[2] = {(cuuint64_t)dimx, (cuuint64_t)dimy};
+  const cuuint64_t strides[1] = {2ull * pitch};
+  const cuuint32_t estr[2] = {1, 1};
+  for (int k = 0; k < kBf16FrameMaps; ++k) {
+    const int hb = 2 * (k < 2 ? 2 : k);
+    const cuuint32_t box[2] = {(cuuint32_t)(8 * hb + 16), (cuuint32_t)kStageBoxRows};
+    if (encode(&out[k], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<uint16_t*>(pix), dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return false;

@@ -17,7 +17,7 @@
 // damped normal equations are solved in FP64 and X and the cumulative grain
 // state accumulate in FP64.
 //
-// One 256-thread block per grain, grains in decreasing pattern size (the
+// One 128-thread block per grain, grains in decreasing pattern size (the
 // level-0 order) so that the large ones start first; the iteration stops when
 // the step is below the tolerance, or after two rejected steps in a row once
 // a step was accepted (the FP32 sums' noise floor: further steps only
@@ -32,7 +32,7 @@ namespace ptk {
 
 namespace {
 
-constexpr int kLmThreads = 256;
+constexpr int kLmThreads = 128;
 constexpr int kNSums = 18;
 
 // exact uint16 -> float: bits of 2^23 + v, minus 2^23
