@@ -188,14 +188,6 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
 }
 
-// 1-D bulk async copy global -> shared (16-byte aligned, size a multiple of 16).
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-      "l"(src), "r"(bytes), "r"(mbar)
-      : "memory");
-}
-
 // One box of a 5-D tensor map global -> shared (TMA, tiled, no multicast):
 // coordinates innermost first; elements outside the tensor are filled with
 // zeros and count toward the transaction bytes.
@@ -310,11 +302,9 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
   // zero-fills the other rotation slots of its A operands
   uint4* slotW = reinterpret_cast<uint4*>(p.wslots) + p.wofs[gi];
   uint4* slotM = slotW + (size_t)rows * p.nrot;
-  __shared__ int s_rlo[kMaxFoot], s_rhi[kMaxFoot];
-  if (tid < G.fw) {
-    s_rlo[tid] = INT_MAX;
-    s_rhi[tid] = -1;
-  }
+  static_assert((kMaxFoot - 1 + 7) / 8 <= 12, "8-column blocks per footprint row");
+  __shared__ unsigned char s_occ[kMaxFoot * 12];  // [row][8-column block]: a point in some rotation step
+  for (int e = tid; e < rows; e += kWThreads) s_occ[e] = 0;
   const double base_rot = g.refrot[gi] + g.drot[gi];  // total_rot = base_rot + step, as the exact search
   if (tid < p.nrot) {
     double sr, cr;
@@ -325,12 +315,14 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
     p.rot_cs[(size_t)gi * kNRot + tid] = make_double2(cr, sr);
   }
   const float mean0 = (float)g.mean0[gi];
-  const int fw2 = G.fw * G.fw;
+  // per rotation step a map of fw rows of fwp = 8 nbf words (the columns past
+  // fw stay zero), so that a block's 8 words are two 16-byte loads
+  const int fwp = 8 * G.nbf, fw2 = G.fw * fwp;
   const int nb_max = max(1, min(p.nrot, kWSmem / (4 * fw2)));
   unsigned* map = reinterpret_cast<unsigned*>(smem);
   for (int r0 = 0; r0 < p.nrot; r0 += nb_max) {
     const int nb = min(nb_max, p.nrot - r0);
-    for (int e = tid; e < nb * fw2; e += kWThreads) map[e] = 0u;
+    for (int e = tid; e < nb * fw2 / 4; e += kWThreads) reinterpret_cast<uint4*>(map)[e] = make_uint4(0, 0, 0, 0);
     __syncthreads();
     // four points per thread at a time: their loads are in flight together
     for (int i0 = tid; i0 < P; i0 += 4 * kWThreads) {
@@ -349,7 +341,7 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
         // rotate_round_fast with the point's conversions hoisted out of the
         // step loop and the map address advanced per step
         const float pxf = small_i2f(q0[u].x), pyf = small_i2f(q0[u].y);
-        unsigned* mk = map + G.half * (G.fw + 1);  // offset (0, 0) of step r0
+        unsigned* mk = map + G.half * (fwp + 1);  // offset (0, 0) of step r0
 #pragma unroll 3
         for (int k = 0; k < nb; ++k, mk += fw2) {
           const float2 cf = s_csf[r0 + k];
@@ -365,38 +357,44 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
           }
           // |q| <= ceil(|p|) = half - 1: always inside the footprint
           if ((unsigned)(qx + G.half) < (unsigned)G.fw && (unsigned)(qy + G.half) < (unsigned)G.fw)
-            atomicAdd(mk + qy * G.fw + qx, add[u]);
+            atomicAdd(mk + qy * fwp + qx, add[u]);
         }
       }
     }
     __syncthreads();
-    for (int e = tid; e < nb * rows; e += kWThreads) {
-      const int rem = e / nb, k = e - rem * nb;
-      const int y = rem / G.nbf, af = rem - y * G.nbf;
-      const unsigned* src = map + k * fw2 + y * G.fw + 8 * af;
-      float v[8], m[8];
+    // thread t converts rotation step k = t % nb of the blocks t / nb, t / nb + per, ...
+    // (consecutive threads write consecutive 16-byte rows of the slot)
+    const int per = kWThreads / nb;
+    if (tid < per * nb) {
+      const int k = tid % nb;
+      int rem = tid / nb;
+      int y = rem / G.nbf, af = rem - y * G.nbf;
+      const int dy = per / G.nbf, daf = per - dy * G.nbf;
+      const unsigned* mapk = map + k * fw2;
+      for (; rem < rows; rem += per) {
+        const uint4* src = reinterpret_cast<const uint4*>(mapk + y * fwp + 8 * af);
+        const uint4 c0 = src[0], c1 = src[1];
+        const unsigned c[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+        float v[8], m[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const unsigned c = (8 * af + j < G.fw) ? src[j] : 0u;
-        const float n = (float)(c >> 24);
-        m[j] = n;
-        v[j] = (float)(c & 0xFFFFFFu) - n * mean0;
-      }
-      {  // occupied blocks of the row, one atomic pair per row and warp
-        const bool occ = m[0] + m[1] + m[2] + m[3] + m[4] + m[5] + m[6] + m[7] > 0.0f;
-        const unsigned same = __match_any_sync(__activemask(), y);
-        const int lo = __reduce_min_sync(same, occ ? af : INT_MAX);
-        const int hi = __reduce_max_sync(same, occ ? af : -1);
-        if ((threadIdx.x & 31) == __ffs(same) - 1 && hi >= 0) {
-          atomicMin(&s_rlo[y], lo);
-          atomicMax(&s_rhi[y], hi);
+        for (int j = 0; j < 8; ++j) {
+          const float n = (float)(c[j] >> 24);
+          m[j] = n;
+          v[j] = (float)(c[j] & 0xFFFFFFu) - n * mean0;
+        }
+        if ((c[0] | c[1] | c[2] | c[3] | c[4] | c[5] | c[6] | c[7]) >> 24) s_occ[rem] = 1;
+        const size_t at = (size_t)rem * p.nrot + r0 + k;
+        slotW[at] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                               pack_bf16x2(v[6], v[7]));
+        slotM[at] = make_uint4(pack_bf16x2(m[0], m[1]), pack_bf16x2(m[2], m[3]), pack_bf16x2(m[4], m[5]),
+                               pack_bf16x2(m[6], m[7]));
+        af += daf;
+        y += dy;
+        if (af >= G.nbf) {
+          af -= G.nbf;
+          ++y;
         }
       }
-      const size_t at = (size_t)rem * p.nrot + r0 + k;
-      slotW[at] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
-                             pack_bf16x2(v[6], v[7]));
-      slotM[at] = make_uint4(pack_bf16x2(m[0], m[1]), pack_bf16x2(m[2], m[3]), pack_bf16x2(m[4], m[5]),
-                             pack_bf16x2(m[6], m[7]));
     }
     __syncthreads();
   }
@@ -404,8 +402,14 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
   // any rotation step (an empty row: first > last)
   unsigned char* rng = reinterpret_cast<unsigned char*>(slotM + (size_t)rows * p.nrot);
   if (tid < G.fw) {
-    rng[2 * tid] = (unsigned char)min(s_rlo[tid], 255);
-    rng[2 * tid + 1] = (unsigned char)max(s_rhi[tid], 0);
+    int lo = 255, hi = 0;
+    for (int a = G.nbf - 1; a >= 0; --a)
+      if (s_occ[tid * G.nbf + a]) {
+        lo = a;
+        hi = max(hi, a);
+      }
+    rng[2 * tid] = (unsigned char)lo;
+    rng[2 * tid + 1] = (unsigned char)hi;
   }
 }
 
