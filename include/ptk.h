@@ -316,6 +316,27 @@ typedef struct ptk_tune_report {
 } ptk_tune_report;
 int ptk_autotune(ptk_ctx* ctx, ptk_tune_report* report);
 
+/* Autotune cache (no reference counterpart).  ptk_set_tune_cache(ctx, path)
+ * (path NULL: off) makes ptk_autotune look up the context's workload
+ * signature in the JSON file at path first: an entry for the same search
+ * method whose choice is admissible is taken without timing (report->n = 0);
+ * otherwise ptk_autotune times the candidates as above and writes its result
+ * into the file (created if missing).  The signature names the GPU (compute
+ * capability, name, SM count), the search method, the frame size, the grain
+ * count, the largest pattern radius and the grains per 8-px radius class,
+ * the level-0 zone, rotation steps and topk: ptk_tune_signature writes it to
+ * buf (capacity cap, PTK_ERR_LIMIT when too small).  ptk_tune_cache_lookup /
+ * ptk_tune_cache_store read and update one entry of such a file on the host
+ * (no GPU): lookup sets *found = 0 when the file or the entry is missing;
+ * both return PTK_ERR_IO for a malformed or unwritable file (which they
+ * leave unchanged). */
+int ptk_set_tune_cache(ptk_ctx* ctx, const char* path);
+int ptk_tune_signature(ptk_ctx* ctx, char* buf, int32_t cap);
+int ptk_tune_cache_lookup(const char* path, const char* signature, int32_t* found, int32_t* method,
+                          int32_t* choice);
+int ptk_tune_cache_store(const char* path, const char* signature, int32_t method, int32_t choice, int32_t n,
+                         const int32_t* values, const float* ms);
+
 /* Image files (host only, no GPU).  ptk_read_image_file decodes a strip
  * TIFF (uncompressed, LZW, Deflate or PackBits, optional horizontal
  * predictor; 8/16-bit grey or RGB) into the grey levels that read_tiff_image

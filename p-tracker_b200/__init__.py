@@ -108,6 +108,11 @@ _SIGS = {
     "ptk_synchronize": (C.c_int, [_P]),
     "ptk_kernel_launches": (C.c_int64, [_P]),
     "ptk_test_bf16_wait_timeout": (C.c_int, [_P, C.c_int]),
+    "ptk_set_tune_cache": (C.c_int, [_P, C.c_char_p]),
+    "ptk_tune_signature": (C.c_int, [_P, C.c_char_p, C.c_int32]),
+    "ptk_tune_cache_lookup": (C.c_int, [C.c_char_p, C.c_char_p] + [C.POINTER(C.c_int32)] * 3),
+    "ptk_tune_cache_store": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int32, C.c_int32, C.c_int32,
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "ptk_abi_sizes": (C.c_int, [C.POINTER(C.c_size_t)] * 3),
     "ptk_search_pixel_noalloc": (C.c_int, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int] + [_P] * 8 +
                                  [C.c_int, C.c_int, C.POINTER(Zone), C.c_int] + [_P] * 5),
@@ -348,11 +353,24 @@ class Tracker:
     def autotune(self) -> dict:
         """Times the level-0 search shapes on the loaded frames and keeps the
         fastest (ptk_autotune): {"method": "bf16"|"exact", "choice": value,
-        "candidates": {value: best ms}}."""
+        "candidates": {value: best ms}, "cached": bool} - with a tune cache
+        set and an entry for this workload, nothing is timed ("cached": True,
+        no candidates)."""
         r = TuneReport()
         self._check(self._L.ptk_autotune(self.h, C.byref(r)), self.h)
         return {"method": "bf16" if r.method else "exact", "choice": int(r.choice),
-                "candidates": {int(r.values[k]): float(r.ms[k]) for k in range(r.n)}}
+                "candidates": {int(r.values[k]): float(r.ms[k]) for k in range(r.n)}, "cached": r.n == 0}
+
+    def set_tune_cache(self, path):
+        """JSON file of autotune choices per (GPU, workload) signature
+        (ptk_set_tune_cache); None turns the cache off."""
+        self._check(self._L.ptk_set_tune_cache(self.h, None if path is None else str(path).encode()), self.h)
+
+    def tune_signature(self) -> str:
+        """The autotune cache key of this context's GPU and workload."""
+        buf = C.create_string_buffer(1024)
+        self._check(self._L.ptk_tune_signature(self.h, buf, len(buf)), self.h)
+        return buf.value.decode()
 
     def search_timed(self, level: int = 0) -> list:
         """The level's search with CUDA events between its kernels: per-kernel
@@ -419,6 +437,29 @@ def abi_sizes() -> tuple[int, int, int]:
     a, b, c = C.c_size_t(), C.c_size_t(), C.c_size_t()
     lib().ptk_abi_sizes(C.byref(a), C.byref(b), C.byref(c))
     return a.value, b.value, c.value
+
+
+def tune_cache_lookup(path: str, signature: str):
+    """(method, choice) stored for signature in the autotune cache at path,
+    or None (ptk_tune_cache_lookup)."""
+    found, method, choice = C.c_int32(), C.c_int32(), C.c_int32()
+    rc = lib().ptk_tune_cache_lookup(str(path).encode(), signature.encode(), C.byref(found), C.byref(method),
+                                     C.byref(choice))
+    if rc != PTK_OK:
+        raise PtkError(rc, f"cannot read the autotune cache {path}")
+    return (method.value, choice.value) if found.value else None
+
+
+def tune_cache_store(path: str, signature: str, method: int, choice: int, values=(), ms=()):
+    """Writes one entry of the autotune cache at path (ptk_tune_cache_store)."""
+    n = len(values)
+    if len(ms) != n:
+        raise ValueError("values and ms differ in length")
+    v = (C.c_int32 * max(n, 1))(*[int(x) for x in values])
+    t = (C.c_float * max(n, 1))(*[float(x) for x in ms])
+    rc = lib().ptk_tune_cache_store(str(path).encode(), signature.encode(), int(method), int(choice), n, v, t)
+    if rc != PTK_OK:
+        raise PtkError(rc, f"cannot write the autotune cache {path}")
 
 
 def read_grains_file(path: str, format13: bool = True) -> np.ndarray:

@@ -32,7 +32,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-O3", "--expt-relaxed-constexpr"]
 NO_FMA = {"ptk_remap.cu", "ptk_disto.cu", "ptk_raw.cu", "ptk_subpix.cu"}
 CU_SOURCES = ["ptk_search.cu", "ptk_search_tiled.cu", "ptk_search_bf16.cu", "ptk_subpix_lm.cu", "ptk_subpix.cu", "ptk_remap.cu", "ptk_api.cu", "ptk_noalloc.cu", "ptk_disto.cu", "ptk_raw.cu"]
-CXX_SOURCES = ["grainfile.cpp", "imageio.cpp"]
+CXX_SOURCES = ["grainfile.cpp", "imageio.cpp", "tunecache.cpp"]
 
 
 def _host_cxx() -> str:

@@ -157,6 +157,7 @@ struct ptk_ctx {
   int tune_ring{0};   // BF16 form: operand-row buffers of the search kernel
   int tune_exact{0};  // exact form: 1 register-tiled kernel, 2 direct kernel
   bool tuned{false};
+  std::string tune_cache;  // ptk_set_tune_cache: JSON file of chosen shapes ("" = none)
 
   int iref{0};
   bool need_precompute{true};
@@ -1263,6 +1264,55 @@ int ptk_search_timed(ptk_ctx* c, int level, float* kernel_ms, int max_kernels, i
   return PTK_OK;
 }
 
+// The autotune cache's key: GPU model, search method and the workload's shape.
+static int tune_signature(ptk_ctx* c, const SearchGeom& sg, std::string* out) {
+  int dev = 0;
+  cudaDeviceProp prop{};
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, dev);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaGetDeviceProperties");
+  // grains per 8-px class of pattern extent (ceil of the largest offset norm)
+  std::vector<int> hist;
+  for (const auto& pat : c->h_pat) {
+    double m = 0.0;
+    for (const short2& q : pat) m = std::max(m, std::sqrt((double)q.x * q.x + (double)q.y * q.y));
+    const size_t k = (size_t)std::ceil(m) / 8;
+    if (hist.size() <= k) hist.resize(k + 1, 0);
+    ++hist[k];
+  }
+  std::string name(prop.name);
+  for (char& ch : name)
+    if ((unsigned char)ch < 0x20 || (unsigned char)ch >= 0x7F || ch == '|') ch = '_';
+  const ptk_zone& z = c->cfg.zone[0];
+  char b[256];
+  snprintf(b, sizeof b, "sm_%d%d %s x%d|%s|frame %dx%d|grains %d|rmax %d|zone %d,%d,%d,%d|nrot %d|topk %d|r8", prop.major,
+           prop.minor, name.c_str(), prop.multiProcessorCount, sg.bf16 ? "bf16" : "exact", c->cfg.dimx, c->cfg.dimy,
+           c->n, c->max_R, z.left, z.right, z.up, z.down, sg.nrot, c->cfg.topk);
+  std::string sig(b);
+  for (size_t k = 0; k < hist.size(); ++k) sig += (k ? "," : " ") + std::to_string(hist[k]);
+  *out = sig;
+  return PTK_OK;
+}
+
+int ptk_set_tune_cache(ptk_ctx* c, const char* path) {
+  if (!c) return fail(c, PTK_ERR_ARG, "null context");
+  c->tune_cache = path ? path : "";
+  return PTK_OK;
+}
+
+int ptk_tune_signature(ptk_ctx* c, char* buf, int32_t cap) {
+  if (!c || !buf || cap < 1) return fail(c, PTK_ERR_ARG, "ptk_tune_signature: null context or buffer");
+  int rc = check_ready(c, true);
+  if (rc) return rc;
+  SearchGeom sg;
+  if ((rc = search_geometry(c, 0, &sg))) return rc;
+  std::string sig;
+  if ((rc = tune_signature(c, sg, &sig))) return rc;
+  if ((int64_t)sig.size() + 1 > cap) return fail(c, PTK_ERR_LIMIT, "ptk_tune_signature: buffer too small");
+  memcpy(buf, sig.c_str(), sig.size() + 1);
+  return PTK_OK;
+}
+
 int ptk_autotune(ptk_ctx* c, ptk_tune_report* report) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
   int rc = check_ready(c, true);
@@ -1286,6 +1336,25 @@ int ptk_autotune(ptk_ctx* c, ptk_tune_report* report) {
     if (search_smem_bytes(c->max_P, span * span) <= 227 * 1024) cand.push_back(2);
   }
   if (cand.empty()) return fail(c, PTK_ERR_STATE, "no admissible search shape");
+  std::string sig;
+  if (!c->tune_cache.empty()) {
+    if ((rc = tune_signature(c, sg, &sig))) return rc;
+    int32_t found = 0, m = 0, ch = 0;
+    if (ptk_tune_cache_lookup(c->tune_cache.c_str(), sig.c_str(), &found, &m, &ch) != PTK_OK)
+      return fail(c, PTK_ERR_IO, "autotune cache unreadable or malformed");
+    if (found && m == method && std::find(cand.begin(), cand.end(), (int)ch) != cand.end()) {
+      if (method) c->tune_ring = ch;
+      else c->tune_exact = ch;
+      c->tuned = true;
+      invalidate(c);
+      if (report) {
+        report->method = method;
+        report->choice = ch;
+        report->n = 0;  // taken from the cache, nothing timed
+      }
+      return PTK_OK;
+    }
+  }
   BlockLayout L(c->n);
   void* snap = nullptr;
   void* flush = nullptr;  // written before every run: each starts with the L2 state a frame sees
@@ -1350,6 +1419,12 @@ int ptk_autotune(ptk_ctx* c, ptk_tune_report* report) {
       report->values[k] = cand[(size_t)k];
       report->ms[k] = best[(size_t)k];
     }
+  }
+  if (!c->tune_cache.empty()) {
+    std::vector<int32_t> vals(cand.begin(), cand.end());
+    if (ptk_tune_cache_store(c->tune_cache.c_str(), sig.c_str(), method, cand[k_best], (int32_t)cand.size(),
+                             vals.data(), best.data()) != PTK_OK)
+      return fail(c, PTK_ERR_IO, "autotune cache could not be written");
   }
   return PTK_OK;
 }

@@ -54,16 +54,30 @@ __global__ void k_precompute(GrainsDev g, FrameDev ref) {
   const int rx = g.refx[gi], ry = g.refy[gi];
   long long S0 = 0, S00 = 0;
   int oob = 0;
-  for (int i = threadIdx.x; i < P; i += blockDim.x) {
-    const short2 q = rotate_round(g.pat[b + i], c0r, s0r);
-    g.pat0[b + i] = q;
-    const int x = rx + q.x, y = ry + q.y;
-    unsigned v = 0;
-    if (x < 0 || y < 0 || x >= ref.dimx || y >= ref.dimy) oob = 1;
-    else v = ref.pix[(size_t)y * ref.pitch + x];
-    g.w0[b + i] = (uint16_t)v;
-    S0 += v;
-    S00 += (long long)v * v;
+  // four points per thread at a time, so that their pixel loads are in flight
+  // together (the integer sums do not depend on the order)
+  const int nt = blockDim.x;
+  for (int i0 = threadIdx.x; i0 < P; i0 += 4 * nt) {
+    unsigned v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * nt;
+      v[u] = 0;
+      if (i >= P) continue;
+      const short2 q = rotate_round(g.pat[b + i], c0r, s0r);
+      g.pat0[b + i] = q;
+      const int x = rx + q.x, y = ry + q.y;
+      if (x < 0 || y < 0 || x >= ref.dimx || y >= ref.dimy) oob = 1;
+      else v[u] = ref.pix[(size_t)y * ref.pitch + x];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * nt;
+      if (i >= P) continue;
+      g.w0[b + i] = (uint16_t)v[u];
+      S0 += v[u];
+      S00 += (long long)v[u] * v[u];
+    }
   }
   __shared__ long long red[2][32];
   __shared__ int s_oob;

@@ -16,6 +16,8 @@
 //     lm_cell PX STEPS                    LM results beyond this cell go to Powell (0 0: none)
 //     autotune 0 | 1                       time the level-0 search shapes
 //                                          before the first frame (ptk_autotune)
+//     autotune_cache FILE                  JSON file of autotune choices per GPU
+//                                          and workload (ptk_set_tune_cache)
 //     undistort_images 0 | 1               resample every frame with the
 //                                          *_corrDistor / *_corrParallax
 //                                          parameters before tracking
@@ -71,7 +73,7 @@ struct PatternOp {
 };
 
 struct Settings {
-  std::string image_name = "%d.tif", dic_name, procedure = "particle_tracking";
+  std::string image_name = "%d.tif", dic_name, procedure = "particle_tracking", tune_cache;
   int iref = 0, ibeg = 0, iend = 0, iinc = 0;
   int raw_images = 0, undistort = 0;
   ptk_config cfg;
@@ -412,6 +414,8 @@ Settings read_commands(const char* path) {
       in >> s.cfg.lm_cell_px >> s.cfg.lm_cell_rot;
     } else if (tok == "autotune") {
       in >> s.cfg.autotune;
+    } else if (tok == "autotune_cache") {
+      in >> s.tune_cache;
     } else if (tok == "undistort_images") {
       in >> s.undistort;
     } else {
@@ -473,6 +477,7 @@ void print_json(const Settings& s) {
     o << (i ? ", " : "") << "[" << s.patterns[i].kind << ", " << s.patterns[i].a << ", " << s.patterns[i].b << ", "
       << s.patterns[i].target << ", \"" << s.patterns[i].file << "\"]";
   o << "], \"search_method\": " << c.search_method << ", \"autotune\": " << c.autotune
+    << ", \"autotune_cache\": \"" << s.tune_cache << "\""
     << ", \"subpix_method\": " << c.subpix_method
     << ", \"undistort_images\": " << s.undistort << ", \"disto\": [";
   for (int k = 0; k < 14; ++k) o << (k ? ", " : "") << s.disto[k];
@@ -683,6 +688,7 @@ int main(int argc, char** argv) {
     if (rc) die(std::string(what) + ": " + ptk_last_error(ctx));
   };
   ck(ptk_create(&ctx, &s.cfg), "ptk_create");
+  if (!s.tune_cache.empty()) ck(ptk_set_tune_cache(ctx, s.tune_cache.c_str()), "ptk_set_tune_cache");
   const int n = (int)s.grains.size();
   ck(ptk_set_grains(ctx, s.grains.data(), n), "ptk_set_grains");
   for (const PatternOp& op : s.patterns) {

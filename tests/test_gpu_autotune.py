@@ -49,3 +49,39 @@ def test_autotune_keeps_results(ptk, wl, pair_cache, cuda_device, form):
     auto.track_frame(1)
     np.testing.assert_array_equal(auto.get_grains(), want)
     auto.close()
+
+
+def test_autotune_cache(ptk, wl, pair_cache, cuda_device, tmp_path):
+    """With a tune cache, the first context times the candidates and records
+    its choice under the workload's signature; a second context on the same
+    workload takes the recorded choice without timing, and tracks to the same
+    results."""
+    pair = pair_cache("small16", seed=31)
+    form = dict(search_method=1, subpix_method=1)
+    cache = tmp_path / "tune.json"
+    t = _tracker(ptk, wl, pair, **form)
+    t.set_tune_cache(cache)
+    sig = t.tune_signature()
+    assert sig.startswith("sm_") and "|bf16|" in sig and "|grains " in sig
+    rep = t.autotune()
+    assert not rep["cached"] and rep["candidates"]
+    assert ptk.tune_cache_lookup(cache, sig) == (1, rep["choice"])
+    t.track_frame(1)
+    want = t.get_grains()
+    t.close()
+    u = _tracker(ptk, wl, pair, **form)
+    u.set_tune_cache(cache)
+    assert u.tune_signature() == sig
+    rep2 = u.autotune()
+    assert rep2["cached"] and rep2["choice"] == rep["choice"] and not rep2["candidates"]
+    u.track_frame(1)
+    np.testing.assert_array_equal(u.get_grains(), want)
+    u.close()
+    # an entry for another form is not taken: the exact form times its own candidates
+    e = _tracker(ptk, wl, pair, search_method=0)
+    e.set_tune_cache(cache)
+    assert "|exact|" in e.tune_signature()
+    assert not e.autotune()["cached"]
+    e.close()
+    data = __import__("json").loads(cache.read_text())
+    assert len(data["entries"]) == 2
