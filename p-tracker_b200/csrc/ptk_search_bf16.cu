@@ -482,6 +482,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
     }
   }
   int zhalf = -1;  // footprint geometry whose zero blocks the operand rows hold
+  int pf_next = -1;   // thread 0: the next work item, taken before this one's epilogue (-1: none)
+  bool pf = false;    // thread 0: its first operand rows and image strip are already on their way
 
   const GrainsDev& g = p.g;
   const int count = *p.list_count;
@@ -491,7 +493,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
   for (;;) {
     __syncthreads();  // every thread is done with the previous grain's shared state
     if (tid == 0) {
-      s_li = atomicAdd(p.work_next, 1);
+      s_li = pf_next >= 0 ? pf_next : atomicAdd(p.work_next, 1);
+      pf_next = -1;
       s_bb[0] = s_bb[2] = INT_MAX;
       s_bb[1] = s_bb[3] = INT_MIN;
     }
@@ -618,14 +621,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
       // or footprint pixels whose weights are zero in every rotation step.
       const int nwin = 8 * G.hb;
       const int Xa = Xi & ~7, xoff = Xi - Xa;
-      auto stage_rows = [&](int ys_) {  // thread 0
+      auto stage_rows_at = [&](int xa, int yi, int ys_) {  // thread 0
         const int boxes = (min(G.rs, G.fw - ys_) + 31 + kStageBoxRows - 1) / kStageBoxRows;
         const uint32_t sb = smem_u32(&s_stage);
         mbar_expect_tx(sb, (uint32_t)(boxes * kStageBoxRows * G.rp));
         for (int j = 0; j < boxes; ++j)
-          tma_load_2d(rbase + (uint32_t)(j * kStageBoxRows * G.rp), fmap, Xa, Yi + ys_ + j * kStageBoxRows, sb);
+          tma_load_2d(rbase + (uint32_t)(j * kStageBoxRows * G.rp), fmap, xa, yi + ys_ + j * kStageBoxRows, sb);
         s_stage_out = 1;
       };
+      auto stage_rows = [&](int ys_) { stage_rows_at(Xa, Yi, ys_); };
       auto wait_rows = [&]() {  // thread 0 (a wait that gives up leaves the staging to the drain)
         if (mbar_wait(smem_u32(&s_stage), sparity)) {
           s_stage_out = 0;
@@ -640,7 +644,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
       // buffer before (nb rows earlier), and is issued nb - 1 rows ahead of its
       // MMAs, so the copies overlap the fills and MMAs.
       const int NB = G.nb;
-      auto issue_row = [&](int y) -> bool {  // thread 0
+      auto issue_row_of = [&](const CUtensorMap* tm, int y) -> bool {  // thread 0
         const int k = y % NB;
         const unsigned use = s_iss[k];
         if (use > 0 && !mbar_wait(smem_u32(&s_free[k]), (use - 1) & 1u)) return false;
@@ -649,19 +653,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
         const uint32_t dst = abase + (uint32_t)(k * 2 * G.wb * 512 + 3 * 512);
         // footprint row y of W (coordinate 4 = 0) and of M (1): nbf blocks of
         // 32 rotation slots x 8 values, 512 bytes per block
-        tma_load_5d(dst, tmap, 0, 0, 0, y, 0, full);
-        tma_load_5d(dst + (uint32_t)(G.wb * 512), tmap, 0, 0, 0, y, 1, full);
+        tma_load_5d(dst, tm, 0, 0, 0, y, 0, full);
+        tma_load_5d(dst + (uint32_t)(G.wb * 512), tm, 0, 0, 0, y, 1, full);
         s_iss[k] = use + 1;
         return true;
       };
-      if (tid == 0)
+      auto issue_row = [&](int y) -> bool { return issue_row_of(tmap, y); };
+      if (tid == 0 && !pf) {  // (a prefetched item's first rows and strip were issued during the last epilogue)
         for (int y = 0; y < min(NB - 1, G.fw); ++y)
           if (!issue_row(y)) {
             s_err = 1;
             atomicOr(p.error, 1);
             break;
           }
-      if (tid == 0 && !s_err) stage_rows(0);
+        if (!s_err) stage_rows(0);
+      }
+      pf = false;
       uint32_t acc = 0u;  // the tile's first MMA into each accumulator overwrites it
       for (int ys = 0; ys < G.fw; ys += G.rs) {
         const int nr = min(G.rs, G.fw - ys);
@@ -752,6 +759,41 @@ __global__ void __launch_bounds__(kThreads, 1) k_search_bf16(Bf16Launch p) {
         if (s_err) break;
       }
       if (s_err) break;
+
+      // Prefetch (thread 0): the next work item is taken now and, when its
+      // grain has this footprint geometry (same shared-memory layout, zero
+      // blocks in place) and its tile lies in the frame by the +-(half - 1)
+      // bound (so that it is searched, not skipped), its first operand rows
+      // and its first strip's image rows are issued into the ring and the
+      // staging rows, which this tile no longer reads, to land during this
+      // tile's epilogue.
+      if (tid == 0) {
+        pf_next = atomicAdd(p.work_next, 1);
+        const int li2 = pf_next / tiles, t2 = pf_next - li2 * tiles;
+        if (li2 < count) {
+          const int gi2 = p.list[li2];
+          const int P2 = g.pstart[gi2 + 1] - g.pstart[gi2];
+          if (!(g.masked[gi2] || (g.flags[gi2] & 2) || P2 <= 0 || P2 > kMaxPatternPoints) && p.half[gi2] == G.half) {
+            const int tu2 = t2 / p.tiles_v, tv2 = t2 - tu2 * p.tiles_v;
+            const int u0b = -p.left + tu2 * kTileU, u1b = min(u0b + kTileU - 1, p.right);
+            const int v0b = -p.up + tv2 * kTileV, v1b = min(v0b + kTileV - 1, p.down);
+            const int X2 = g.refx[gi2] + (int)round(g.dx[gi2]), Y2 = g.refy[gi2] + (int)round(g.dy[gi2]);
+            const int e = G.half - 1;
+            if (X2 - e + u0b >= 0 && Y2 - e + v0b >= 0 && X2 + e + u1b < p.cur.dimx && Y2 + e + v1b < p.cur.dimy) {
+              const CUtensorMap* tm2 = p.tmaps + gi2;
+              asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tm2) : "memory");
+              pf = true;
+              for (int y = 0; y < min(NB - 1, G.fw); ++y)
+                if (!issue_row_of(tm2, y)) {
+                  s_err = 1;
+                  atomicOr(p.error, 1);
+                  break;
+                }
+              if (!s_err) stage_rows_at((X2 - G.half + u0b) & ~7, Y2 - G.half + v0b, 0);
+            }
+          }
+        }
+      }
 
       // ---- epilogue: per rotation lane D / sqrt(S), max over rotations, keep the best candidates
       const int q = warp & 3, h = warp >> 2;  // TMEM lane quadrant (x shift j) and column quarter
