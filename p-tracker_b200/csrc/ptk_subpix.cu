@@ -3,11 +3,11 @@
 //
 // The objective (objective_exact) follows the reference's FP64 operations
 // (src/p-tracker.cpp:1018-1088, src/interpol.cpp:19-144) in their order and
-// without FMA contraction (this file is compiled with -fmad=false); only its
-// three sums over the pattern points are taken in parallel and rounded once
-// (correctly rounded, where the reference rounds after every point), and
-// cos / sin come from ptk_crtrig.cuh.  Inside Powell the frame region under
-// the grain is staged in shared memory.
+// without FMA contraction (this file is compiled with -fmad=false): the
+// interpolated values are computed in parallel, and its sums run over the
+// pattern points in point order, rounded after every point, as the
+// reference's loops round them; cos / sin come from ptk_crtrig.cuh.  Inside
+// Powell the frame region under the grain is staged in shared memory.
 //
 // One CTA of kSubpixThreads refines one grain.  The Powell driver
 // (follow_pattern_subpixel_xyR, src/p-tracker.cpp:1090-1128; the minimiser
@@ -183,10 +183,9 @@ __device__ __forceinline__ double patch_px(const Patch& pt, int x, int y) {
 // cosine and sine of the last rotation angle.
 struct ExactObj {
   const uint16_t* w0;    // P reference values (staged)
-  double* bcast;         // 8 doubles: [3] cos, [4] sin, [5] C0C0, [6] [7] sum of d0 (double-double)
-  double* red2;          // 6 doubles per warp: the block sums' partials
+  double* v;             // P interpolated values of the current evaluation (shared memory)
+  double* bcast;         // 8 doubles: [0] the evaluation's NCC, [3] cos, [4] sin, [5] C0C0
   double inv_num_pix;    // 1 / P
-  double sd0_hi, sd0_lo; // sum over the points of d0_i = (double)I0_i - mean0, double-double
   double last_rot, c1, s1;
 };
 
@@ -201,95 +200,19 @@ __device__ double c0c0_in_order(const uint16_t* w0, int P, double mean0) {
   return c;
 }
 
-// Compensated summation (Ogita, Rump and Oishi, "Accurate sum and dot
-// product", SIAM J. Sci. Comput. 26 (2005), algorithm Sum2): s + c carries the
-// running sum to about twice the working precision, so the final s + c is the
-// exact sum rounded once (up to an error far below half an ulp), whatever the
-// order the terms come in.  Each step is Knuth's error-free two-sum; this file
-// is compiled without FMA contraction, which none of it uses anyway.
-struct Sum2 {
-  double s = 0.0, c = 0.0;
-  __device__ __forceinline__ void add(double x) {
-    const double t = s + x;
-    const double bp = t - s;
-    c += (s - (t - bp)) + (x - bp);
-    s = t;
-  }
-  __device__ __forceinline__ void add(const Sum2& o) {
-    add(o.s);
-    c += o.c;
-  }
-};
-
-// The block's three Sum2 partials combined in a fixed order (lanes by a
-// butterfly, then the warps in index order): every thread returns the same
-// three double-double sums, normalised (hi + lo with |lo| <= ulp(hi) / 2).
-template <int NT>
-__device__ __forceinline__ void block_sum2x3(Sum2 v[3], double* red2, crtrig::dd out[3]) {
-  for (int o = 16; o > 0; o >>= 1) {
-    // both lanes of a pair combine the same two values in the same order
-    const bool lo = (threadIdx.x & o) == 0;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      Sum2 w;
-      w.s = __shfl_xor_sync(0xffffffffu, v[k].s, o);
-      w.c = __shfl_xor_sync(0xffffffffu, v[k].c, o);
-      Sum2 a = lo ? v[k] : w, b = lo ? w : v[k];
-      a.add(b);
-      v[k] = a;
-    }
-  }
-  const int wp = threadIdx.x >> 5;
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      red2[6 * wp + 2 * k] = v[k].s;
-      red2[6 * wp + 2 * k + 1] = v[k].c;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    Sum2 t;
-#pragma unroll
-    for (int w = 0; w < NT / 32; ++w) {
-      Sum2 x;
-      x.s = red2[6 * w + 2 * k];
-      x.c = red2[6 * w + 2 * k + 1];
-      t.add(x);
-    }
-    out[k] = crtrig::fast_two_sum(t.s, t.c);
-  }
-}
-
-// a / d for a double-double a and a double d (one correction step).
-__device__ __forceinline__ crtrig::dd dd_div_d(crtrig::dd a, double d) {
-  const double q1 = a.hi / d;
-  const crtrig::dd p = crtrig::two_prod(q1, d);
-  const double r = ((a.hi - p.hi) - p.lo) + a.lo;
-  return crtrig::fast_two_sum(q1, r / d);
-}
-
-// NCC_to_minimize_xyR (src/p-tracker.cpp:1018-1088) in one pass over the
-// points: the sample positions xpix1 + c1 x + s1 y and ypix1 - s1 x + c1 y and
-// the interpolators in the reference's operations and order, every product and
-// sum rounded separately (this file is compiled without FMA contraction), cos /
-// sin correctly rounded (ptk_crtrig.cuh) where the host C library is within an
-// ulp; and the reference's two-pass sums
-//     mean1 = (sum v) / P,  C1C1 = sum (v - mean1)^2,  C0C1 = sum d0 (v - mean1)
-// (d0 = I0 - mean0, rounded as the reference rounds it) from the exact sums
-// sum v, sum v^2 and sum d0 v - each product split exactly by a fused
-// multiply-add, the terms added with compensation (Sum2), the block's
-// partials combined in a fixed order - as
-//     C1C1 = sum v^2 - (sum v)^2 / P,  C0C1 = sum d0 v - (sum v)(sum d0) / P
-// evaluated in double-double and rounded once.  Each is the exact value of
-// the reference's expression with the exact mean (the reference rounds after
-// every point instead, and centres on the rounded mean1, a difference of
-// P (mean1 - sum v / P)^2, far below its own rounding), so the objective
-// differs from the reference's only by the reference's own rounding.  Called
-// by every thread of the block with the same X; returns the same value on
-// every thread.
+// NCC_to_minimize_xyR (src/p-tracker.cpp:1018-1088): the sample positions
+// xpix1 + c1 x + s1 y and ypix1 - s1 x + c1 y and the interpolators in the
+// reference's operations and order, every product and sum rounded separately
+// (this file is compiled without FMA contraction), cos / sin correctly
+// rounded (ptk_crtrig.cuh) where the host C library is within an ulp.  The
+// block's threads interpolate the points in parallel into shared memory; one
+// thread then runs the reference's two loops over them in point order,
+//     mean1 = (sum v) * (1 / P),  C0C1 = sum d0 (v - mean1),  C1C1 = sum (v - mean1)^2
+// (d0 = I0 - mean0), each sum rounded after every point as the reference's
+// loops round it, so that the value is the reference's bit for bit and Powell
+// takes the reference's path even where the objective is flat.  Called by
+// every thread of the block with the same X; returns the same value on every
+// thread.
 template <int NT>
 __device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const SubpixParams& sp,
                                   const ObjGrain& o, const Patch& pt, ExactObj& ex, const double X[3],
@@ -307,7 +230,6 @@ __device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const
     ex.last_rot = rot;
   }
   const double c1 = ex.c1, s1 = ex.s1;
-  Sum2 acc[3];  // sum v, sum v^2, sum d0 v
   for (int i = tid; i < o.P; i += NT) {
     const short2 q = g.pat0[o.b + i];
     const double x = (double)q.x, y = (double)q.y;
@@ -329,21 +251,27 @@ __device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const
     } else {
       v = interp(cur, sp.interp, xs, ys, clamped);
     }
-    const double d0 = (double)ex.w0[i] - o.mean0;
-    acc[0].add(v);
-    const double vv = v * v, d0v = d0 * v;
-    acc[1].add(vv);
-    acc[1].c += fma(v, v, -vv);  // the products' rounding errors, exact by the fused multiply-add
-    acc[2].add(d0v);
-    acc[2].c += fma(d0, v, -d0v);
+    ex.v[i] = v;
   }
-  crtrig::dd S[3];
-  block_sum2x3<NT>(acc, ex.red2, S);
-  const double P = (double)o.P;
-  const crtrig::dd sumd0{ex.sd0_hi, ex.sd0_lo};
-  const crtrig::dd c11 = crtrig::dd_add(S[1], crtrig::dd_neg(dd_div_d(crtrig::dd_mul(S[0], S[0]), P)));
-  const crtrig::dd c01 = crtrig::dd_add(S[2], crtrig::dd_neg(dd_div_d(crtrig::dd_mul(S[0], sumd0), P)));
-  const double ncc = (c01.hi + c01.lo) / sqrt(o.c0c0 * (c11.hi + c11.lo));
+  __syncthreads();
+  if (tid == 0) {
+    const double* v = ex.v;
+    double mean1 = 0.0;
+#pragma unroll 8
+    for (int i = 0; i < o.P; ++i) mean1 += v[i];
+    mean1 *= ex.inv_num_pix;
+    double c01 = 0.0, c11 = 0.0;
+#pragma unroll 8
+    for (int i = 0; i < o.P; ++i) {
+      const double d1 = v[i] - mean1;
+      const double d0 = (double)ex.w0[i] - o.mean0;
+      c01 += d0 * d1;
+      c11 += d1 * d1;
+    }
+    ex.bcast[0] = c01 / sqrt(o.c0c0 * c11);
+  }
+  __syncthreads();
+  const double ncc = ex.bcast[0];
   double W = 1.0;
   const double disp = sqrt(X[0] * X[0] + X[1] * X[1]);
   if (disp > sp.disp_max) W = sp.stiffness * (disp - sp.disp_max) + 1.0;
@@ -351,19 +279,9 @@ __device__ double objective_exact(const GrainsDev& g, const FrameDev& cur, const
 }
 
 // Once per grain: C0C0 as do_precomputations sums it (point order, each step
-// rounded; src/p-tracker.cpp:646-651) in bcast[5], and the double-double sum
-// of the points' d0 in bcast[6..7].  Every thread must call it.
-template <int NT>
-__device__ void grain_sums(const uint16_t* w0, int P, double mean0, double* bcast, double* red2) {
+// rounded; src/p-tracker.cpp:646-651) in bcast[5].  Every thread must call it.
+__device__ void grain_sums(const uint16_t* w0, int P, double mean0, double* bcast) {
   if (threadIdx.x == 0) bcast[5] = c0c0_in_order(w0, P, mean0);
-  Sum2 acc[3];
-  for (int i = threadIdx.x; i < P; i += NT) acc[0].add((double)w0[i] - mean0);
-  crtrig::dd S[3];
-  block_sum2x3<NT>(acc, red2, S);
-  if (threadIdx.x == 0) {
-    bcast[6] = S[0].hi;
-    bcast[7] = S[0].lo;
-  }
   __syncthreads();
 }
 
@@ -620,7 +538,8 @@ __device__ void powell_minimize(F& f, double p[3], const double step[3], double 
 
 // Dynamic shared memory of the Powell kernel: the staged frame region (its
 // cap in uint16 elements first), then per pattern point its uint16 reference
-// value.
+// value, then per pattern point the interpolated value of the current
+// evaluation (double).
 struct PowellSmem {
   int patch_cap;   // elements of the staged frame region
   int max_points;  // largest pattern of the grains
@@ -631,15 +550,20 @@ __host__ __device__ inline size_t powell_vals_offset(int patch_cap) {
   return ((size_t)patch_cap * sizeof(uint16_t) + 15) & ~(size_t)15;
 }
 
+// bytes of the staged reference values, padded so that the interpolated
+// values (doubles) after them stay 16-byte aligned
+__host__ __device__ inline size_t powell_w0_bytes(int max_points) {
+  return ((size_t)max_points * sizeof(uint16_t) + 15) & ~(size_t)15;
+}
+
 // follow_pattern_subpixel_xyR (src/p-tracker.cpp:1090-1128) for every grain,
 // one block per grain, grains taken in `order` (decreasing pattern size) when
 // given.
-__global__ void __launch_bounds__(kSubpixThreads, 5) k_subpix_powell(GrainsDev g, FrameDev cur, SubpixParams sp,
+__global__ void __launch_bounds__(kSubpixThreads, 3) k_subpix_powell(GrainsDev g, FrameDev cur, SubpixParams sp,
                                                                        int patch_cap, int max_points,
                                                                        const int* order, const int* list_count) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double bcast[8];
-  __shared__ double red2[6 * (kSubpixThreads / 32)];
   __shared__ int s_clamped, s_bb[4];
   if (list_count && (int)blockIdx.x >= *list_count) return;
   const int gi = order ? order[blockIdx.x] : (int)blockIdx.x;
@@ -655,6 +579,7 @@ __global__ void __launch_bounds__(kSubpixThreads, 5) k_subpix_powell(GrainsDev g
   __syncthreads();
   uint16_t* s_patch = reinterpret_cast<uint16_t*>(smem);
   uint16_t* s_w0 = reinterpret_cast<uint16_t*>(smem + powell_vals_offset(patch_cap));
+  double* s_v = reinterpret_cast<double*>(smem + powell_vals_offset(patch_cap) + powell_w0_bytes(max_points));
   int xmn = 1 << 30, xmx = -(1 << 30), ymn = 1 << 30, ymx = -(1 << 30);
   for (int i = threadIdx.x; i < o.P; i += kSubpixThreads) {
     const short2 q = g.pat0[o.b + i];
@@ -680,11 +605,10 @@ __global__ void __launch_bounds__(kSubpixThreads, 5) k_subpix_powell(GrainsDev g
     s_patch[e] = cur.pix[(size_t)(py0 + yy) * cur.pitch + (px0 + xx)];
   }
   __syncthreads();
-  grain_sums<kSubpixThreads>(s_w0, o.P, o.mean0, bcast, red2);
+  grain_sums(s_w0, o.P, o.mean0, bcast);
   o.c0c0 = bcast[5];
   const Patch pt{s_patch, px0, py0, pw, ph};
-  ExactObj ex{s_w0, bcast, red2, 1.0 / (double)o.P, bcast[6], bcast[7], __longlong_as_double(0x7ff8000000000000ll),
-              0.0, 0.0};
+  ExactObj ex{s_w0, s_v, bcast, 1.0 / (double)o.P, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0};
   bool clamped = false;
   PowellEval<kSubpixThreads> f{&g, &cur, &sp, &o, &pt, &ex, &clamped, 0};
   double X[3] = {0.0, 0.0, 0.0};
@@ -712,7 +636,6 @@ __global__ void __launch_bounds__(kSubpixThreads) k_objective(GrainsDev g, Frame
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[kSubpixThreads / 32];
   __shared__ double bcast[8];
-  __shared__ double red2[6 * (kSubpixThreads / 32)];
   const int gi = blockIdx.x;
   ObjGrain o = load_grain(g, gi);
   if (o.P <= 0 || o.P > max_points) {
@@ -736,13 +659,13 @@ __global__ void __launch_bounds__(kSubpixThreads) k_objective(GrainsDev g, Frame
     }
   } else {
     uint16_t* s_w0 = reinterpret_cast<uint16_t*>(smem);
+    double* s_v = reinterpret_cast<double*>(smem + powell_w0_bytes(max_points));
     for (int i = threadIdx.x; i < o.P; i += kSubpixThreads) s_w0[i] = g.w0[o.b + i];
     __syncthreads();
-    grain_sums<kSubpixThreads>(s_w0, o.P, o.mean0, bcast, red2);
+    grain_sums(s_w0, o.P, o.mean0, bcast);
     o.c0c0 = bcast[5];
     const Patch none{nullptr, 0, 0, 0, 0};
-    ExactObj ex{s_w0, bcast, red2, 1.0 / (double)o.P, bcast[6], bcast[7], __longlong_as_double(0x7ff8000000000000ll),
-                0.0, 0.0};
+    ExactObj ex{s_w0, s_v, bcast, 1.0 / (double)o.P, __longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0};
     val = objective_exact<kSubpixThreads>(g, cur, sp, o, none, ex, X, &clamped);
   }
   if (threadIdx.x == 0) f[gi] = val;
@@ -752,7 +675,7 @@ static PowellSmem powell_smem(int max_points, int max_r) {
   PowellSmem m;
   const size_t side = (size_t)(2 * max_r + 1 + 2 * 6 + 2);
   size_t patch = side * side;
-  const size_t rest = (size_t)max_points * sizeof(uint16_t);
+  const size_t rest = powell_w0_bytes(max_points) + (size_t)max_points * sizeof(double);
   constexpr size_t kCap = 227 * 1024 - 1024;  // the kernel's static shared memory included
   if (powell_vals_offset((int)patch) + rest > kCap)
     patch = rest < kCap ? (kCap - rest) / sizeof(uint16_t) - 8 : 0;  // samples outside the region read the frame
@@ -765,8 +688,10 @@ static PowellSmem powell_smem(int max_points, int max_r) {
 void prepare_subpix(int max_points, int max_r) {
   const PowellSmem m = powell_smem(max_points, max_r);
   ensure_smem((const void*)k_subpix_powell, m.bytes);
-  const size_t b = (size_t)max_points * sizeof(double) * 3;
-  if (b <= 227 * 1024) ensure_smem((const void*)k_objective, b);
+  // the objective alone: reference and interpolated values; with the gradient: three doubles per point
+  const size_t bf = powell_w0_bytes(max_points) + (size_t)max_points * sizeof(double);
+  const size_t bg = (size_t)max_points * sizeof(double) * 3;
+  ensure_smem((const void*)k_objective, bg <= 227 * 1024 && bg > bf ? bg : bf);
 }
 
 void launch_subpix_powell(const GrainsDev& g, const FrameDev& cur, const FrameDev& /*ref*/, const SubpixParams& sp,
@@ -781,7 +706,8 @@ void launch_objective(const GrainsDev& g, const FrameDev& cur, const SubpixParam
                       double* grad, int max_points, cudaStream_t s) {
   if (g.n <= 0) return;
   prepare_subpix(max_points, 0);
-  const size_t smem = grad ? (size_t)max_points * sizeof(double) * 3 : (size_t)max_points * sizeof(uint16_t);
+  const size_t smem = grad ? (size_t)max_points * sizeof(double) * 3
+                           : powell_w0_bytes(max_points) + (size_t)max_points * sizeof(double);
   k_objective<<<g.n, kSubpixThreads, smem, s>>>(g, cur, sp, X, f, grad, max_points);
 }
 
