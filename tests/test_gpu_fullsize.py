@@ -7,8 +7,9 @@ the bench's own pair (seed 1000), every grain:
   * exact and BF16 pixel stages: the same integer offset and rotation step on
     every grain whose two best NCC values differ by more than 1e-6, NCC within
     1e-5;
-  * plain form (exact search + Powell): subpixel positions within 1e-3 px and
-    rotations within 1e-4 rad;
+  * plain form (exact search + Powell): subpixel positions within 1e-5 px and
+    rotations within 1e-6 rad (the bar is 1e-3 px / 1e-4 rad; the objective
+    repeats the reference's arithmetic, so Powell takes its path);
   * headline form (BF16 search + adjoint LM): within 0.01 px and 1e-4 rad.
 cfg4 (cfg2 with noise of 5 % of the range): the FP64 and FP32 adjoint
 gradients of 1 - NCC on 200 sampled grains against the FP64 CPU gradient and
@@ -85,8 +86,8 @@ def test_cfg2_plain_form_all_grains(ptk, wl, oracle, cuda_device, cfg2, cfg2_cpu
     g = t.get_grains()
     t.close()
     clear = (top2[:, 0] - top2[:, 1]) > 1e-6
-    assert np.abs(g[clear, 4:6] - sub[clear, 4:6]).max() <= 1e-3
-    assert np.abs(g[clear, 6] - sub[clear, 6]).max() <= 1e-4
+    assert np.abs(g[clear, 4:6] - sub[clear, 4:6]).max() <= 1e-5
+    assert np.abs(g[clear, 6] - sub[clear, 6]).max() <= 1e-6
     assert np.abs(g[clear, 12] - sub[clear, 12]).max() <= 1e-5
 
 

@@ -6,7 +6,9 @@ the same remapped frames (the remap is bit-exact to the oracle's).
 
 Headline form (BF16 search + adjoint LM): same integer positions and rescue
 counts as the oracle's exact search, positions within 0.01 px and rotations
-within 1e-4 rad of its FP64 Powell.  Plain form: within 1e-3 px / 1e-4 rad."""
+within 1e-4 rad of its FP64 Powell.  Plain form: within 1e-5 px / 1e-6 rad
+(its objective is the reference's bit for bit wherever the C library's cos /
+sin are correctly rounded, so Powell takes the reference's path)."""
 from __future__ import annotations
 
 import os
@@ -34,7 +36,7 @@ def long_seq(wl):
     return wl.make_sequence(p, seed=11, frames=24)
 
 
-def _track(ptk, wl, oracle, s, tol_px, **form):
+def _track(ptk, wl, oracle, s, tol_px, tol_rad=1e-4, **form):
     p = s["params"]
     o = wl.tracker_options(p)
     X = s["disto"]
@@ -66,7 +68,7 @@ def _track(ptk, wl, oracle, s, tol_px, **form):
         rescued += len(res)
         np.testing.assert_array_equal(gr[:, 0:2], cr[:, 0:2])
         assert np.abs(gr[:, 4:6] - cr[:, 4:6]).max() <= tol_px, f"frame {k}"
-        assert np.abs(gr[:, 2] + gr[:, 6] - cr[:, 2] - cr[:, 6]).max() <= 1e-4, f"frame {k}"
+        assert np.abs(gr[:, 2] + gr[:, 6] - cr[:, 2] - cr[:, 6]).max() <= tol_rad, f"frame {k}"
     assert rescued > 0, "the jumps must trigger rescue searches"
     return t
 
@@ -76,11 +78,11 @@ def test_sequence_headline_form(ptk, wl, oracle, cuda_device, seq):
 
 
 def test_sequence_plain_form(ptk, wl, oracle, cuda_device, seq):
-    _track(ptk, wl, oracle, seq, 1e-3)
+    _track(ptk, wl, oracle, seq, 1e-5, 1e-6)
 
 
 def test_long_sequence_plain_form(ptk, wl, oracle, cuda_device, long_seq):
     """The plain form along 23 reference changes: every grain-frame within
-    1e-3 px and 1e-4 rad of the oracle (the device objective and Powell repeat
+    1e-5 px and 1e-6 rad of the oracle (the device objective and Powell repeat
     the reference's operations, so the two trajectories do not drift apart)."""
-    _track(ptk, wl, oracle, long_seq, 1e-3)
+    _track(ptk, wl, oracle, long_seq, 1e-5, 1e-6)
