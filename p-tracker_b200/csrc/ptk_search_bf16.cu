@@ -349,15 +349,17 @@ __global__ void __launch_bounds__(kWThreads) k_weights_bf16(Bf16Launch p) {
           const float yf = fmaf(cf.x, pyf, -(cf.y * pxf));
           const float mx = xf + 12582912.0f, my = yf + 12582912.0f;
           int qx = __float_as_int(mx) - 0x4B400000, qy = __float_as_int(my) - 0x4B400000;
-          if (!(fabsf(xf - (mx - 12582912.0f)) < 0.499f && fabsf(yf - (my - 12582912.0f)) < 0.499f)) {
+          // the float rounding is the FP64 one unless a coordinate lies within
+          // 0.001 of a half-integer (the inputs are finite)
+          if (!(fmaxf(fabsf(xf - (mx - 12582912.0f)), fabsf(yf - (my - 12582912.0f))) < 0.499f)) {
             const double2 cd = s_cs[r0 + k];
             const short2 q = rotate_round_b(q0[u], cd.x, cd.y);
             qx = q.x;
             qy = q.y;
           }
-          // |q| <= ceil(|p|) = half - 1: always inside the footprint
-          if ((unsigned)(qx + G.half) < (unsigned)G.fw && (unsigned)(qy + G.half) < (unsigned)G.fw)
-            atomicAdd(mk + qy * fwp + qx, add[u]);
+          // |q| <= round(|p|) <= ceil(max |offset|) = half - 1 in each
+          // coordinate, for every rotation: always inside the footprint
+          atomicAdd(mk + qy * fwp + qx, add[u]);
         }
       }
     }
