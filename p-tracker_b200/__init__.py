@@ -439,6 +439,35 @@ def abi_sizes() -> tuple[int, int, int]:
     return a.value, b.value, c.value
 
 
+class _PinnedBuffer:
+    """Page-locked host memory from ptk_host_alloc, freed with the last array
+    that views it (numpy keeps this object as the array's base)."""
+
+    def __init__(self, shape, dtype):
+        dt = np.dtype(dtype)
+        nbytes = max(int(np.prod(shape)) * dt.itemsize, 1)
+        self.ptr = C.c_void_p()
+        rc = lib().ptk_host_alloc(C.byref(self.ptr), nbytes)
+        if rc != PTK_OK:
+            raise PtkError(rc, "ptk_host_alloc")
+        self.__array_interface__ = {"shape": tuple(shape), "typestr": dt.str, "data": (self.ptr.value, False),
+                                    "version": 3}
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and self.ptr.value:
+            lib().ptk_host_free(self.ptr)
+            self.ptr = None
+
+
+def pinned_copy(a: np.ndarray) -> np.ndarray:
+    """A copy of `a` in page-locked host memory, so that Tracker.load_frame
+    uploads it asynchronously (from pageable memory an upload is synchronous)."""
+    a = np.ascontiguousarray(a)
+    out = np.asarray(_PinnedBuffer(a.shape, a.dtype))
+    out[...] = a
+    return out
+
+
 def tune_cache_lookup(path: str, signature: str):
     """(method, choice) stored for signature in the autotune cache at path,
     or None (ptk_tune_cache_lookup)."""

@@ -67,13 +67,20 @@ struct ptk_ctx {
   cudaStream_t stream{nullptr};
   cudaStream_t own_stream{nullptr};
   cudaStream_t cap_stream{nullptr};
-  // Host uploads of the current frame go to copy_stream, after the work
-  // already on the context stream (main_mark), and record cur_ready; the
-  // frame's graph waits for cur_ready just before its first kernel that reads
-  // the current frame, every other reader at its entry (sync_cur).
-  cudaStream_t copy_stream{nullptr};
-  cudaEvent_t cur_ready{nullptr}, main_mark{nullptr};
-  bool cur_pending{false};
+  // Host uploads into frame buffer p go to copy_stream[p] and record
+  // buf_ready[p].  An upload waits for the buffer's last reader: when the
+  // last work queued on the context stream is a frame graph (tail_is_graph),
+  // that is the graph's record of buf_free[p] (right after the precompute
+  // for the reference buffer, at the end for the current one); otherwise all
+  // the work queued so far (main_mark).  A frame's graph waits for the
+  // current buffer's upload just before its first kernel that reads it, for
+  // the reference buffer's before the graph; every other reader at its entry
+  // (sync_cur).
+  cudaStream_t copy_stream[2]{nullptr, nullptr};
+  cudaEvent_t buf_ready[2]{nullptr, nullptr}, buf_free[2]{nullptr, nullptr}, main_mark{nullptr};
+  bool ready_pending[2]{false, false};
+  bool free_valid[2]{false, false};
+  bool tail_is_graph{false};
   std::string err;
   int64_t launches{0};
 
@@ -196,10 +203,15 @@ void invalidate(ptk_ctx* c) { c->graph_dirty = true; }
 // The context stream waits for a current-frame upload still in flight on the
 // copy stream (entry of every call that reads the current frame or reuses
 // its staging outside a frame's graph).
+// The context stream waits for every pending frame upload; the work that
+// follows is no longer a frame graph's alone.
 void sync_cur(ptk_ctx* c) {
-  if (!c->cur_pending) return;
-  cudaStreamWaitEvent(c->stream, c->cur_ready, 0);
-  c->cur_pending = false;
+  c->tail_is_graph = false;
+  for (int p = 0; p < 2; ++p)
+    if (c->ready_pending[p]) {
+      cudaStreamWaitEvent(c->stream, c->buf_ready[p], 0);
+      c->ready_pending[p] = false;
+    }
 }
 
 FrameDev frame(const ptk_ctx* c, int phys) {
@@ -718,16 +730,24 @@ int prepare_searches(ptk_ctx* c) {
 }
 
 // Enqueues one frame body; `swap` decided by the caller.
+// Captured into the frame's graph: the reference buffer's last reader is the
+// precompute (buf_free recorded after it), the current buffer's the graph's
+// end.
 int enqueue_frame(ptk_ctx* c, bool precompute, bool swap, cudaStream_t s) {
   int rc;
-  if (precompute && (rc = enqueue_precompute(c, s))) return rc;
-  if (c->cfg.rescue_level >= 0 && (rc = enqueue_search(c, 0, s, nullptr, c->cur_ready))) return rc;
-  if (c->cfg.rescue_level < 0) cudaStreamWaitEvent(s, c->cur_ready, cudaEventWaitExternal);
+  const int ref_phys = c->ref_slot, cur_phys = c->cur_slot;
+  if (precompute) {
+    if ((rc = enqueue_precompute(c, s))) return rc;
+    cudaEventRecordWithFlags(c->buf_free[ref_phys], s, cudaEventRecordExternal);
+  }
+  if (c->cfg.rescue_level >= 0 && (rc = enqueue_search(c, 0, s, nullptr, c->buf_ready[cur_phys]))) return rc;
+  if (c->cfg.rescue_level < 0) cudaStreamWaitEvent(s, c->buf_ready[cur_phys], cudaEventWaitExternal);
   if (c->cfg.rescue_level >= 1 && (rc = enqueue_search(c, 1, s))) return rc;
   if (c->cfg.rescue_level >= 2 && (rc = enqueue_search(c, 2, s))) return rc;
   if (c->cfg.subpixel && (rc = enqueue_subpixel(c, c->cfg.subpix_method, s))) return rc;
   launch_end_frame(c->g, swap ? 1 : 0, s);
   c->launches += 1;
+  cudaEventRecordWithFlags(c->buf_free[cur_phys], s, cudaEventRecordExternal);
   return PTK_OK;
 }
 
@@ -784,9 +804,12 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
   e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
-  e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
-  e = cudaEventCreateWithFlags(&c->cur_ready, cudaEventDisableTiming);
+  for (int p = 0; p < 2 && e == cudaSuccess; ++p) {
+    e = cudaStreamCreateWithFlags(&c->copy_stream[p], cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
+    e = cudaEventCreateWithFlags(&c->buf_ready[p], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->buf_free[p], cudaEventDisableTiming);
+  }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->main_mark, cudaEventDisableTiming);
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaEventCreate"));
   c->stream = c->own_stream;
@@ -825,7 +848,8 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
 int ptk_destroy(ptk_ctx* c) {
   if (!c) return PTK_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+  for (int p = 0; p < 2; ++p)
+    if (c->copy_stream[p]) cudaStreamSynchronize(c->copy_stream[p]);
   drop_graphs(c);
   cudaFree(c->d_img[0]);
   cudaFree(c->d_img[1]);
@@ -862,8 +886,11 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_gr);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
-  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
-  if (c->cur_ready) cudaEventDestroy(c->cur_ready);
+  for (int p = 0; p < 2; ++p) {
+    if (c->copy_stream[p]) cudaStreamDestroy(c->copy_stream[p]);
+    if (c->buf_ready[p]) cudaEventDestroy(c->buf_ready[p]);
+    if (c->buf_free[p]) cudaEventDestroy(c->buf_free[p]);
+  }
   if (c->main_mark) cudaEventDestroy(c->main_mark);
   delete c;
   return PTK_OK;
@@ -1084,29 +1111,30 @@ int ptk_load_frame(ptk_ctx* c, int slot, const void* pix, int dimx, int dimy, in
   if (bpp != 1 && bpp != 2) return fail(c, PTK_ERR_ARG, "bytes_per_px must be 1 or 2");
   if (pitch_bytes < (size_t)dimx * bpp) return fail(c, PTK_ERR_ARG, "pitch smaller than a row");
   const int phys = slot == 0 ? c->ref_slot : c->cur_slot;
-  sync_cur(c);  // a previous current-frame upload (and its 8-bit staging) is done first
-  if (!c->d_u8 && bpp == 1) CK(cudaMalloc(&c->d_u8, (size_t)c->pitch * dimy));
-  // the current frame goes up on the copy stream, after the work queued so far
-  // (which may still read that slot); the reference frame on the context stream
-  cudaStream_t cs = c->stream;
-  if (slot == 1) {
+  // The upload waits for the buffer's last reader: a frame graph's record of
+  // buf_free when the graph is the last work queued, else all queued work.
+  const bool after_graph = c->tail_is_graph && c->free_valid[phys];
+  cudaStream_t cs = c->copy_stream[phys];
+  if (after_graph) {
+    CK(cudaStreamWaitEvent(cs, c->buf_free[phys], 0));
+  } else {
     CK(cudaEventRecord(c->main_mark, c->stream));
-    CK(cudaStreamWaitEvent(c->copy_stream, c->main_mark, 0));
-    cs = c->copy_stream;
+    CK(cudaStreamWaitEvent(cs, c->main_mark, 0));
   }
+  if (!c->d_u8 && bpp == 1) CK(cudaMalloc(&c->d_u8, (size_t)c->pitch * dimy));
   if (bpp == 2) {
     CK(cudaMemcpy2DAsync(c->d_img[phys], (size_t)c->pitch * 2, pix, pitch_bytes, (size_t)dimx * 2, dimy,
                          cudaMemcpyHostToDevice, cs));
   } else {
+    // the 8-bit staging buffer is shared: after the other buffer's last upload
+    CK(cudaStreamWaitEvent(cs, c->buf_ready[1 - phys], 0));
     CK(cudaMemcpy2DAsync(c->d_u8, (size_t)c->pitch, pix, pitch_bytes, (size_t)dimx, dimy, cudaMemcpyHostToDevice,
                          cs));
     launch_widen_u8(c->d_u8, (size_t)c->pitch, c->d_img[phys], c->pitch, dimx, dimy, cs);
     c->launches += 1;
   }
-  if (slot == 1) {
-    CK(cudaEventRecord(c->cur_ready, cs));
-    c->cur_pending = true;
-  }
+  CK(cudaEventRecord(c->buf_ready[phys], cs));
+  c->ready_pending[phys] = true;
   c->loaded[slot] = true;
   if (slot == 0) c->need_precompute = true;
   return PTK_OK;
@@ -1506,8 +1534,19 @@ int ptk_track_frame(ptk_ctx* c, int num_image) {
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
     c->launches = before;  // counted again at each replay below
   }
+  const int ref_phys = c->ref_slot, cur_phys = c->cur_slot;
+  c->tail_is_graph = false;  // (set again once the graph is queued)
+  if (c->ready_pending[ref_phys]) {  // the precompute reads the reference buffer first
+    CK(cudaStreamWaitEvent(c->stream, c->buf_ready[ref_phys], 0));
+    c->ready_pending[ref_phys] = false;
+  }
   CK(cudaGraphLaunch(c->graph[key], c->stream));
-  c->cur_pending = false;  // the graph waited for the upload before reading the frame
+  c->ready_pending[cur_phys] = false;  // the graph waits for it before its first kernel reading the frame
+  // the graph records each buffer's release: the reference after its
+  // precompute (none without one), the current one at its end
+  c->tail_is_graph = true;
+  c->free_valid[ref_phys] = pre;
+  c->free_valid[cur_phys] = true;
   // launches of one frame: precompute, stage_begin, (search, finalize) per level,
   // subpixel, end_frame
   int64_t nk = (pre ? 1 : 0) + 1;
