@@ -578,10 +578,15 @@ def run_sequence(args, rank: int, world: int, local: int) -> int:
         e1 = torch.cuda.Event(enable_timing=True)
         stream.synchronize()
         e0.record(stream)
+        # the next frame is handed over before the current one's records are
+        # read back: its upload (into the old reference's buffer) overlaps the
+        # tracking from the end of the precompute on
+        t.load_frame(1, pinned[1])
         for k in range(1, nf):
-            t.load_frame(1, pinned[k])
             t.remap(1)
             t.track_frame(k)
+            if k + 1 < nf:
+                t.load_frame(1, pinned[k + 1])
             out = t.get_grains()
         e1.record(stream)
         e1.synchronize()

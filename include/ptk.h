@@ -148,7 +148,13 @@ int ptk_pattern_size(ptk_ctx* ctx, int grain, int* npts);
  * im_index_ref / im_index_current], src/p-tracker.hpp:80-83).  `pix` is a
  * row-major host buffer of 1- or 2-byte grey levels with `pitch_bytes` per
  * row; 1-byte values are widened to uint16 unchanged.  Replaces read_image
- * (src/p-tracker.cpp:75-83) after decode. */
+ * (src/p-tracker.cpp:75-83) after decode.  The copy runs on a copy stream of
+ * the frame buffer it fills: after a queued ptk_track_frame it waits only
+ * until that frame no longer reads the buffer (the reference buffer after
+ * its precompute, the current one at the frame's end), otherwise until all
+ * queued work is done; calls that read the frame wait for the copy.  `pix`
+ * must stay unchanged until a frame that reads it has been tracked and its
+ * records read back, or ptk_synchronize has returned. */
 int ptk_load_frame(ptk_ctx* ctx, int slot, const void* pix, int dimx, int dimy, int bytes_per_px,
                    size_t pitch_bytes);
 /* Same with a device pointer (uint16, row-major, pitch in bytes). */

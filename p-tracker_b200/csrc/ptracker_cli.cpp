@@ -825,16 +825,36 @@ int main(int argc, char** argv) {
   };
   refill();
   std::vector<ptk_grain> out((size_t)n);
+  // The next frame is handed to the library right after the current one is
+  // queued, before its records are read back, so that its upload overlaps the
+  // tracking; it stays alive (its pinned buffer unchanged) until it is tracked.
+  Frame next;
+  bool have_next = false;
+  auto take = [&]() {
+    Frame f = ahead.front().get();
+    ahead.pop_front();
+    if (f.rc) die(f.error);
+    refill();
+    return f;
+  };
   for (int num = s.ibeg; num <= s.iend; num += s.iinc) {
     const double t0 = now();
-    Frame cur = ahead.front().get();
-    ahead.pop_front();
-    if (cur.rc) die(cur.error);
-    refill();
+    Frame cur;
+    if (have_next) {
+      cur = std::move(next);
+      have_next = false;
+    } else {
+      cur = take();
+      load(1, cur);
+    }
     std::printf("\n____ Correlations from image %d towards image %d (%d/%d)\n", iref, num, num - s.ibeg + 1,
                 s.iend - s.ibeg + 1);
-    load(1, cur);
     ck(ptk_track_frame(ctx, num), "ptk_track_frame");
+    if (num + s.iinc <= s.iend) {
+      next = take();
+      load(1, next);  // into the buffer the queued frame reads last (the old reference after a change)
+      have_next = true;
+    }
     ck(ptk_get_grains(ctx, out.data(), n), "ptk_get_grains");  // waits for the frame
     int nres = 0, nsup = 0;
     ck(ptk_get_rescue_counts(ctx, &nres, &nsup), "ptk_get_rescue_counts");
