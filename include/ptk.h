@@ -11,8 +11,9 @@
  * Ownership: the caller owns every host array passed in or out; the context
  * owns its device memory and one CUDA stream (or borrows a caller stream, see
  * ptk_set_stream).  A context is not thread-safe; distinct contexts are
- * independent.  All device work of a call is enqueued on the context stream;
- * calls that return host data synchronise that stream.
+ * independent.  All device work of a call is enqueued on the context stream
+ * (host frame uploads on the context's copy streams, ordered with it, see
+ * ptk_load_frame); calls that return host data synchronise that stream.
  */
 #ifndef PTK_H
 #define PTK_H
