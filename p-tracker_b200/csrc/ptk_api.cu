@@ -1238,6 +1238,7 @@ int ptk_precompute(ptk_ctx* c) {
   int rc = check_ready(c, false);
   if (rc) return rc;
   if (!c->loaded[0]) return fail(c, PTK_ERR_STATE, "reference frame not loaded");
+  sync_cur(c);  // the reference frame's upload first
   rc = enqueue_precompute(c, c->stream);
   if (rc) return rc;
   c->need_precompute = false;

@@ -61,3 +61,30 @@ def test_pipelined_loads_give_the_same_records(ptk, wl, pair_cache, cuda_device,
         np.testing.assert_array_equal(a, b, err_msg=f"pair {k}")
     # the four pairs give four different results (the uploads matter)
     assert not np.array_equal(want[0], want[1])
+
+
+def test_stagewise_calls_wait_for_the_uploads(ptk, wl, pair_cache, cuda_device):
+    """The stage-by-stage calls (precompute, search, subpixel) issued right
+    after asynchronous uploads from page-locked memory read the new frames:
+    the same records as with the frames uploaded from ordinary memory."""
+    cases = [pair_cache("small16", seed=s) for s in (51, 52, 53)]
+    p, rec = cases[0]["params"], cases[0]["rec"]
+    kw = dict(search_method=ptk.SEARCH_EXACT, subpix_method=ptk.SUBPIX_POWELL)
+
+    def run(pinned):
+        t = _tracker(ptk, wl, p, rec, 1000, **kw)
+        out = []
+        for c in cases:
+            ref, cur = (ptk.pinned_copy(c["ref"]), ptk.pinned_copy(c["cur"])) if pinned else (c["ref"], c["cur"])
+            t.set_grains(rec)
+            t.load_frame(0, ref)
+            t.load_frame(1, cur)
+            t.precompute()
+            t.search(0)
+            t.subpixel(ptk.SUBPIX_POWELL)
+            out.append(t.get_grains())
+        t.close()
+        return out
+
+    for k, (a, b) in enumerate(zip(run(False), run(True))):
+        np.testing.assert_array_equal(a, b, err_msg=f"pair {k}")
