@@ -841,7 +841,7 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg2")
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--ref-sample", type=int, default=0, help="grains per reference-arm step (0: 32 per host thread)")
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="grains of the CPU baseline (0: all, up to 200 per host thread; cfg5: 20 per host thread)")

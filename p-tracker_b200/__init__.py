@@ -447,6 +447,7 @@ class _PinnedBuffer:
         dt = np.dtype(dtype)
         nbytes = max(int(np.prod(shape)) * dt.itemsize, 1)
         self.ptr = C.c_void_p()
+        self._free = lib().ptk_host_free  # kept: module globals may be gone when the last array dies
         rc = lib().ptk_host_alloc(C.byref(self.ptr), nbytes)
         if rc != PTK_OK:
             raise PtkError(rc, "ptk_host_alloc")
@@ -455,7 +456,7 @@ class _PinnedBuffer:
 
     def __del__(self):
         if getattr(self, "ptr", None) and self.ptr.value:
-            lib().ptk_host_free(self.ptr)
+            self._free(self.ptr)
             self.ptr = None
 
 

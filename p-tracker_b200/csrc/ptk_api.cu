@@ -36,6 +36,7 @@ cudaError_t ptk::ensure_smem(const void* func, size_t bytes) {
 namespace {
 
 constexpr int kMaxRotSteps = 4096;
+constexpr int kFrameBufs = 3;  // device frame buffers: the two slots and a spare for overlapped uploads
 thread_local std::string g_static_error;
 
 // Layout of the grain block: 16 double fields, 2 int64 fields, 3 int32 fields,
@@ -67,32 +68,36 @@ struct ptk_ctx {
   cudaStream_t stream{nullptr};
   cudaStream_t own_stream{nullptr};
   cudaStream_t cap_stream{nullptr};
-  // Host uploads into frame buffer p go to copy_stream[p] and record
-  // buf_ready[p].  An upload waits for the buffer's last reader: when the
-  // last work queued on the context stream is a frame graph (tail_is_graph),
-  // that is the graph's record of buf_free[p] (right after the precompute
-  // for the reference buffer, at the end for the current one); otherwise all
-  // the work queued so far (main_mark).  A frame's graph waits for the
-  // current buffer's upload just before its first kernel that reads it, for
-  // the reference buffer's before the graph; every other reader at its entry
-  // (sync_cur).
-  cudaStream_t copy_stream[2]{nullptr, nullptr};
-  cudaEvent_t buf_ready[2]{nullptr, nullptr}, buf_free[2]{nullptr, nullptr}, main_mark{nullptr};
-  bool ready_pending[2]{false, false};
-  bool free_valid[2]{false, false};
-  bool tail_is_graph{false};
+  // Three frame buffers: the reference and current slots' and a spare.  Host
+  // uploads into buffer p go to copy_stream[p] and record buf_ready[p].  An
+  // upload waits for the buffer's last reader: while free_valid[p], that is a
+  // frame graph's record of buf_free[p] (right after its precompute for the
+  // reference buffer, at its end for the current one, and nothing since);
+  // otherwise all the work queued so far (main_mark).  An upload into a slot
+  // may go to the spare buffer instead when the spare is released earlier
+  // (the slot then uses the spare, and its old buffer becomes the spare).  A
+  // frame's graph waits for the current buffer's upload just before its first
+  // kernel that reads it, for the reference buffer's before the graph; every
+  // other reader at its entry (sync_cur).
+  cudaStream_t copy_stream[kFrameBufs]{};
+  cudaEvent_t buf_ready[kFrameBufs]{}, buf_free[kFrameBufs]{}, main_mark{nullptr};
+  bool ready_pending[kFrameBufs]{};
+  bool free_valid[kFrameBufs]{};
+  bool released_early[kFrameBufs]{};  // the latest graph using it released it after its precompute
+  int64_t used_by_graph[kFrameBufs]{};  // sequence number of the latest graph that read it
+  int64_t graph_seq{0};
   std::string err;
   int64_t launches{0};
 
   // frames
   int pitch{0};
-  uint16_t* d_img[2]{nullptr, nullptr};
+  uint16_t* d_img[kFrameBufs]{};
   uint16_t* d_tmp{nullptr};
   uint8_t* d_u8{nullptr};
   uint16_t* d_raw{nullptr};  // staging of a host RAW mosaic (ptk_load_frame_raw)
   size_t raw_cap{0};         // elements
   unsigned* d_minmax{nullptr};
-  int ref_slot{0}, cur_slot{1};
+  int ref_slot{0}, cur_slot{1}, spare_buf{2};  // frame buffers of the slots, and the spare
   bool loaded[2]{false, false};
 
   // grains
@@ -156,8 +161,8 @@ struct ptk_ctx {
   double* d_f{nullptr};
   double* d_gr{nullptr};
 
-  // per-frame graphs, keyed by (ref_slot, precompute, swap)
-  cudaGraphExec_t graph[8]{};
+  // per-frame graphs, keyed by (reference buffer, current buffer, precompute, swap)
+  cudaGraphExec_t graph[kFrameBufs * kFrameBufs * 4]{};
   bool graph_dirty{true};
 
   // level-0 search shape chosen by ptk_autotune (0: the built-in choice)
@@ -203,11 +208,22 @@ void invalidate(ptk_ctx* c) { c->graph_dirty = true; }
 // The context stream waits for a current-frame upload still in flight on the
 // copy stream (entry of every call that reads the current frame or reuses
 // its staging outside a frame's graph).
+// After the context stream was synchronised from the host, no queued work
+// reads any frame buffer any more (uploads into a buffer stay ordered on its
+// copy stream): an upload need not wait for anything else.
+void all_released(ptk_ctx* c) {
+  for (int b = 0; b < kFrameBufs; ++b) {
+    c->free_valid[b] = true;
+    c->used_by_graph[b] = 0;
+  }
+}
+
 // The context stream waits for every pending frame upload; the work that
 // follows is no longer a frame graph's alone.
 void sync_cur(ptk_ctx* c) {
-  c->tail_is_graph = false;
-  for (int p = 0; p < 2; ++p)
+  // the slots' buffers may be read or written by the work that follows
+  c->free_valid[c->ref_slot] = c->free_valid[c->cur_slot] = false;
+  for (int p = 0; p < kFrameBufs; ++p)
     if (c->ready_pending[p]) {
       cudaStreamWaitEvent(c->stream, c->buf_ready[p], 0);
       c->ready_pending[p] = false;
@@ -804,7 +820,7 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
   e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
-  for (int p = 0; p < 2 && e == cudaSuccess; ++p) {
+  for (int p = 0; p < kFrameBufs && e == cudaSuccess; ++p) {
     e = cudaStreamCreateWithFlags(&c->copy_stream[p], cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamCreate"));
     e = cudaEventCreateWithFlags(&c->buf_ready[p], cudaEventDisableTiming);
@@ -815,15 +831,22 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
   c->stream = c->own_stream;
   c->pitch = (cfg->dimx + 63) & ~63;
   const size_t bytes = (size_t)c->pitch * cfg->dimy * sizeof(uint16_t);
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < kFrameBufs; ++k) {
     e = cudaMalloc(&c->d_img[k], bytes);
     if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(frame)"));
     cudaMemset(c->d_img[k], 0, bytes);
   }
-  {  // the BF16 search's tensor maps of both frame buffers (left unset without the driver's encoder)
-    CUtensorMap h[2 * kBf16FrameMaps];
-    if (bf16_encode_frame_tmaps(c->d_img[0], cfg->dimx, cfg->dimy, c->pitch, h) &&
-        bf16_encode_frame_tmaps(c->d_img[1], cfg->dimx, cfg->dimy, c->pitch, h + kBf16FrameMaps)) {
+  // no work has read the buffers yet (the zeroing above is finished): an
+  // upload into any of them need not wait
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaDeviceSynchronize"));
+  for (int k = 0; k < kFrameBufs; ++k) c->free_valid[k] = true;
+  {  // the BF16 search's tensor maps of the frame buffers (left unset without the driver's encoder)
+    CUtensorMap h[kFrameBufs * kBf16FrameMaps];
+    bool ok = true;
+    for (int k = 0; k < kFrameBufs && ok; ++k)
+      ok = bf16_encode_frame_tmaps(c->d_img[k], cfg->dimx, cfg->dimy, c->pitch, h + k * kBf16FrameMaps);
+    if (ok) {
       e = cudaMalloc(&c->d_frame_tmaps, sizeof(h));
       if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(frame maps)"));
       e = cudaMemcpy(c->d_frame_tmaps, h, sizeof(h), cudaMemcpyHostToDevice);
@@ -848,11 +871,10 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
 int ptk_destroy(ptk_ctx* c) {
   if (!c) return PTK_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (int p = 0; p < 2; ++p)
+  for (int p = 0; p < kFrameBufs; ++p)
     if (c->copy_stream[p]) cudaStreamSynchronize(c->copy_stream[p]);
   drop_graphs(c);
-  cudaFree(c->d_img[0]);
-  cudaFree(c->d_img[1]);
+  for (int k = 0; k < kFrameBufs; ++k) cudaFree(c->d_img[k]);
   cudaFree(c->d_tmp);
   cudaFree(c->d_u8);
   cudaFree(c->d_raw);
@@ -886,7 +908,7 @@ int ptk_destroy(ptk_ctx* c) {
   cudaFree(c->d_gr);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
-  for (int p = 0; p < 2; ++p) {
+  for (int p = 0; p < kFrameBufs; ++p) {
     if (c->copy_stream[p]) cudaStreamDestroy(c->copy_stream[p]);
     if (c->buf_ready[p]) cudaEventDestroy(c->buf_ready[p]);
     if (c->buf_free[p]) cudaEventDestroy(c->buf_free[p]);
@@ -928,7 +950,9 @@ int ptk_set_search_zone(ptk_ctx* c, int level, const ptk_zone* z) {
 int ptk_set_grains(ptk_ctx* c, const ptk_grain* grains, int n) {
   if (!c || (n > 0 && !grains) || n < 0) return fail(c, PTK_ERR_ARG, "bad grain arguments");
   CK(cudaStreamSynchronize(c->stream));
-  if (n != c->n) {
+  all_released(c);
+  const bool resized = n != c->n;
+  if (resized) {
     cudaFree(c->d_block);
     cudaFree(c->d_snap);
     cudaFree(c->d_lists);
@@ -980,7 +1004,9 @@ int ptk_set_grains(ptk_ctx* c, const ptk_grain* grains, int n) {
   if (n) CK(cudaMemcpyAsync(c->d_block, h, L.total, cudaMemcpyHostToDevice, c->stream));
   bind_grains(c);
   c->need_precompute = true;
-  invalidate(c);
+  // the frame graphs hold the grain block's addresses, which change only with
+  // the grain count: new values for as many grains keep them
+  if (resized) invalidate(c);
   return PTK_OK;
 }
 
@@ -990,6 +1016,7 @@ int ptk_get_grains(ptk_ctx* c, ptk_grain* out, int n) {
   if (n == 0) return PTK_OK;
   BlockLayout L(n);
   CK(cudaStreamSynchronize(c->stream));
+  all_released(c);
   int rc = ensure_stage(c, L.total);
   if (rc) return rc;
   const char* h = static_cast<const char*>(c->h_stage);
@@ -1110,10 +1137,20 @@ int ptk_load_frame(ptk_ctx* c, int slot, const void* pix, int dimx, int dimy, in
   if (dimx != c->cfg.dimx || dimy != c->cfg.dimy) return fail(c, PTK_ERR_ARG, "frame size differs from the context");
   if (bpp != 1 && bpp != 2) return fail(c, PTK_ERR_ARG, "bytes_per_px must be 1 or 2");
   if (pitch_bytes < (size_t)dimx * bpp) return fail(c, PTK_ERR_ARG, "pitch smaller than a row");
-  const int phys = slot == 0 ? c->ref_slot : c->cur_slot;
   // The upload waits for the buffer's last reader: a frame graph's record of
-  // buf_free when the graph is the last work queued, else all queued work.
-  const bool after_graph = c->tail_is_graph && c->free_valid[phys];
+  // buf_free while that is valid, else all queued work.  Of the slot's buffer
+  // and the spare, the one released first takes it: one the latest graph did
+  // not read, then one it released after its precompute, then one it
+  // released at its end, then one waiting for all queued work.
+  auto release_rank = [&](int b) {
+    if (!c->free_valid[b]) return 3;
+    if (c->used_by_graph[b] < c->graph_seq) return 0;
+    return c->released_early[b] ? 1 : 2;
+  };
+  int& slot_buf = slot == 0 ? c->ref_slot : c->cur_slot;
+  if (release_rank(c->spare_buf) < release_rank(slot_buf)) std::swap(slot_buf, c->spare_buf);
+  const int phys = slot_buf;
+  const bool after_graph = c->free_valid[phys];
   cudaStream_t cs = c->copy_stream[phys];
   if (after_graph) {
     CK(cudaStreamWaitEvent(cs, c->buf_free[phys], 0));
@@ -1126,8 +1163,9 @@ int ptk_load_frame(ptk_ctx* c, int slot, const void* pix, int dimx, int dimy, in
     CK(cudaMemcpy2DAsync(c->d_img[phys], (size_t)c->pitch * 2, pix, pitch_bytes, (size_t)dimx * 2, dimy,
                          cudaMemcpyHostToDevice, cs));
   } else {
-    // the 8-bit staging buffer is shared: after the other buffer's last upload
-    CK(cudaStreamWaitEvent(cs, c->buf_ready[1 - phys], 0));
+    // the 8-bit staging buffer is shared: after the other buffers' last uploads
+    for (int b = 0; b < kFrameBufs; ++b)
+      if (b != phys) CK(cudaStreamWaitEvent(cs, c->buf_ready[b], 0));
     CK(cudaMemcpy2DAsync(c->d_u8, (size_t)c->pitch, pix, pitch_bytes, (size_t)dimx, dimy, cudaMemcpyHostToDevice,
                          cs));
     launch_widen_u8(c->d_u8, (size_t)c->pitch, c->d_img[phys], c->pitch, dimx, dimy, cs);
@@ -1512,7 +1550,7 @@ int ptk_track_frame(ptk_ctx* c, int num_image) {
   if (c->graph_dirty) drop_graphs(c);
   const bool pre = c->need_precompute;
   const bool swap = num_image - c->iref >= c->cfg.iraz;
-  const int key = (c->ref_slot ? 4 : 0) | (pre ? 2 : 0) | (swap ? 1 : 0);
+  const int key = ((c->ref_slot * kFrameBufs + c->cur_slot) * 2 + (pre ? 1 : 0)) * 2 + (swap ? 1 : 0);
   if (!c->graph[key]) {
     // all attribute and occupancy queries happen before capture
     for (int l = 0; l <= c->cfg.rescue_level && l < 3; ++l) {
@@ -1536,7 +1574,6 @@ int ptk_track_frame(ptk_ctx* c, int num_image) {
     c->launches = before;  // counted again at each replay below
   }
   const int ref_phys = c->ref_slot, cur_phys = c->cur_slot;
-  c->tail_is_graph = false;  // (set again once the graph is queued)
   if (c->ready_pending[ref_phys]) {  // the precompute reads the reference buffer first
     CK(cudaStreamWaitEvent(c->stream, c->buf_ready[ref_phys], 0));
     c->ready_pending[ref_phys] = false;
@@ -1545,9 +1582,12 @@ int ptk_track_frame(ptk_ctx* c, int num_image) {
   c->ready_pending[cur_phys] = false;  // the graph waits for it before its first kernel reading the frame
   // the graph records each buffer's release: the reference after its
   // precompute (none without one), the current one at its end
-  c->tail_is_graph = true;
+  ++c->graph_seq;
+  c->used_by_graph[ref_phys] = c->used_by_graph[cur_phys] = c->graph_seq;
   c->free_valid[ref_phys] = pre;
+  c->released_early[ref_phys] = pre;
   c->free_valid[cur_phys] = true;
+  c->released_early[cur_phys] = false;
   // launches of one frame: precompute, stage_begin, (search, finalize) per level,
   // subpixel, end_frame
   int64_t nk = (pre ? 1 : 0) + 1;
@@ -1660,6 +1700,7 @@ int ptk_synchronize(ptk_ctx* c) {
   if (!c) return fail(c, PTK_ERR_ARG, "null context");
   sync_cur(c);
   CK(cudaStreamSynchronize(c->stream));
+  all_released(c);
   int flag = 0;  // set by a device wait that gave up (BF16 search)
   CK(cudaMemcpy(&flag, c->d_counts + 3, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {
