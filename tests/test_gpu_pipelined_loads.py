@@ -88,3 +88,30 @@ def test_stagewise_calls_wait_for_the_uploads(ptk, wl, pair_cache, cuda_device):
 
     for k, (a, b) in enumerate(zip(run(False), run(True))):
         np.testing.assert_array_equal(a, b, err_msg=f"pair {k}")
+
+
+def test_slots_read_back_what_was_loaded(ptk, wl, pair_cache, cuda_device):
+    """With uploads moving slots between the three frame buffers, each slot
+    reads back the frame last loaded into it - right after the load, after a
+    tracked frame and after reference changes - and the records match a loop
+    that waits for every step."""
+    cases = [pair_cache("small16", seed=s) for s in (61, 62, 63, 64, 65)]
+    p, rec = cases[0]["params"], cases[0]["rec"]
+    frames = [(ptk.pinned_copy(c["ref"]), ptk.pinned_copy(c["cur"])) for c in cases]
+    kw = dict(search_method=ptk.SEARCH_BF16, subpix_method=ptk.SUBPIX_ADJOINT_LM)
+    t = _tracker(ptk, wl, p, rec, 0, **kw)
+    want = _run(_tracker(ptk, wl, p, rec, 0, **kw), frames, rec, pipelined=False)
+    t.load_frame(0, frames[0][0])
+    t.load_frame(1, frames[0][1])
+    for k in range(len(frames)):
+        t.set_grains(rec)
+        t.track_frame(k + 1)
+        if k + 1 < len(frames):
+            t.load_frame(0, frames[k + 1][0])
+            t.load_frame(1, frames[k + 1][1])
+        np.testing.assert_array_equal(t.get_grains(), want[k], err_msg=f"pair {k}")
+        if k + 1 < len(frames):
+            # stage-by-stage reads of both slots: the frames just handed over
+            np.testing.assert_array_equal(t.read_frame(0), np.asarray(frames[k + 1][0]))
+            np.testing.assert_array_equal(t.read_frame(1), np.asarray(frames[k + 1][1]))
+    t.close()
