@@ -829,7 +829,9 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->main_mark, cudaEventDisableTiming);
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaEventCreate"));
   c->stream = c->own_stream;
-  c->pitch = (cfg->dimx + 63) & ~63;
+  // rows of whole 16-byte units as they are (host rows and device rows then
+  // coincide and an upload is one contiguous copy), else padded to 64 pixels
+  c->pitch = cfg->dimx % 16 == 0 ? cfg->dimx : (cfg->dimx + 63) & ~63;
   const size_t bytes = (size_t)c->pitch * cfg->dimy * sizeof(uint16_t);
   for (int k = 0; k < kFrameBufs; ++k) {
     e = cudaMalloc(&c->d_img[k], bytes);
