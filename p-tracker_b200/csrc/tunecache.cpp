@@ -8,8 +8,12 @@
 //
 // The reader accepts any JSON of that shape (whitespace, key order, other
 // keys ignored); an entry whose fields are missing or mistyped makes the
-// file malformed.  Writes replace the file through a temporary file and a
-// rename, so a reader never sees half a file.
+// file malformed.  Writes replace the file through a temporary file of their
+// own (named for the process and the call) and a rename, so a reader never
+// sees half a file; of two writers at once, the last rename wins.
+#include <unistd.h>
+
+#include <atomic>
 #include <cerrno>
 #include <cstdio>
 #include <cstring>
@@ -263,7 +267,9 @@ int save(const char* path, const std::map<std::string, Entry>& m) {
     o += "]}";
   }
   o += "\n}}\n";
-  const std::string tmp = std::string(path) + ".tmp";
+  static std::atomic<unsigned> seq{0};
+  const std::string tmp = std::string(path) + ".tmp." + std::to_string((long)getpid()) + "." +
+                          std::to_string(seq.fetch_add(1));
   FILE* f = fopen(tmp.c_str(), "wb");
   if (!f) return PTK_ERR_IO;
   const bool okw = fwrite(o.data(), 1, o.size(), f) == o.size();
