@@ -270,7 +270,7 @@ int build_steps(ptk_ctx* c, int level) {
   c->d_steps[level] = nullptr;
   cudaError_t e = cudaMalloc(&c->d_steps[level], sizeof(double) * (s.size() ? s.size() : 1));
   if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc(steps)");
-  e = cudaMemcpy(c->d_steps[level], s.data(), sizeof(double) * s.size(), cudaMemcpyHostToDevice);
+  e = cudaMemcpyAsync(c->d_steps[level], s.data(), sizeof(double) * s.size(), cudaMemcpyHostToDevice, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "cudaMemcpy(steps)");
   invalidate(c);
   return PTK_OK;
@@ -347,16 +347,16 @@ int upload_patterns(ptk_ctx* c) {
   CK(cudaMalloc(&c->d_pat0, sizeof(short2) * (total ? total : 1)));
   CK(cudaMalloc(&c->d_w0, sizeof(uint16_t) * (total ? total : 1)));
   CK(cudaMalloc(&c->d_order, sizeof(int) * (n ? n : 1)));
-  CK(cudaMemcpy(c->d_pstart, start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-  if (total) CK(cudaMemcpy(c->d_pat, flat.data(), sizeof(short2) * total, cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(c->d_pstart, start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c->stream));
+  if (total) CK(cudaMemcpyAsync(c->d_pat, flat.data(), sizeof(short2) * total, cudaMemcpyHostToDevice, c->stream));
   // level-0 work order: decreasing pattern size (heavy grains first)
   std::vector<int> order(n);
   for (int i = 0; i < n; ++i) order[i] = i;
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return c->h_pat[a].size() > c->h_pat[b].size(); });
-  if (n) CK(cudaMemcpy(c->d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  if (n) CK(cudaMemcpyAsync(c->d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
   int cnt0 = n;
-  CK(cudaMemcpy(c->d_counts, &cnt0, sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(c->d_counts, &cnt0, sizeof(int), cudaMemcpyHostToDevice, c->stream));
   c->max_P = maxP;
   c->max_R = (int)std::ceil(maxnorm) + 1;
   int max_dup = 1;
@@ -489,8 +489,8 @@ int ensure_bf16(ptk_ctx* c, size_t items) {
     c->d_bf_wofs = nullptr;
     CK(cudaMalloc(&c->d_bf_half, sizeof(int) * half.size()));
     CK(cudaMalloc(&c->d_bf_wofs, sizeof(size_t) * wofs.size()));
-    CK(cudaMemcpy(c->d_bf_half, half.data(), sizeof(int) * half.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->d_bf_wofs, wofs.data(), sizeof(size_t) * wofs.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(c->d_bf_half, half.data(), sizeof(int) * half.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_bf_wofs, wofs.data(), sizeof(size_t) * wofs.size(), cudaMemcpyHostToDevice, c->stream));
     c->h_bf_half = half;
     c->h_bf_wofs = wofs;
     cudaFree(c->d_bf_rot_cs);
@@ -509,7 +509,7 @@ int ensure_bf16(ptk_ctx* c, size_t items) {
       CK(cudaMalloc(&c->d_bf_wslots, bytes));
       c->bf_wslots_bytes = bytes;
       // rotation slots beyond a level's steps are copied with their block: defined contents
-      CK(cudaMemset(c->d_bf_wslots, 0, bytes));
+      CK(cudaMemsetAsync(c->d_bf_wslots, 0, bytes, c->stream));
     }
     c->bf_geom_dirty = false;
     invalidate(c);
@@ -546,7 +546,7 @@ int ensure_bf16_tmaps(ptk_ctx* c, int level, int nrot) {
                                      maps.data()))
     return fail(c, PTK_ERR_CUDA, "cuTensorMapEncodeTiled refused the BF16 operand maps");
   if (!c->d_bf_tmaps[level]) CK(cudaMalloc(&c->d_bf_tmaps[level], sizeof(CUtensorMap) * (size_t)n));
-  CK(cudaMemcpy(c->d_bf_tmaps[level], maps.data(), sizeof(CUtensorMap) * (size_t)n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(c->d_bf_tmaps[level], maps.data(), sizeof(CUtensorMap) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
   c->bf_tmaps_nrot[level] = nrot;
   return PTK_OK;
 }
@@ -836,12 +836,13 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
   for (int k = 0; k < kFrameBufs; ++k) {
     e = cudaMalloc(&c->d_img[k], bytes);
     if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(frame)"));
-    cudaMemset(c->d_img[k], 0, bytes);
+    e = cudaMemsetAsync(c->d_img[k], 0, bytes, c->stream);
+    if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMemsetAsync(frame)"));
   }
   // no work has read the buffers yet (the zeroing above is finished): an
   // upload into any of them need not wait
-  e = cudaDeviceSynchronize();
-  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaDeviceSynchronize"));
+  e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamSynchronize"));
   for (int k = 0; k < kFrameBufs; ++k) c->free_valid[k] = true;
   {  // the BF16 search's tensor maps of the frame buffers (left unset without the driver's encoder)
     CUtensorMap h[kFrameBufs * kBf16FrameMaps];
@@ -851,7 +852,7 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
     if (ok) {
       e = cudaMalloc(&c->d_frame_tmaps, sizeof(h));
       if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(frame maps)"));
-      e = cudaMemcpy(c->d_frame_tmaps, h, sizeof(h), cudaMemcpyHostToDevice);
+      e = cudaMemcpyAsync(c->d_frame_tmaps, h, sizeof(h), cudaMemcpyHostToDevice, c->stream);
       if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMemcpy(frame maps)"));
     }
   }
@@ -859,13 +860,17 @@ int ptk_create(ptk_ctx** out, const ptk_config* cfg) {
   // [4 + level] exact re-search list of a BF16 level
   e = cudaMalloc(&c->d_counts, 8 * sizeof(int));
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(counts)"));
-  cudaMemset(c->d_counts, 0, 8 * sizeof(int));
+  // (on the context stream: the legacy stream does not order with it)
+  e = cudaMemsetAsync(c->d_counts, 0, 8 * sizeof(int), c->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMemsetAsync(counts)"));
   e = cudaMalloc(&c->d_work, 2 * sizeof(int));  // work-queue heads of the BF16 and exact kernels
   if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaMalloc(work)"));
   for (int l = 0; l < 3; ++l) {
     int rc = build_steps(c, l);
     if (rc) return bail(rc);
   }
+  e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaStreamSynchronize"));
   *out = c;
   return PTK_OK;
 }
@@ -1706,7 +1711,7 @@ int ptk_synchronize(ptk_ctx* c) {
   int flag = 0;  // set by a device wait that gave up (BF16 search)
   CK(cudaMemcpy(&flag, c->d_counts + 3, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {
-    CK(cudaMemset(c->d_counts + 3, 0, sizeof(int)));
+    CK(cudaMemsetAsync(c->d_counts + 3, 0, sizeof(int), c->stream));
     return fail(c, PTK_ERR_TIMEOUT, "a tensor-core search wait gave up");
   }
   return PTK_OK;
