@@ -436,18 +436,20 @@ int ptk_disto_create(ptk_disto** out, int dimx, int dimy, const int32_t* refx, c
       ox[g] = (double)refx[g];
       oy[g] = (double)refy[g];
     }
-    ok = cudaMemcpy(d->d_refx, refx, sizeof(int32_t) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(d->d_refy, refy, sizeof(int32_t) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+    ok = cudaMemcpyAsync(d->d_refx, refx, sizeof(int32_t) * n, cudaMemcpyHostToDevice, d->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_refy, refy, sizeof(int32_t) * n, cudaMemcpyHostToDevice, d->stream) == cudaSuccess &&
          (npairs == 0 ||
-          cudaMemcpy(d->d_pairs, pairs_ij, sizeof(int2) * npairs, cudaMemcpyHostToDevice) == cudaSuccess) &&
-         cudaMemcpy(d->d_dx, dx, sizeof(double) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(d->d_dy, dy, sizeof(double) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(d->d_dx0, dx, sizeof(double) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(d->d_dy0, dy, sizeof(double) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(d->d_ncc, ncc_subpix, sizeof(double) * ng, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(d->d_origx, ox.data(), sizeof(double) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(d->d_origy, oy.data(), sizeof(double) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemset(d->d_done, 0, sizeof(unsigned)) == cudaSuccess;
+          cudaMemcpyAsync(d->d_pairs, pairs_ij, sizeof(int2) * npairs, cudaMemcpyHostToDevice, d->stream) == cudaSuccess) &&
+         cudaMemcpyAsync(d->d_dx, dx, sizeof(double) * ng, cudaMemcpyHostToDevice, d->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_dy, dy, sizeof(double) * ng, cudaMemcpyHostToDevice, d->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_dx0, dx, sizeof(double) * ng, cudaMemcpyHostToDevice, d->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_dy0, dy, sizeof(double) * ng, cudaMemcpyHostToDevice, d->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_ncc, ncc_subpix, sizeof(double) * ng, cudaMemcpyHostToDevice, d->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_origx, ox.data(), sizeof(double) * n, cudaMemcpyHostToDevice, d->stream) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_origy, oy.data(), sizeof(double) * n, cudaMemcpyHostToDevice, d->stream) == cudaSuccess &&
+         cudaMemsetAsync(d->d_done, 0, sizeof(unsigned), d->stream) == cudaSuccess &&
+         // (on the fit's stream, which does not order with the legacy stream)
+         cudaStreamSynchronize(d->stream) == cudaSuccess;
   }
   if (!ok) {
     ptk_disto_destroy(d);
@@ -597,8 +599,9 @@ int ptk_disto_objective_timed(ptk_disto* d, const double* params14, int reps, do
 int ptk_disto_tracked(ptk_disto* d, double* dx, double* dy) {
   if (!d || !dx || !dy) return dfail(d, PTK_ERR_ARG, "null argument");
   const size_t ng = (size_t)d->nimg1 * d->n;
-  cudaError_t e = cudaMemcpy(dx, d->d_dx, sizeof(double) * ng, cudaMemcpyDeviceToHost);
-  if (e == cudaSuccess) e = cudaMemcpy(dy, d->d_dy, sizeof(double) * ng, cudaMemcpyDeviceToHost);
+  cudaError_t e = cudaMemcpyAsync(dx, d->d_dx, sizeof(double) * ng, cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dy, d->d_dy, sizeof(double) * ng, cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
   if (e != cudaSuccess) return dfail(d, PTK_ERR_CUDA, cudaGetErrorString(e));
   return PTK_OK;
 }
