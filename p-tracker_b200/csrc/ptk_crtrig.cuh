@@ -92,7 +92,6 @@ PTK_HD dd dd_add(dd a, dd b) {
   s.lo = add_rn(s.lo, t.lo);
   return fast_two_sum(s.hi, s.lo);
 }
-PTK_HD dd dd_neg(dd a) { return dd{-a.hi, -a.lo}; }
 PTK_HD dd dd_mul(dd a, dd b) {
   dd p = two_prod(a.hi, b.hi);
   p.lo = add_rn(p.lo, add_rn(mul_rn(a.hi, b.lo), mul_rn(a.lo, b.hi)));
